@@ -1,0 +1,108 @@
+/* rxcuda: C ABI of the B200 ReaxFF force + charge-equilibration engine (librxcuda.so).
+ *
+ * This is the boundary the reference's LAMMPS adapter binds for its GPU path. Each entry point names the reference
+ * interface it replaces (file:line in the reference tree):
+ *   - the device context  reaxmetal::mtl::Context          include/reaxmetal/metal_backend.hpp:57-95
+ *   - the force-field reader  parse_force_field           src/io/ffield_parser.cpp:91, include/reaxmetal/forcefield.hpp:134
+ *   - the pair style's compute  PairReaxFFMetal::compute  plugin/adapter/pair_reaxff_metal.cpp:412-524
+ *   - the charge fix  FixQEqReaxFFMetal::{compute_H, CG, sparse_matvec, calculate_Q}
+ *                                                          plugin/adapter/fix_qeq_reaxff_metal.cpp:65-205
+ *
+ * Conventions (as the reference's Context): the caller owns every host array; the context copies inputs into
+ * persistent device buffers and copies results back; one context per host thread; every call is synchronous with
+ * respect to the host arrays it takes. Errors never cross the ABI as exceptions: every call returns an RX_* status
+ * and rx_last_error() holds the message. Units are LAMMPS `real`: Angstrom, kcal/mol, e, fs, g/mol.
+ *
+ * A context holds one or more independent periodic systems ("batch"); atoms of system s occupy the index range
+ * [offset_s, offset_s + natoms_s) of every per-atom array, in system order.
+ */
+#ifndef RXCUDA_H
+#define RXCUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RX_OK 0
+#define RX_ERR_INVALID 1        /* invalid argument or input (SystemError / FfieldError in the reference) */
+#define RX_ERR_FFIELD 2         /* force-field text rejected by the strict reader */
+#define RX_ERR_CAPACITY 3       /* a per-atom list overflowed after the grow-and-retry budget (neighbor.cpp:362-374) */
+#define RX_ERR_CUDA 4           /* CUDA runtime error or no device */
+#define RX_ERR_NOT_CONVERGED 5  /* charge equilibration hit its iteration limit in strict mode (fix_qeq_reaxff_metal.cpp:79-80) */
+#define RX_ERR_STATE 6          /* entry point called before what it needs (force field, systems) */
+#define RX_ERR_TIMEOUT 7        /* a device wait exceeded its bound */
+
+/* rx_compute flags */
+#define RX_COMPUTE_QEQ 1        /* solve the charges (fix qeq/reaxff/metal resident) before the force evaluation */
+#define RX_COMPUTE_CENSUS 2     /* fill the decision census (include/reaxmetal/census.hpp:12-20) */
+
+typedef struct rx_context rx_context;
+
+/* mtl::Context construction (metal_backend.hpp:57-60). device: CUDA ordinal, or -1 for a host-only context that reads
+ * and inspects force fields only (every device entry point then returns RX_ERR_STATE). NULL on failure (no device). */
+rx_context* rx_create(int device);
+void rx_destroy(rx_context* ctx);
+/* message of the last failed call on this context ("" if none); also valid for ctx == NULL (creation errors) */
+const char* rx_last_error(const rx_context* ctx);
+
+/* parse_force_field (src/io/ffield_parser.cpp:91-451): strict reader; lgvdw = 1 for `pair_style reaxff lgvdw yes`. */
+int rx_set_forcefield(rx_context* ctx, const char* ffield_text, int lgvdw);
+/* canonical_table_dump (src/io/table_dump.cpp:20-84) of the parsed tables. Returns the length (without NUL) and
+ * writes at most outlen bytes including the NUL; negative on error. */
+long rx_forcefield_dump(rx_context* ctx, int portable, char* out, long outlen);
+/* PairReaxFFMetal::extract("chi"|"eta"|"gamma") (pair_reaxff_metal.cpp:212-227): per force-field type, eta is twice the
+ * file value. Arrays of ntypes entries (0-based type index). */
+int rx_forcefield_params(rx_context* ctx, int* ntypes, double* chi, double* eta, double* gamma, double* mass);
+
+/* ControlParams (include/reaxmetal/forcefield.hpp:73-78) and the `enobonds` pair_style keyword (bonded.hpp:25). */
+int rx_set_control(rx_context* ctx, double bond_cut, double hbond_cut, double thb_cut, double thb_cutsq, int enobonds);
+
+/* The systems of this context. natoms[nsys]; origin[3*nsys]; box[9*nsys] lattice vectors a, b, c as rows;
+ * periodic[3*nsys] (must be 1: the engine is periodic in all directions); type[NA] force-field type index;
+ * tag[NA] atom ids, unique within a system (the owner-computes tie-breaks of neighbor.cpp:295-310 use them). */
+int rx_set_systems(rx_context* ctx, int nsys, const int* natoms, const double* origin, const double* box, const int* periodic,
+                   const int* type, const int64_t* tag);
+int rx_num_atoms(const rx_context* ctx);
+int rx_set_positions(rx_context* ctx, const double* x);   /* x[3*NA] */
+int rx_get_positions(rx_context* ctx, double* x);         /* positions as held (wrapped into the primary cell) */
+int rx_set_charges(rx_context* ctx, const double* q);     /* q[NA] */
+int rx_get_charges(rx_context* ctx, double* q);
+
+/* fix qeq/reaxff/metal <nevery> <swa> <swb> <tol> reaxff [maxiter imax] (fix_qeq_reaxff_metal.cpp; ENGINE_SPEC 7).
+ * strict = 1: non-convergence is an error (RX_ERR_NOT_CONVERGED), 0: it is reported through iters/rel only. */
+int rx_set_qeq(rx_context* ctx, double swa, double swb, double tol, int imax, int strict);
+/* mtl::Context::qeq_solve (metal_backend.hpp:84-86): builds H (compute_H), solves H s = -chi and H t = -1 with the
+ * Jacobi-preconditioned CG from the history-extrapolated guesses (Q-23), sets q = s - (sum s / sum t) t
+ * (calculate_Q) and advances the histories. iters[2*nsys] and rel[2*nsys] (s then t per system) may be NULL. */
+int rx_qeq_solve(rx_context* ctx, int* iters, double* rel);
+/* mtl::Context::qeq_matvec (metal_backend.hpp:82): y = (diag(eta) + H) v over the owned atoms, v[NA], y[NA]. */
+int rx_qeq_matvec(rx_context* ctx, const double* v, double* y);
+
+/* PairReaxFFMetal::compute (pair_reaxff_metal.cpp:412-524) for every system: energies[13*nsys] in the reference's
+ * EnergyTerm order (bond, over, under, lone_pair, valence, penalty, coalition, hbond, torsion, conjugation, vdw,
+ * coulomb, polarization; kcal/mol), grad[3*NA] = dE/dx (the physical force is -grad), census[7*NA] (bonds,
+ * angle_sets, torsions, hbonds, nonbonded, sbo_region, lp_trunc; only with RX_COMPUTE_CENSUS), counts[4] (bonds,
+ * counted non-bonded pairs, neighbor entries, H-bond triples). Any output pointer may be NULL. */
+int rx_compute(rx_context* ctx, int flags, double* energies, double* grad, int32_t* census, int64_t* counts);
+
+/* Nose-Hoover chain NVT (the LAMMPS `fix nvt temp Tstart Tstop Tdamp` the reference's examples run), velocity Verlet
+ * with dt [fs]. mass[ntypes] g/mol per force-field type. Charges are re-equilibrated before every force evaluation. */
+int rx_md_setup(rx_context* ctx, const double* mass, double dt, double t_start, double t_stop, double t_damp, int chain);
+int rx_set_velocities(rx_context* ctx, const double* v);  /* v[3*NA] A/fs */
+int rx_get_velocities(rx_context* ctx, double* v);
+/* nsteps steps of every system; energies (13*nsys, last step) and temperature (nsys) may be NULL */
+int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature);
+
+/* The CUDA stream the context launches on (a cudaStream_t), for callers that time or order work around it. */
+void* rx_stream(rx_context* ctx);
+/* Per-phase device time of the last rx_compute / rx_md_run (milliseconds, summed over the call) when timing is on:
+ * names is a '\n'-separated list written into names_out; returns the number of phases. */
+int rx_set_timing(rx_context* ctx, int on);
+int rx_phase_times(rx_context* ctx, char* names_out, long names_len, double* ms, int max_phases);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,178 @@
+// Device-side data layout of the B200 ReaxFF engine.
+//
+// Periodic images are never materialised as ghost atoms. Every neighbor and bond entry of an owned atom names its
+// partner as (owner atom index, lattice shift), packed into one 32-bit code: the low `abits` bits hold the atom index,
+// the high bits the shift index sidx = ((sx+smax)*S + (sy+smax))*S + (sz+smax), S = 2*smax+1. The reverse entry of
+// (i -> j, s) is (j -> i, -s), whose shift index is S^3-1-sidx. Results equal those of the reference's ghost-native
+// traversal (src/neighbor/neighbor.cpp:18-88 expands images, src/cpu/bonded.cpp runs over them) wherever its ghost
+// shell is complete, which its shell rule guarantees for owned atoms.
+//
+// Per-atom bond slots: atom a owns slots [a*bcap, a*bcap + bcnt[a]); every slot knows the global index of its reverse
+// slot (bsym). All cross-atom contributions (forces on bond partners, CdDelta of partners, torsion contributions to
+// second neighbors) are written into slots owned by the writing atom and gathered by the receiving atom in a fixed
+// order: no atomics, bitwise reproducible.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rx {
+
+constexpr int kTerms = 13;   // bond, over, under, lone_pair, valence, penalty, coalition, hbond, torsion, conjugation, vdw, coulomb, polarization
+constexpr int kCensus = 7;   // bonds, angle_sets, torsions, hbonds, nonbonded, sbo_region, lp_trunc
+enum Term { E_BOND, E_OV, E_UN, E_LP, E_ANG, E_PEN, E_COA, E_HB, E_TOR, E_CON, E_VDW, E_ELE, E_POL };
+
+// status bits written by kernels (read by the host after a launch sequence)
+enum Status : int {
+  ST_NBR_OVERFLOW = 1,
+  ST_BOND_OVERFLOW = 2,
+  ST_SYM_MISSING = 4,
+  ST_SHIFT_RANGE = 8,
+  ST_CG_BREAKDOWN = 16,
+  ST_NONFINITE = 32,
+};
+
+struct SysInfo {
+  double origin[3];
+  double L[9];    // lattice vectors a, b, c as rows
+  double R[9];    // rows of the inverse transform: f_d = R[d] . (r - origin)
+  int begin, natoms;
+  int nc[3];      // cells per lattice direction
+  int cell_begin;
+  int range[3];   // cell search range per direction
+};
+
+struct DevFF {
+  int nt, vdw_type, lg;
+  double bo_cut, nonb_low, nonb_cut;
+  const double* gp;
+  const double* sb;
+  const double* tb;
+  const int* thb_n;
+  const double* thb;
+  const int* fb_on;
+  const double* fb;
+  const int* hb_on;
+  const double* hb;
+  double tap[8];   // taper coefficients on [nonb_low, nonb_cut] (include/reaxmetal/terms_host.hpp:16-29)
+};
+
+struct DevCtl {
+  double bond_cut, hbond_cut, thb_cut, thb_cutsq;
+  int enobonds;
+};
+
+struct AtomQ {   // atom_quantities (include/reaxmetal/terms.hpp:141-164) plus the corrected total bond order
+  double total_bo, Delta, Delta_e, Delta_boc, Delta_val, vlpex, nlp, Delta_lp, dDelta_lp, Delta_lp_temp;
+};
+
+struct Dev {
+  int na, nsys;
+  const SysInfo* sys;
+  const int* sys_of;
+  double4* x;            // positions (w unused)
+  const int* type;
+  const long long* tag;
+  double* q;             // charges
+  // cells
+  int* cell_key;         // global cell of every atom (sort key)
+  int* cell_atoms;       // atoms sorted by cell
+  int* cell_start;       // ncell_total + 1
+  int ncell_total;
+  // neighbor rows (full: both directions, every image within nonb_cut)
+  int ncap;
+  unsigned* nbr;
+  int* nbr_cnt;
+  double* hval;          // charge-matrix entry of every neighbor entry (0 beyond swb)
+  int abits;
+  unsigned amask;
+  int smax, S;
+  // bonds
+  int bcap;
+  unsigned* bcode;
+  int* bsym;
+  int* bcnt;
+  double4* bdv;          // x_partner - x_self (xyz), distance (w)
+  double4* bBO;          // BO, BO_s, BO_pi, BO_pi2 (uncorrected minus bo_cut, then corrected in place)
+  double4* bdBOp;        // dBOp (xyz)
+  double4* bdlnpi;       // dln_BOp_pi (xyz)
+  double4* bdlnpi2;      // dln_BOp_pi2 (xyz)
+  double4* bC0;          // C1dbo, C2dbo, C3dbo, C1dbopi
+  double4* bC1;          // C2dbopi, C3dbopi, C4dbopi, C1dbopi2
+  double4* bC2;          // C2dbopi2, C3dbopi2, C4dbopi2, -
+  double4* bacc;         // Cdbo, Cdbopi, Cdbopi2, CdDelta contribution to the partner
+  double4* bfn;          // gradient contribution to the partner (xyz)
+  double4* Tl;           // torsion: per (central slot, position in the far atom's slots): gradient xyz, Cdbo (w)
+  // atoms
+  double* Deltap;
+  double* Deltap_boc;
+  double4* dDp_self;
+  AtomQ* aq;
+  double4* fown;         // gradient on the atom itself (xyz), own CdDelta (w)
+  double* cdtot;
+  double* W;
+  double4* fdb;
+  double4* fnb;          // non-bonded gradient
+  double4* grad;         // result
+  double* eatom;         // kTerms per atom
+  int* census;           // kCensus per atom (atom-major: census[c*na + a])
+  int* status;
+  long long* counters;   // [0] neighbor entries, [1] counted pairs, [2] bonds (directed), [3] H-bond triples
+};
+
+// ----------------------------------------------------------------------------------------------- helpers
+__host__ __device__ inline int floor_div(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
+
+__device__ inline void decode_shift(int sidx, int S, int smax, int& sx, int& sy, int& sz) {
+  sz = sidx % S - smax;
+  sy = (sidx / S) % S - smax;
+  sx = sidx / (S * S) - smax;
+}
+
+// Lattice shift L.s summed in the reference's order (src/core/system.cpp:52-57: r[c] += s[k] * vectors[k][c]).
+__device__ inline void lattice_shift(const SysInfo& s, int sx, int sy, int sz, double* sh) {
+  for (int c = 0; c < 3; ++c) {
+    double r = 0.0;
+    r += static_cast<double>(sx) * s.L[0 + c];
+    r += static_cast<double>(sy) * s.L[3 + c];
+    r += static_cast<double>(sz) * s.L[6 + c];
+    sh[c] = r;
+  }
+}
+
+// Canonical separation vector of the entry (i -> j at shift s): computed from the lower-index end (for i == j from the
+// positive shift) and negated for the other direction, so both directions of a pair see bitwise-negated vectors and
+// identical distances; every cut-off decision is therefore symmetric.
+__device__ inline void pair_dvec(const Dev& d, const SysInfo& s, int i, int j, int sidx, double* dv) {
+  int sx, sy, sz;
+  decode_shift(sidx, d.S, d.smax, sx, sy, sz);
+  const int center = (d.S * d.S * d.S - 1) / 2;
+  const bool fwd = (j > i) || (j == i && sidx > center);
+  double sh[3];
+  if (fwd) {
+    lattice_shift(s, sx, sy, sz, sh);
+    const double4 xi = d.x[i], xj = d.x[j];
+    dv[0] = (xj.x + sh[0]) - xi.x;
+    dv[1] = (xj.y + sh[1]) - xi.y;
+    dv[2] = (xj.z + sh[2]) - xi.z;
+  } else {
+    lattice_shift(s, -sx, -sy, -sz, sh);
+    const double4 xi = d.x[i], xj = d.x[j];
+    dv[0] = -((xi.x + sh[0]) - xj.x);
+    dv[1] = -((xi.y + sh[1]) - xj.y);
+    dv[2] = -((xi.z + sh[2]) - xj.z);
+  }
+}
+
+__device__ inline double safe_exp(double v) { return exp(v > 700.0 ? 700.0 : v); }
+__device__ inline float safe_expf(float v) { return __expf(v > 40.f ? 40.f : v); }
+
+__device__ inline double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ inline float warp_sumf(float v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace rx

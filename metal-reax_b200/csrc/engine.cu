@@ -1,0 +1,868 @@
+// Host side of the engine: device buffers, capacity growth, the launch sequence of one force evaluation, the charge
+// solve, the NVT loop, and the C ABI declared in include/rxcuda.h.
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/rxcuda.h"
+#include "device.cuh"
+#include "ffield.hpp"
+#include "kernels.hpp"
+#include "md.hpp"
+
+namespace rx {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define RXCU(call)                                                                                             \
+  do {                                                                                                         \
+    cudaError_t e_ = (call);                                                                                   \
+    if (e_ != cudaSuccess) throw ::rx::Error(RX_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+  } while (0)
+
+// A device allocation that only grows.
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { if (p) cudaFree(p); }
+  void ensure(size_t want) {
+    if (want <= n && p) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    const size_t m = want > 0 ? want : 1;
+    RXCU(cudaMalloc(&p, m * sizeof(T)));
+    n = m;
+  }
+};
+
+static void taper_coeffs(double swa, double swb, double* c) {   // include/reaxmetal/terms_host.hpp:16-29
+  const double d1 = swb - swa, d7 = std::pow(d1, 7.0);
+  const double swa2 = swa * swa, swa3 = swa * swa * swa, swb2 = swb * swb, swb3 = swb * swb * swb;
+  c[7] = 20.0 / d7;
+  c[6] = -70.0 * (swa + swb) / d7;
+  c[5] = 84.0 * (swa2 + 3.0 * swa * swb + swb2) / d7;
+  c[4] = -35.0 * (swa3 + 9.0 * swa2 * swb + 9.0 * swa * swb2 + swb3) / d7;
+  c[3] = 140.0 * (swa3 * swb + 3.0 * swa2 * swb2 + swa * swb3) / d7;
+  c[2] = -210.0 * (swa3 * swb2 + swa2 * swb3) / d7;
+  c[1] = 140.0 * swa3 * swb3 / d7;
+  c[0] = (-35.0 * swa3 * swb2 * swb2 + 21.0 * swa2 * swb3 * swb2 - 7.0 * swa * swb3 * swb3 + swb3 * swb3 * swb) / d7;
+}
+
+struct Phase {
+  const char* name;
+  cudaEvent_t a, b;
+  double ms;
+};
+
+struct Context {
+  int device = 0;
+  int nsm = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  bool have_ff = false;
+  ForceField ff;
+  DBuf<double> ff_buf;
+  DevFF dff{};
+  DevCtl ctl{5.0, 7.5, 0.001, 0.00001, 1};
+  QeqParams qp{};
+  double qeq_tol = 1e-6;
+  int qeq_imax = 200;
+  int qeq_strict = 0;
+
+  // systems
+  int nsys = 0, na = 0;
+  std::vector<SysInfo> hsys;
+  std::vector<int> hsys_of;
+  DBuf<SysInfo> sys;
+  DBuf<int> sys_of, type, cell_key, cell_key_sorted, cell_atoms, atom_iota, cell_start;
+  DBuf<long long> tag;
+  DBuf<double4> x;
+  DBuf<double> q;
+  DBuf<unsigned char> cub_tmp;
+  int ncell_total = 0;
+  int smax = 1, S = 3, abits = 27;
+  bool have_pos = false;
+
+  // lists
+  int ncap = 0, bcap = 0;
+  DBuf<unsigned> nbr, bcode;
+  DBuf<int> nbr_cnt, bsym, bcnt;
+  DBuf<double> hval;
+  DBuf<double4> bdv, bBO, bdBOp, bdlnpi, bdlnpi2, bC0, bC1, bC2, bacc, bfn, Tl;
+  // atoms
+  DBuf<double> Deltap, Deltap_boc, cdtot, W, eatom;
+  DBuf<double4> dDp_self, fown, fdb, fnb, grad;
+  DBuf<AtomQ> aq;
+  DBuf<int> census, status;
+  DBuf<long long> counters;
+  DBuf<double> energies;
+  // QEq
+  DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
+  DBuf<double> cg_eta, cg_part, s_hist, t_hist, cg_rel;
+  DBuf<int> cg_iters;
+  std::vector<int> last_iters;
+  std::vector<double> last_rel;
+  // MD
+  bool md_ready = false;
+  DBuf<double4> v;
+  DBuf<double> mass, ke, temp, scale, xi, vxi;
+  MdDev md{};
+  long long md_step = 0;
+  // timing
+  bool timing = false;
+  std::vector<Phase> phases;
+
+  // dev < 0: a host-only context (force-field reading and inspection; every device entry point reports RX_ERR_STATE)
+  bool host_only = false;
+  explicit Context(int dev) : device(dev) {
+    if (dev < 0) {
+      host_only = true;
+      device = 0;
+      return;
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) throw Error(RX_ERR_CUDA, "no CUDA device");
+    if (dev < 0 || dev >= n) throw Error(RX_ERR_INVALID, "device ordinal out of range");
+    RXCU(cudaSetDevice(dev));
+    RXCU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    RXCU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    status.ensure(4);
+    counters.ensure(8);
+    set_qeq(0.0, 10.0, 1e-6, 200, 0);
+  }
+  ~Context() {
+    if (host_only) return;
+    for (auto& p : phases) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  // ------------------------------------------------------------------ configuration
+  void set_forcefield(const char* text, int lg) {
+    if (!text) throw Error(RX_ERR_INVALID, "null force-field text");
+    try {
+      ff = parse_force_field(text, lg != 0);
+    } catch (const FfieldError& e) {
+      throw Error(RX_ERR_FFIELD, e.what());
+    }
+    const size_t nsb = ff.sb.size(), ntb = ff.tb.size(), nthb = ff.thb.size(), nfb = ff.fb.size(), nhb = ff.hb.size();
+    const size_t nthn = ff.thb_n.size(), nfo = ff.fb_on.size(), nho = ff.hb_on.size();
+    // ints are stored in the same buffer as doubles (one double slot per int)
+    const size_t total = 64 + nsb + ntb + nthb + nfb + nhb + nthn + nfo + nho;
+    std::vector<double> h(total, 0.0);
+    size_t off = 0;
+    auto put = [&](const double* src, size_t n) { std::memcpy(h.data() + off, src, n * sizeof(double)); size_t o = off; off += n; return o; };
+    std::vector<double> gp(64, 0.0);
+    std::copy(ff.gp.begin(), ff.gp.end(), gp.begin());
+    const size_t o_gp = put(gp.data(), 64), o_sb = put(ff.sb.data(), nsb), o_tb = put(ff.tb.data(), ntb), o_thb = put(ff.thb.data(), nthb);
+    const size_t o_fb = put(ff.fb.data(), nfb), o_hb = put(ff.hb.data(), nhb);
+    auto put_int = [&](const std::vector<int>& v) {
+      const size_t o = off;
+      std::memcpy(reinterpret_cast<int*>(h.data() + off), v.data(), v.size() * sizeof(int));
+      off += (v.size() * sizeof(int) + sizeof(double) - 1) / sizeof(double);
+      return o;
+    };
+    const size_t o_thn = put_int(ff.thb_n), o_fo = put_int(ff.fb_on), o_ho = put_int(ff.hb_on);
+    if (host_only) {
+      have_ff = true;
+      return;
+    }
+    ff_buf.ensure(total);
+    RXCU(cudaMemcpy(ff_buf.p, h.data(), total * sizeof(double), cudaMemcpyHostToDevice));
+    dff.nt = ff.nt;
+    dff.vdw_type = ff.vdw_type;
+    dff.lg = lg != 0;
+    dff.bo_cut = ff.bo_cut;
+    dff.nonb_low = ff.nonb_low;
+    dff.nonb_cut = ff.nonb_cut;
+    dff.gp = ff_buf.p + o_gp;
+    dff.sb = ff_buf.p + o_sb;
+    dff.tb = ff_buf.p + o_tb;
+    dff.thb = ff_buf.p + o_thb;
+    dff.fb = ff_buf.p + o_fb;
+    dff.hb = ff_buf.p + o_hb;
+    dff.thb_n = reinterpret_cast<const int*>(ff_buf.p + o_thn);
+    dff.fb_on = reinterpret_cast<const int*>(ff_buf.p + o_fo);
+    dff.hb_on = reinterpret_cast<const int*>(ff_buf.p + o_ho);
+    taper_coeffs(ff.nonb_low, ff.nonb_cut, dff.tap);
+    have_ff = true;
+    if (nsys > 0) layout_systems();
+  }
+
+  void set_control(double bond_cut, double hbond_cut, double thb_cut, double thb_cutsq, int enobonds) {
+    if (!(bond_cut > 0) || !(hbond_cut >= 0) || !std::isfinite(bond_cut) || !std::isfinite(hbond_cut))
+      throw Error(RX_ERR_INVALID, "cut-offs must be finite, bond_cut > 0, hbond_cut >= 0");
+    ctl = DevCtl{bond_cut, hbond_cut, thb_cut, thb_cutsq, enobonds};
+  }
+
+  void set_qeq(double swa, double swb, double tol, int imax, int strict) {
+    if (!(swb > swa) || !(tol > 0) || imax < 1) throw Error(RX_ERR_INVALID, "fix qeq: need swb > swa, tol > 0, imax >= 1");
+    qp.swa = swa;
+    qp.swb = swb;
+    taper_coeffs(swa, swb, qp.tap);
+    qeq_tol = tol;
+    qeq_imax = imax;
+    qeq_strict = strict;
+  }
+
+  void require_ff() const { if (!have_ff) throw Error(RX_ERR_STATE, "no force field set"); }
+  void require_sys() const {
+    if (host_only) throw Error(RX_ERR_STATE, "host-only context (created with device < 0)");
+    if (nsys == 0) throw Error(RX_ERR_STATE, "no systems set");
+  }
+
+  void set_systems(int n_sys, const int* natoms, const double* origin, const double* box, const int* periodic, const int* types,
+                   const int64_t* tags) {
+    require_ff();
+    if (host_only) throw Error(RX_ERR_STATE, "host-only context (created with device < 0)");
+    if (n_sys <= 0 || !natoms || !origin || !box || !types || !tags) throw Error(RX_ERR_INVALID, "set_systems: null or empty input");
+    long long total = 0;
+    for (int s = 0; s < n_sys; ++s) {
+      if (natoms[s] <= 0) throw Error(RX_ERR_INVALID, "every system needs at least one atom");
+      total += natoms[s];
+      if (periodic)
+        for (int k = 0; k < 3; ++k)
+          if (!periodic[3 * s + k]) throw Error(RX_ERR_INVALID, "the engine handles fully periodic systems only");
+    }
+    if (total > (1LL << 30)) throw Error(RX_ERR_INVALID, "too many atoms");
+    for (long long a = 0; a < total; ++a)
+      if (types[a] < 0 || types[a] >= ff.nt) throw Error(RX_ERR_INVALID, "atom " + std::to_string(a) + " has a type outside the force field");
+    nsys = n_sys;
+    na = static_cast<int>(total);
+    hsys.assign(static_cast<size_t>(nsys), SysInfo{});
+    hsys_of.resize(static_cast<size_t>(na));
+    int begin = 0;
+    for (int s = 0; s < nsys; ++s) {
+      SysInfo& si = hsys[static_cast<size_t>(s)];
+      for (int c = 0; c < 3; ++c) si.origin[c] = origin[3 * s + c];
+      for (int c = 0; c < 9; ++c) si.L[c] = box[9 * s + c];
+      si.begin = begin;
+      si.natoms = natoms[s];
+      for (int a = 0; a < natoms[s]; ++a) hsys_of[static_cast<size_t>(begin + a)] = s;
+      begin += natoms[s];
+    }
+    sys_of.ensure(static_cast<size_t>(na));
+    type.ensure(static_cast<size_t>(na));
+    tag.ensure(static_cast<size_t>(na));
+    RXCU(cudaMemcpy(sys_of.p, hsys_of.data(), sizeof(int) * na, cudaMemcpyHostToDevice));
+    RXCU(cudaMemcpy(type.p, types, sizeof(int) * na, cudaMemcpyHostToDevice));
+    static_assert(sizeof(long long) == sizeof(int64_t), "tag width");
+    RXCU(cudaMemcpy(tag.p, tags, sizeof(long long) * na, cudaMemcpyHostToDevice));
+    x.ensure(static_cast<size_t>(na));
+    q.ensure(static_cast<size_t>(na));
+    RXCU(cudaMemset(q.p, 0, sizeof(double) * na));
+    s_hist.ensure(4 * static_cast<size_t>(na));
+    t_hist.ensure(4 * static_cast<size_t>(na));
+    RXCU(cudaMemset(s_hist.p, 0, sizeof(double) * 4 * na));
+    RXCU(cudaMemset(t_hist.p, 0, sizeof(double) * 4 * na));
+    have_pos = false;
+    md_ready = false;
+    ncap = 0;
+    bcap = 0;
+    layout_systems();
+  }
+
+  // cell grids, search ranges, shift encoding, neighbor capacity estimate
+  void layout_systems() {
+    const double rc = ff.nonb_cut;
+    if (!(rc > 0)) throw Error(RX_ERR_INVALID, "force field has no positive non-bonded cut-off");
+    if (ctl.bond_cut > rc || ctl.hbond_cut > rc) throw Error(RX_ERR_INVALID, "bond_cut and hbond_cut must not exceed the non-bonded cut-off");
+    if (qp.swb > rc) throw Error(RX_ERR_INVALID, "fix qeq: the taper radius exceeds the force field's nonb_cut (qeq_device.cpp:14)");
+    int cell_begin = 0, sm = 1;
+    double max_density = 0;
+    for (auto& si : hsys) {
+      const double* L = si.L;
+      const double* a = L; const double* b = L + 3; const double* c = L + 6;
+      auto cross = [](const double* u, const double* w, double* o) { o[0] = u[1] * w[2] - u[2] * w[1]; o[1] = u[2] * w[0] - u[0] * w[2]; o[2] = u[0] * w[1] - u[1] * w[0]; };
+      double bc[3], ca[3], ab[3];
+      cross(b, c, bc); cross(c, a, ca); cross(a, b, ab);
+      const double det = a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2];
+      if (!(det > 0) || !std::isfinite(det)) throw Error(RX_ERR_INVALID, "box must be right-handed and non-degenerate");
+      for (int k = 0; k < 3; ++k) { si.R[k] = bc[k] / det; si.R[3 + k] = ca[k] / det; si.R[6 + k] = ab[k] / det; }
+      const double h[3] = {det / std::sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]), det / std::sqrt(ca[0] * ca[0] + ca[1] * ca[1] + ca[2] * ca[2]),
+                           det / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2])};
+      long long ncell = 1;
+      for (int k = 0; k < 3; ++k) {
+        int n = static_cast<int>(std::floor(h[k] * 2.0 / rc));
+        n = std::max(1, std::min(n, 512));
+        si.nc[k] = n;
+        const double w = h[k] / n;
+        si.range[k] = static_cast<int>(std::ceil(rc / w - 1e-12));
+        const int s_lo = (si.range[k] + n - 1) / n;
+        const int s_hi = (n - 1 + si.range[k]) / n;
+        sm = std::max(sm, std::max(s_lo, s_hi));
+        ncell *= n;
+      }
+      si.cell_begin = cell_begin;
+      cell_begin += static_cast<int>(ncell);
+      max_density = std::max(max_density, si.natoms / det);
+    }
+    smax = sm;
+    S = 2 * smax + 1;
+    const long long nshift = static_cast<long long>(S) * S * S;
+    int sbits = 0;
+    while ((1LL << sbits) < nshift) ++sbits;
+    abits = 32 - sbits;
+    if (static_cast<long long>(na) >= (1LL << abits))
+      throw Error(RX_ERR_INVALID, "too many atoms for the periodic-image encoding of these boxes");
+    ncell_total = cell_begin;
+    sys.ensure(static_cast<size_t>(nsys));
+    RXCU(cudaMemcpy(sys.p, hsys.data(), sizeof(SysInfo) * nsys, cudaMemcpyHostToDevice));
+    cell_key.ensure(static_cast<size_t>(na));
+    cell_key_sorted.ensure(static_cast<size_t>(na));
+    cell_atoms.ensure(static_cast<size_t>(na));
+    atom_iota.ensure(static_cast<size_t>(na));
+    cell_start.ensure(static_cast<size_t>(ncell_total) + 1);
+    {
+      std::vector<int> io(static_cast<size_t>(na));
+      for (int a = 0; a < na; ++a) io[static_cast<size_t>(a)] = a;
+      RXCU(cudaMemcpy(atom_iota.p, io.data(), sizeof(int) * na, cudaMemcpyHostToDevice));
+    }
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, 32, stream);
+    cub_tmp.ensure(tmp);
+    const double expect = 4.0 / 3.0 * M_PI * rc * rc * rc * max_density;
+    const int want_ncap = static_cast<int>(std::ceil((expect * 1.3 + 32) / 32.0)) * 32;
+    if (ncap < want_ncap) ncap = want_ncap;
+    if (bcap < 8) bcap = 8;
+    alloc_atoms();
+    alloc_lists();
+  }
+
+  void alloc_atoms() {
+    const size_t n = static_cast<size_t>(na);
+    Deltap.ensure(n); Deltap_boc.ensure(n); cdtot.ensure(n); W.ensure(n); eatom.ensure(n * kTerms);
+    dDp_self.ensure(n); fown.ensure(n); fdb.ensure(n); fnb.ensure(n); grad.ensure(n);
+    aq.ensure(n); census.ensure(n * kCensus);
+    nbr_cnt.ensure(n); bcnt.ensure(n);
+    energies.ensure(static_cast<size_t>(nsys) * kTerms);
+    cg_x.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
+    cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
+    cg_part.ensure(8 * static_cast<size_t>(std::max(nsm, 1)) * 32);
+  }
+
+  void alloc_lists() {
+    const size_t n = static_cast<size_t>(na);
+    nbr.ensure(n * ncap);
+    hval.ensure(n * ncap);
+    const size_t nb = n * bcap;
+    bcode.ensure(nb); bsym.ensure(nb);
+    bdv.ensure(nb); bBO.ensure(nb); bdBOp.ensure(nb); bdlnpi.ensure(nb); bdlnpi2.ensure(nb);
+    bC0.ensure(nb); bC1.ensure(nb); bC2.ensure(nb); bacc.ensure(nb); bfn.ensure(nb);
+    Tl.ensure(nb * bcap);
+  }
+
+  Dev dev() {
+    Dev d{};
+    d.na = na; d.nsys = nsys; d.sys = sys.p; d.sys_of = sys_of.p; d.x = x.p; d.type = type.p; d.tag = tag.p; d.q = q.p;
+    d.cell_key = cell_key.p; d.cell_atoms = cell_atoms.p; d.cell_start = cell_start.p; d.ncell_total = ncell_total;
+    d.ncap = ncap; d.nbr = nbr.p; d.nbr_cnt = nbr_cnt.p; d.hval = hval.p;
+    d.abits = abits; d.amask = (abits >= 32) ? 0xffffffffu : ((1u << abits) - 1u); d.smax = smax; d.S = S;
+    d.bcap = bcap; d.bcode = bcode.p; d.bsym = bsym.p; d.bcnt = bcnt.p; d.bdv = bdv.p; d.bBO = bBO.p; d.bdBOp = bdBOp.p;
+    d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p;
+    d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
+    d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.census = census.p; d.status = status.p;
+    d.counters = counters.p;
+    return d;
+  }
+
+  // ------------------------------------------------------------------ timing
+  void tic(int k, const char* name) {
+    if (!timing) return;
+    while (static_cast<int>(phases.size()) <= k) {
+      Phase p{name, nullptr, nullptr, 0.0};
+      cudaEventCreate(&p.a);
+      cudaEventCreate(&p.b);
+      phases.push_back(p);
+    }
+    phases[static_cast<size_t>(k)].name = name;
+    cudaEventRecord(phases[static_cast<size_t>(k)].a, stream);
+  }
+  void toc(int k) {
+    if (!timing) return;
+    cudaEventRecord(phases[static_cast<size_t>(k)].b, stream);
+  }
+  void collect_times() {
+    if (!timing) return;
+    for (auto& p : phases) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) p.ms += ms;
+    }
+  }
+
+  // ------------------------------------------------------------------ the force evaluation
+  static unsigned blocks(long long n, int per) { return static_cast<unsigned>((n + per - 1) / per); }
+
+  void build_lists(const Dev& d) {
+    tic(0, "neighbors");
+    k_wrap_bin<<<blocks(na, 256), 256, 0, stream>>>(d);
+    size_t tmp = cub_tmp.n;
+    RXCU(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, 32, stream));
+    k_cell_start<<<blocks(na + 1, 256), 256, 0, stream>>>(d, cell_key_sorted.p);
+    k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, qp);
+    toc(0);
+  }
+
+  CgArgs cg_args() {
+    CgArgs a{};
+    a.imax = qeq_imax; a.tol = qeq_tol;
+    a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.eta = cg_eta.p; a.part = cg_part.p;
+    a.out_iters = cg_iters.p; a.out_rel = cg_rel.p;
+    return a;
+  }
+
+  void launch_qeq(const Dev& d) {
+    tic(1, "qeq");
+    CgArgs a = cg_args();
+    k_qeq_prepare<<<blocks(na, 256), 256, 0, stream>>>(d, dff, a, s_hist.p, t_hist.p);
+    if (nsys == 1 && na > 4096) {
+      const int threads = 256;
+      int per_sm = 0;
+      RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_grid, threads, 0));
+      int grid = std::max(1, std::min(per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
+      grid = std::min(grid, nsm * 32);
+      a.begin = 0;
+      a.n = na;
+      void* args[] = {const_cast<Dev*>(&d), &a};
+      RXCU(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_grid), dim3(grid), dim3(threads), args, 0, stream));
+    } else {
+      k_cg_block<<<nsys, 512, 0, stream>>>(d, a);
+    }
+    toc(1);
+  }
+
+  void launch_bonded(const Dev& d) {
+    tic(2, "bond_orders");
+    k_bonds<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, ctl);
+    k_bond_sym<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d);
+    k_bo_correct<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d, dff);
+    k_atom_quantities<<<blocks(na, 128), 128, 0, stream>>>(d, dff);
+    toc(2);
+    tic(3, "bonded_terms");
+    k_bonded_atom<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
+    k_hbond_acceptor<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
+    toc(3);
+    tic(4, "torsion");
+    k_torsion<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
+    toc(4);
+  }
+
+  void launch_nonbonded(const Dev& d) {
+    tic(5, "nonbonded");
+    k_nonbonded<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff);
+    toc(5);
+  }
+
+  void launch_gather(const Dev& d) {
+    tic(6, "gather");
+    k_fold<<<blocks(na, 128), 128, 0, stream>>>(d);
+    k_dbond<<<blocks(na, 128), 128, 0, stream>>>(d);
+    k_force_final<<<blocks(na, 128), 128, 0, stream>>>(d);
+    toc(6);
+  }
+
+  // One force evaluation of every system, with grow-and-retry of the list capacities (neighbor.cpp:362-374,
+  // bonded_device.cpp:117-190). With `do_qeq` the charges are equilibrated first and the histories advanced on success.
+  void evaluate(bool do_qeq) {
+    require_ff();
+    require_sys();
+    if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
+    for (int attempt = 0;; ++attempt) {
+      RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * 4, stream));
+      const Dev d = dev();
+      build_lists(d);
+      if (do_qeq) launch_qeq(d);
+      launch_bonded(d);
+      launch_nonbonded(d);
+      launch_gather(d);
+      int st[4];
+      RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
+      RXCU(cudaStreamSynchronize(stream));
+      RXCU(cudaGetLastError());
+      if (st[0] & (ST_NBR_OVERFLOW | ST_BOND_OVERFLOW)) {
+        if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "list capacity still exceeded after 4 grow attempts");
+        if (st[0] & ST_NBR_OVERFLOW) ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
+        if (st[0] & ST_BOND_OVERFLOW) bcap = std::max(bcap, ((st[2] * 5 / 4) + 3) / 4 * 4);
+        alloc_lists();
+        continue;
+      }
+      if (st[0] & ST_SHIFT_RANGE) throw Error(RX_ERR_INVALID, "a periodic image outside the shift encoding was requested");
+      if (st[0] & ST_NONFINITE) throw Error(RX_ERR_INVALID, "non-finite coordinate");
+      if (st[0] & ST_SYM_MISSING) throw Error(RX_ERR_INVALID, "inconsistent bond list (a bond without its reverse)");
+      if (do_qeq) {
+        if (st[0] & ST_CG_BREAKDOWN) throw Error(RX_ERR_NOT_CONVERGED, "charge equilibration: CG breakdown");
+        finish_qeq();
+      }
+      break;
+    }
+    collect_times();
+  }
+
+  void finish_qeq() {
+    last_iters.resize(2 * static_cast<size_t>(nsys));
+    last_rel.resize(2 * static_cast<size_t>(nsys));
+    RXCU(cudaMemcpy(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost));
+    RXCU(cudaMemcpy(last_rel.data(), cg_rel.p, sizeof(double) * 2 * nsys, cudaMemcpyDeviceToHost));
+    k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(dev(), cg_x.p, s_hist.p, t_hist.p);
+    RXCU(cudaStreamSynchronize(stream));
+    if (qeq_strict)
+      for (size_t k = 0; k < last_rel.size(); ++k)
+        if (!(last_rel[k] <= qeq_tol))
+          throw Error(RX_ERR_NOT_CONVERGED, "charge equilibration did not converge after " + std::to_string(qeq_imax) +
+                                                " iterations (relative residual " + std::to_string(last_rel[k]) + ")");
+  }
+
+  void energy_sums() {
+    k_energy_sum<<<nsys, 256, 0, stream>>>(dev(), energies.p);
+  }
+
+  // ------------------------------------------------------------------ state I/O
+  void set_positions(const double* xin) {
+    require_sys();
+    std::vector<double4> h(static_cast<size_t>(na));
+    for (int a = 0; a < na; ++a) h[static_cast<size_t>(a)] = make_double4(xin[3 * a], xin[3 * a + 1], xin[3 * a + 2], 0.0);
+    RXCU(cudaMemcpyAsync(x.p, h.data(), sizeof(double4) * na, cudaMemcpyHostToDevice, stream));
+    RXCU(cudaStreamSynchronize(stream));
+    have_pos = true;
+  }
+  void get_positions(double* xout) {
+    require_sys();
+    std::vector<double4> h(static_cast<size_t>(na));
+    RXCU(cudaMemcpyAsync(h.data(), x.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, stream));
+    RXCU(cudaStreamSynchronize(stream));
+    for (int a = 0; a < na; ++a) { xout[3 * a] = h[a].x; xout[3 * a + 1] = h[a].y; xout[3 * a + 2] = h[a].z; }
+  }
+
+  void compute(int flags, double* e_out, double* g_out, int32_t* cen_out, int64_t* counts) {
+    evaluate((flags & RX_COMPUTE_QEQ) != 0);
+    energy_sums();
+    if (e_out) RXCU(cudaMemcpyAsync(e_out, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
+    std::vector<double4> g;
+    if (g_out) {
+      g.resize(static_cast<size_t>(na));
+      RXCU(cudaMemcpyAsync(g.data(), grad.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, stream));
+    }
+    if (cen_out) RXCU(cudaMemcpyAsync(cen_out, census.p, sizeof(int) * kCensus * na, cudaMemcpyDeviceToHost, stream));
+    std::vector<int> nb, bc;
+    if (counts) {
+      nb.resize(static_cast<size_t>(na));
+      bc.resize(static_cast<size_t>(na));
+      RXCU(cudaMemcpyAsync(nb.data(), nbr_cnt.p, sizeof(int) * na, cudaMemcpyDeviceToHost, stream));
+      RXCU(cudaMemcpyAsync(bc.data(), bcnt.p, sizeof(int) * na, cudaMemcpyDeviceToHost, stream));
+    }
+    RXCU(cudaStreamSynchronize(stream));
+    if (g_out)
+      for (int a = 0; a < na; ++a) { g_out[3 * a] = g[a].x; g_out[3 * a + 1] = g[a].y; g_out[3 * a + 2] = g[a].z; }
+    if (counts) {
+      long long sb = 0, sn = 0;
+      for (int a = 0; a < na; ++a) { sb += bc[a]; sn += nb[a]; }
+      std::vector<int> cen(static_cast<size_t>(kCensus) * na);
+      RXCU(cudaMemcpy(cen.data(), census.p, sizeof(int) * kCensus * na, cudaMemcpyDeviceToHost));
+      long long pairs = 0, hb = 0;
+      for (int a = 0; a < na; ++a) { pairs += cen[4 * static_cast<size_t>(na) + a]; hb += cen[3 * static_cast<size_t>(na) + a]; }
+      counts[0] = sb / 2;
+      counts[1] = pairs;
+      counts[2] = sn;
+      counts[3] = hb;
+    }
+  }
+
+  void qeq_solve(int* iters, double* rel) {
+    require_ff();
+    require_sys();
+    if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
+    for (int attempt = 0;; ++attempt) {
+      RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * 4, stream));
+      const Dev d = dev();
+      build_lists(d);
+      launch_qeq(d);
+      int st[4];
+      RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
+      RXCU(cudaStreamSynchronize(stream));
+      RXCU(cudaGetLastError());
+      if (st[0] & ST_NBR_OVERFLOW) {
+        if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "neighbor capacity still exceeded after 4 grow attempts");
+        ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
+        alloc_lists();
+        continue;
+      }
+      if (st[0] & ST_SHIFT_RANGE) throw Error(RX_ERR_INVALID, "a periodic image outside the shift encoding was requested");
+      if (st[0] & ST_NONFINITE) throw Error(RX_ERR_INVALID, "non-finite coordinate");
+      if (st[0] & ST_CG_BREAKDOWN) throw Error(RX_ERR_NOT_CONVERGED, "charge equilibration: CG breakdown");
+      finish_qeq();
+      break;
+    }
+    if (iters) std::copy(last_iters.begin(), last_iters.end(), iters);
+    if (rel) std::copy(last_rel.begin(), last_rel.end(), rel);
+  }
+
+  void qeq_matvec(const double* vin, double* yout) {
+    require_ff();
+    require_sys();
+    if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
+    for (int attempt = 0;; ++attempt) {
+      RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * 4, stream));
+      build_lists(dev());
+      int st[4];
+      RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
+      RXCU(cudaStreamSynchronize(stream));
+      if (st[0] & ST_NBR_OVERFLOW) {
+        if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "neighbor capacity still exceeded after 4 grow attempts");
+        ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
+        alloc_lists();
+        continue;
+      }
+      break;
+    }
+    std::vector<double2> h(static_cast<size_t>(na));
+    for (int a = 0; a < na; ++a) h[static_cast<size_t>(a)] = make_double2(vin[a], 0.0);
+    RXCU(cudaMemcpy(cg_d.p, h.data(), sizeof(double2) * na, cudaMemcpyHostToDevice));
+    k_qeq_matvec<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(dev(), dff, cg_d.p, cg_q.p);
+    RXCU(cudaMemcpyAsync(h.data(), cg_q.p, sizeof(double2) * na, cudaMemcpyDeviceToHost, stream));
+    RXCU(cudaStreamSynchronize(stream));
+    for (int a = 0; a < na; ++a) yout[a] = h[static_cast<size_t>(a)].x;
+  }
+
+  // ------------------------------------------------------------------ MD
+  void md_setup(const double* mass_in, double dt, double t0, double t1, double tdamp, int chain) {
+    require_ff();
+    require_sys();
+    if (!(dt > 0) || !(t0 > 0) || !(t1 > 0) || !(tdamp > 0) || chain < 1 || chain > kMaxChain)
+      throw Error(RX_ERR_INVALID, "md_setup: need dt, temperatures, damping > 0 and 1 <= chain <= 8");
+    mass.ensure(static_cast<size_t>(ff.nt));
+    RXCU(cudaMemcpy(mass.p, mass_in, sizeof(double) * ff.nt, cudaMemcpyHostToDevice));
+    v.ensure(static_cast<size_t>(na));
+    ke.ensure(static_cast<size_t>(nsys)); temp.ensure(static_cast<size_t>(nsys)); scale.ensure(static_cast<size_t>(nsys));
+    xi.ensure(static_cast<size_t>(nsys) * kMaxChain); vxi.ensure(static_cast<size_t>(nsys) * kMaxChain);
+    RXCU(cudaMemset(xi.p, 0, sizeof(double) * nsys * kMaxChain));
+    RXCU(cudaMemset(vxi.p, 0, sizeof(double) * nsys * kMaxChain));
+    RXCU(cudaMemset(v.p, 0, sizeof(double4) * na));
+    md = MdDev{v.p, mass.p, ke.p, temp.p, scale.p, xi.p, vxi.p, dt, t0, t1, tdamp, chain};
+    md_ready = true;
+    md_step = 0;
+  }
+
+  void set_velocities(const double* vin) {
+    if (!md_ready) throw Error(RX_ERR_STATE, "call rx_md_setup first");
+    std::vector<double4> h(static_cast<size_t>(na));
+    for (int a = 0; a < na; ++a) h[static_cast<size_t>(a)] = make_double4(vin[3 * a], vin[3 * a + 1], vin[3 * a + 2], 0.0);
+    RXCU(cudaMemcpy(v.p, h.data(), sizeof(double4) * na, cudaMemcpyHostToDevice));
+  }
+  void get_velocities(double* vout) {
+    if (!md_ready) throw Error(RX_ERR_STATE, "call rx_md_setup first");
+    std::vector<double4> h(static_cast<size_t>(na));
+    RXCU(cudaMemcpy(h.data(), v.p, sizeof(double4) * na, cudaMemcpyDeviceToHost));
+    for (int a = 0; a < na; ++a) { vout[3 * a] = h[a].x; vout[3 * a + 1] = h[a].y; vout[3 * a + 2] = h[a].z; }
+  }
+
+  void thermostat_half(double frac) {
+    k_md_kinetic<<<nsys, 256, 0, stream>>>(md, sys.p, type.p);
+    k_md_chain<<<blocks(nsys, 64), 64, 0, stream>>>(md, sys.p, nsys, frac);
+    k_md_scale<<<blocks(na, 256), 256, 0, stream>>>(md, sys_of.p, na);
+  }
+
+  void md_run(int nsteps, double* e_out, double* t_out, long long total_steps_hint) {
+    if (!md_ready) throw Error(RX_ERR_STATE, "call rx_md_setup first");
+    if (md_step == 0) evaluate(true);   // forces of the initial configuration
+    const long long span = total_steps_hint > 0 ? total_steps_hint : nsteps;
+    for (int s = 0; s < nsteps; ++s) {
+      const double frac = span > 0 ? static_cast<double>(s) / static_cast<double>(span) : 0.0;
+      thermostat_half(frac);
+      k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 1);
+      evaluate(true);
+      k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 0);
+      thermostat_half(frac);
+      ++md_step;
+    }
+    energy_sums();
+    if (e_out) RXCU(cudaMemcpyAsync(e_out, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
+    if (t_out) {
+      k_md_kinetic<<<nsys, 256, 0, stream>>>(md, sys.p, type.p);
+      std::vector<double> kk(static_cast<size_t>(nsys));
+      RXCU(cudaMemcpyAsync(kk.data(), ke.p, sizeof(double) * nsys, cudaMemcpyDeviceToHost, stream));
+      RXCU(cudaStreamSynchronize(stream));
+      for (int s = 0; s < nsys; ++s) t_out[s] = 2.0 * kk[s] / ((3.0 * hsys[s].natoms - 3.0) * 0.0019872067);
+    }
+    RXCU(cudaStreamSynchronize(stream));
+  }
+};
+
+}  // namespace rx
+
+// ======================================================================================================== C ABI
+struct rx_context {
+  std::unique_ptr<rx::Context> c;
+  std::string err;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(rx_context* ctx, F&& f) {
+  if (!ctx || !ctx->c) return RX_ERR_STATE;
+  try {
+    if (!ctx->c->host_only) cudaSetDevice(ctx->c->device);
+    f(*ctx->c);
+    ctx->err.clear();
+    return RX_OK;
+  } catch (const rx::Error& e) {
+    ctx->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    ctx->err = e.what();
+    return RX_ERR_INVALID;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+rx_context* rx_create(int device) {
+  try {
+    auto* ctx = new rx_context;
+    ctx->c = std::make_unique<rx::Context>(device);
+    g_create_error.clear();
+    return ctx;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    return nullptr;
+  }
+}
+
+void rx_destroy(rx_context* ctx) { delete ctx; }
+
+const char* rx_last_error(const rx_context* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+int rx_set_forcefield(rx_context* ctx, const char* text, int lgvdw) {
+  return guarded(ctx, [&](rx::Context& c) { c.set_forcefield(text, lgvdw); });
+}
+
+long rx_forcefield_dump(rx_context* ctx, int portable, char* out, long outlen) {
+  long result = -1;
+  const int rc = guarded(ctx, [&](rx::Context& c) {
+    c.require_ff();
+    const std::string s = c.ff.canonical_dump(portable != 0);
+    if (out && outlen > 0) {
+      const size_t m = std::min<size_t>(s.size(), static_cast<size_t>(outlen - 1));
+      std::memcpy(out, s.data(), m);
+      out[m] = 0;
+    }
+    result = static_cast<long>(s.size());
+  });
+  return rc == RX_OK ? result : -1;
+}
+
+int rx_forcefield_params(rx_context* ctx, int* ntypes, double* chi, double* eta, double* gamma, double* mass) {
+  return guarded(ctx, [&](rx::Context& c) {
+    c.require_ff();
+    if (ntypes) *ntypes = c.ff.nt;
+    for (int t = 0; t < c.ff.nt; ++t) {
+      if (chi) chi[t] = c.ff.s(t, rx::SB_CHI);
+      if (eta) eta[t] = c.ff.s(t, rx::SB_ETA);
+      if (gamma) gamma[t] = c.ff.s(t, rx::SB_GAMMA);
+      if (mass) mass[t] = c.ff.s(t, rx::SB_MASS);
+    }
+  });
+}
+
+int rx_set_control(rx_context* ctx, double bond_cut, double hbond_cut, double thb_cut, double thb_cutsq, int enobonds) {
+  return guarded(ctx, [&](rx::Context& c) { c.set_control(bond_cut, hbond_cut, thb_cut, thb_cutsq, enobonds); });
+}
+
+int rx_set_systems(rx_context* ctx, int nsys, const int* natoms, const double* origin, const double* box, const int* periodic,
+                   const int* type, const int64_t* tag) {
+  return guarded(ctx, [&](rx::Context& c) { c.set_systems(nsys, natoms, origin, box, periodic, type, tag); });
+}
+
+int rx_num_atoms(const rx_context* ctx) { return (ctx && ctx->c) ? ctx->c->na : 0; }
+
+int rx_set_positions(rx_context* ctx, const double* x) {
+  return guarded(ctx, [&](rx::Context& c) {
+    if (!x) throw rx::Error(RX_ERR_INVALID, "null positions");
+    c.set_positions(x);
+  });
+}
+int rx_get_positions(rx_context* ctx, double* x) { return guarded(ctx, [&](rx::Context& c) { c.get_positions(x); }); }
+
+int rx_set_charges(rx_context* ctx, const double* q) {
+  return guarded(ctx, [&](rx::Context& c) {
+    c.require_sys();
+    RXCU(cudaMemcpy(c.q.p, q, sizeof(double) * c.na, cudaMemcpyHostToDevice));
+  });
+}
+int rx_get_charges(rx_context* ctx, double* q) {
+  return guarded(ctx, [&](rx::Context& c) {
+    c.require_sys();
+    RXCU(cudaMemcpy(q, c.q.p, sizeof(double) * c.na, cudaMemcpyDeviceToHost));
+  });
+}
+
+int rx_set_qeq(rx_context* ctx, double swa, double swb, double tol, int imax, int strict) {
+  return guarded(ctx, [&](rx::Context& c) {
+    c.set_qeq(swa, swb, tol, imax, strict);
+    if (c.have_ff && c.nsys > 0) c.layout_systems();
+  });
+}
+int rx_qeq_solve(rx_context* ctx, int* iters, double* rel) { return guarded(ctx, [&](rx::Context& c) { c.qeq_solve(iters, rel); }); }
+int rx_qeq_matvec(rx_context* ctx, const double* v, double* y) { return guarded(ctx, [&](rx::Context& c) { c.qeq_matvec(v, y); }); }
+
+int rx_compute(rx_context* ctx, int flags, double* energies, double* grad, int32_t* census, int64_t* counts) {
+  return guarded(ctx, [&](rx::Context& c) { c.compute(flags, energies, grad, census, counts); });
+}
+
+int rx_md_setup(rx_context* ctx, const double* mass, double dt, double t_start, double t_stop, double t_damp, int chain) {
+  return guarded(ctx, [&](rx::Context& c) { c.md_setup(mass, dt, t_start, t_stop, t_damp, chain); });
+}
+int rx_set_velocities(rx_context* ctx, const double* v) { return guarded(ctx, [&](rx::Context& c) { c.set_velocities(v); }); }
+int rx_get_velocities(rx_context* ctx, double* v) { return guarded(ctx, [&](rx::Context& c) { c.get_velocities(v); }); }
+int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature) {
+  return guarded(ctx, [&](rx::Context& c) { c.md_run(nsteps, energies, temperature, 0); });
+}
+
+void* rx_stream(rx_context* ctx) { return (ctx && ctx->c) ? reinterpret_cast<void*>(ctx->c->stream) : nullptr; }
+
+int rx_set_timing(rx_context* ctx, int on) {
+  return guarded(ctx, [&](rx::Context& c) {
+    c.timing = on != 0;
+    for (auto& p : c.phases) p.ms = 0.0;
+  });
+}
+
+int rx_phase_times(rx_context* ctx, char* names_out, long names_len, double* ms, int max_phases) {
+  if (!ctx || !ctx->c) return 0;
+  std::string names;
+  int n = 0;
+  for (auto& p : ctx->c->phases) {
+    if (n >= max_phases) break;
+    if (ms) ms[n] = p.ms;
+    names += p.name;
+    names += "\n";
+    ++n;
+  }
+  if (names_out && names_len > 0) {
+    const size_t m = std::min<size_t>(names.size(), static_cast<size_t>(names_len - 1));
+    std::memcpy(names_out, names.data(), m);
+    names_out[m] = 0;
+  }
+  return n;
+}
+
+}  // extern "C"

@@ -1,0 +1,54 @@
+// Kernel entry points and their argument structs (shared by the kernel files and the host engine).
+#pragma once
+#include "device.cuh"
+#include "ffield.hpp"
+
+namespace rx {
+
+constexpr int SB_N = SB_NFIELDS;
+constexpr int TB_N = TB_NFIELDS;
+
+struct QeqParams {
+  double swa, swb;
+  double tap[8];   // taper coefficients on [swa, swb]
+};
+
+struct CgArgs {
+  int begin, n, imax;
+  double tol;
+  double2* x;      // (s, t)
+  double2* b;
+  double2* r;
+  double2* d;
+  double2* p;
+  double2* q;
+  double* eta;
+  double* part;    // 2 * 4 * gridDim.x partial sums (double-buffered)
+  int* out_iters;
+  double* out_rel;
+};
+using CgBatchArgs = CgArgs;
+
+__global__ void k_wrap_bin(Dev d);
+__global__ void k_cell_start(Dev d, const int* sorted_keys);
+__global__ void k_neighbors(Dev d, DevFF ff, QeqParams qp);
+__global__ void k_nonbonded(Dev d, DevFF ff);
+__global__ void k_cg_grid(Dev d, CgArgs a);
+__global__ void k_cg_block(Dev d, CgBatchArgs a);
+__global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, const double* t_hist);
+__global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist);
+__global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y);
+__global__ void k_energy_sum(Dev d, double* out);
+
+__global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl);
+__global__ void k_bond_sym(Dev d);
+__global__ void k_bo_correct(Dev d, DevFF ff);
+__global__ void k_atom_quantities(Dev d, DevFF ff);
+__global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl);
+__global__ void k_hbond_acceptor(Dev d, DevFF ff, DevCtl ctl);
+__global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl);
+__global__ void k_fold(Dev d);
+__global__ void k_dbond(Dev d);
+__global__ void k_force_final(Dev d);
+
+}  // namespace rx

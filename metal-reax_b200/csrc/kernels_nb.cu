@@ -1,0 +1,594 @@
+// Cell lists, full neighbor rows with the charge matrix, non-bonded forces, charge-equilibration CG, energy sums.
+#include <cooperative_groups.h>
+
+#include "device.cuh"
+#include "kernels.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace rx {
+
+// ------------------------------------------------------------------------------------------------ wrap + bin
+// Owned atoms are wrapped into the primary cell first (expand_images with wrap_owned, src/neighbor/neighbor.cpp:45-61),
+// then binned into a uniform grid over the fractional coordinates of their system.
+__global__ void k_wrap_bin(Dev d) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= d.na) return;
+  const SysInfo s = d.sys[d.sys_of[a]];
+  double4 x = d.x[a];
+  double r[3] = {x.x, x.y, x.z};
+  double f[3];
+  for (int k = 0; k < 3; ++k) f[k] = s.R[3 * k] * (r[0] - s.origin[0]) + s.R[3 * k + 1] * (r[1] - s.origin[1]) + s.R[3 * k + 2] * (r[2] - s.origin[2]);
+  bool moved = false;
+  for (int k = 0; k < 3; ++k) {
+    const double fl = floor(f[k]);
+    if (fl != 0.0) {
+      for (int c = 0; c < 3; ++c) r[c] -= fl * s.L[3 * k + c];
+      moved = true;
+    }
+  }
+  if (moved) {
+    for (int k = 0; k < 3; ++k) f[k] = s.R[3 * k] * (r[0] - s.origin[0]) + s.R[3 * k + 1] * (r[1] - s.origin[1]) + s.R[3 * k + 2] * (r[2] - s.origin[2]);
+    x.x = r[0]; x.y = r[1]; x.z = r[2];
+    d.x[a] = x;
+  }
+  if (!(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]))) atomicOr(d.status, ST_NONFINITE);
+  int c[3];
+  for (int k = 0; k < 3; ++k) {
+    int v = static_cast<int>(floor(f[k] * s.nc[k]));
+    v = v < 0 ? 0 : (v >= s.nc[k] ? s.nc[k] - 1 : v);
+    c[k] = v;
+  }
+  d.cell_key[a] = s.cell_begin + (c[2] * s.nc[1] + c[1]) * s.nc[0] + c[0];
+}
+
+// cell_start[c] = first position in the sorted order whose key is >= c
+__global__ void k_cell_start(Dev d, const int* sorted_keys) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > d.na) return;
+  const int prev = p == 0 ? -1 : sorted_keys[p - 1];
+  const int cur = p == d.na ? d.ncell_total : sorted_keys[p];
+  for (int c = prev + 1; c <= cur; ++c) d.cell_start[c] = p;
+}
+
+// ------------------------------------------------------------------------------------------------ neighbor rows
+__device__ inline void taper_horner(const double* c, double r, double& Tap, double& dTap) {
+  double t = c[7] * r + c[6];
+  t = t * r + c[5]; t = t * r + c[4]; t = t * r + c[3]; t = t * r + c[2]; t = t * r + c[1]; t = t * r + c[0];
+  double g = 7 * c[7] * r + 6 * c[6];
+  g = g * r + 5 * c[5]; g = g * r + 4 * c[4]; g = g * r + 3 * c[3]; g = g * r + 2 * c[2];
+  g += c[1] / r;
+  Tap = t;
+  dTap = g;
+}
+
+// One warp per atom: every image of every atom within nonb_cut (the owned-row cut-off of build_far_list,
+// src/neighbor/neighbor.cpp:180-212), found through the cells within `range` of the atom's cell, periodic images
+// included. Entries are written in cell-scan order through a warp ballot (deterministic). Fused: the charge-matrix
+// entry H = 14.4 Tap(r) / cbrt(r^3 + (gamma_i gamma_j)^-1.5) for r <= swb (ENGINE_SPEC 7; fix_qeq_reaxff compute_H).
+__global__ void k_neighbors(Dev d, DevFF ff, QeqParams qp) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= d.na) return;
+  const int i = warp;
+  const SysInfo s = d.sys[d.sys_of[i]];
+  const int key = d.cell_key[i] - s.cell_begin;
+  const int cx = key % s.nc[0], cy = (key / s.nc[0]) % s.nc[1], cz = key / (s.nc[0] * s.nc[1]);
+  const double rc2 = ff.nonb_cut * ff.nonb_cut;
+  const int ti = d.type[i];
+  const double gi = ff.sb[ti * SB_N + SB_GAMMA];
+  int count = 0;
+  const unsigned lt = (1u << lane) - 1u;
+  const int center = (d.S * d.S * d.S - 1) / 2;
+  for (int oz = -s.range[2]; oz <= s.range[2]; ++oz) {
+    const int zz = cz + oz, shz = floor_div(zz, s.nc[2]), wz = zz - shz * s.nc[2];
+    for (int oy = -s.range[1]; oy <= s.range[1]; ++oy) {
+      const int yy = cy + oy, shy = floor_div(yy, s.nc[1]), wy = yy - shy * s.nc[1];
+      for (int ox = -s.range[0]; ox <= s.range[0]; ++ox) {
+        const int xx = cx + ox, shx = floor_div(xx, s.nc[0]), wx = xx - shx * s.nc[0];
+        if (shx < -d.smax || shx > d.smax || shy < -d.smax || shy > d.smax || shz < -d.smax || shz > d.smax) {
+          if (lane == 0) atomicOr(d.status, ST_SHIFT_RANGE);
+          continue;
+        }
+        const int sidx = ((shx + d.smax) * d.S + (shy + d.smax)) * d.S + (shz + d.smax);
+        const int cell = s.cell_begin + (wz * s.nc[1] + wy) * s.nc[0] + wx;
+        const int c0 = d.cell_start[cell], c1 = d.cell_start[cell + 1];
+        for (int base = c0; base < c1; base += 32) {
+          const int p = base + lane;
+          bool ok = false;
+          int j = 0;
+          double r2 = 0.0;
+          if (p < c1) {
+            j = d.cell_atoms[p];
+            if (!(j == i && sidx == center)) {
+              double dv[3];
+              pair_dvec(d, s, i, j, sidx, dv);
+              r2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+              ok = r2 <= rc2;
+            }
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, ok);
+          if (ok) {
+            const int pos = count + __popc(m & lt);
+            if (pos < d.ncap) {
+              const size_t e = static_cast<size_t>(i) * d.ncap + pos;
+              d.nbr[e] = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
+              const double r = sqrt(r2);
+              double h = 0.0;
+              if (r <= qp.swb) {
+                double Tap, dTap;
+                taper_horner(qp.tap, r, Tap, dTap);
+                const double shld = pow(gi * ff.sb[d.type[j] * SB_N + SB_GAMMA], -1.5);
+                h = Tap * 14.4 / cbrt(r * r * r + shld);
+              }
+              d.hval[e] = h;
+            }
+          }
+          count += __popc(m);
+        }
+      }
+    }
+  }
+  if (lane == 0) {
+    d.nbr_cnt[i] = count;
+    if (count > d.ncap) {
+      atomicOr(d.status, ST_NBR_OVERFLOW);
+      atomicMax(d.status + 1, count);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ non-bonded
+// taper_stable (include/reaxmetal/terms.hpp:268-272): the FP32-safe form in t = (r - swa)/(swb - swa)
+__device__ inline void taper_stable_f(float swa, float swb, float r, float& Tap, float& dTap) {
+  const float dd = swb - swa, t = (r - swa) / dd, t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
+  Tap = 1.f - t4 * (35.f - 84.f * t + 70.f * t2 - 20.f * t3);
+  dTap = (t3 * (-140.f + 420.f * t - 420.f * t2 + 140.f * t3)) / (dd * r);
+}
+
+// One warp per atom over its full row (FP32 pair arithmetic, FP64 accumulation). The gradient of atom i collects
+// -CE * dvec from every entry of its own row, so no write ever touches another atom. Energies use the reference's
+// counted pairs (owner-computes rule, classify_nonbonded_entry, src/neighbor/neighbor.cpp:295-310): an entry counts
+// at i if it is owned-owned with j > i, or a periodic image with tag_i < tag_j or, for an image of i itself, the
+// positive direction; each counted entry contributes its full pair energy (terms::nonbonded_pair, terms.hpp:282-323).
+__global__ void k_nonbonded(Dev d, DevFF ff) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= d.na) return;
+  const int i = warp;
+  const SysInfo s = d.sys[d.sys_of[i]];
+  const int ti = d.type[i];
+  const int cnt = min(d.nbr_cnt[i], d.ncap);
+  const float p_vdW1 = static_cast<float>(ff.gp[28]), p_vdW1i = 1.f / p_vdW1;
+  const float swa = static_cast<float>(ff.nonb_low), swb = static_cast<float>(ff.nonb_cut);
+  const float qi = static_cast<float>(d.q[i]);
+  const long long tag_i = d.tag[i];
+  const int center = (d.S * d.S * d.S - 1) / 2;
+  double gx = 0, gy = 0, gz = 0, ev = 0, ee = 0;
+  int counted = 0;
+  for (int e = lane; e < cnt; e += 32) {
+    const unsigned code = d.nbr[static_cast<size_t>(i) * d.ncap + e];
+    const int j = static_cast<int>(code & d.amask);
+    const int sidx = static_cast<int>(code >> d.abits);
+    double dvd[3];
+    pair_dvec(d, s, i, j, sidx, dvd);
+    const float dx = static_cast<float>(dvd[0]), dy = static_cast<float>(dvd[1]), dz = static_cast<float>(dvd[2]);
+    const float r = static_cast<float>(sqrt(dvd[0] * dvd[0] + dvd[1] * dvd[1] + dvd[2] * dvd[2]));
+    const int tj = d.type[j];
+    const double* tb = ff.tb + (static_cast<size_t>(ti) * ff.nt + tj) * TB_N;
+    float Tap, dTap;
+    taper_stable_f(swa, swb, r, Tap, dTap);
+    const float alpha = static_cast<float>(tb[TB_ALPHA]), D = static_cast<float>(tb[TB_D]), r_vdW = static_cast<float>(tb[TB_R_VDW]);
+    float e_vdW = 0.f, CEvd;
+    if (ff.vdw_type == 1 || ff.vdw_type == 3) {
+      const float powr_vdW1 = powf(r, p_vdW1);
+      const float powgi_vdW1 = powf(1.f / static_cast<float>(tb[TB_GAMMA_W]), p_vdW1);
+      const float fn13 = powf(powr_vdW1 + powgi_vdW1, p_vdW1i);
+      const float exp1 = __expf(alpha * (1.f - fn13 / r_vdW));
+      const float exp2 = __expf(0.5f * alpha * (1.f - fn13 / r_vdW));
+      const float evd = D * (exp1 - 2.f * exp2);
+      e_vdW += Tap * evd;
+      const float dfn13 = powf(powr_vdW1 + powgi_vdW1, p_vdW1i - 1.f) * powf(r, p_vdW1 - 2.f);
+      CEvd = dTap * evd - Tap * D * (alpha / r_vdW) * (exp1 - exp2) * dfn13;
+    } else {
+      const float exp1 = __expf(alpha * (1.f - r / r_vdW));
+      const float exp2 = __expf(0.5f * alpha * (1.f - r / r_vdW));
+      const float evd = D * (exp1 - 2.f * exp2);
+      e_vdW += Tap * evd;
+      CEvd = dTap * evd - Tap * D * (alpha / r_vdW) * (exp1 - exp2) / r;
+    }
+    if (ff.vdw_type == 2 || ff.vdw_type == 3) {
+      const float ecore = static_cast<float>(tb[TB_ECORE]), acore = static_cast<float>(tb[TB_ACORE]), rcore = static_cast<float>(tb[TB_RCORE]);
+      const float e_core = ecore * __expf(acore * (1.f - (r / rcore)));
+      e_vdW += Tap * e_core;
+      const float de_core = -(acore / rcore) * e_core;
+      CEvd += dTap * e_core + Tap * de_core / r;
+      if (ff.lg) {
+        const float r5 = powf(r, 5.f), r6 = powf(r, 6.f), re6 = powf(static_cast<float>(tb[TB_LGRE]), 6.f);
+        const float e_lg = -(static_cast<float>(tb[TB_LGCIJ]) / (r6 + re6));
+        e_vdW += Tap * e_lg;
+        const float de_lg = -6.f * e_lg * r5 / (r6 + re6);
+        CEvd += dTap * e_lg + Tap * de_lg / r;
+      }
+    }
+    const float qj = static_cast<float>(d.q[j]);
+    const float dr3gamij_1 = r * r * r + static_cast<float>(tb[TB_GAMMA]);
+    const float dr3gamij_3 = cbrtf(dr3gamij_1);
+    const float e_ele = 332.06371f * qi * qj * (Tap / dr3gamij_3);
+    const float CEclmb = 332.06371f * qi * qj * (dTap - Tap * r / dr3gamij_1) / dr3gamij_3;
+    const float CE = CEvd + CEclmb;
+    gx -= static_cast<double>(CE * dx);
+    gy -= static_cast<double>(CE * dy);
+    gz -= static_cast<double>(CE * dz);
+    // owner-computes counting of the energy
+    bool count = false;
+    if (sidx == center) count = j > i;
+    else {
+      const long long tag_j = d.tag[j];
+      if (tag_i < tag_j) count = true;
+      else if (tag_i == tag_j) {
+        const double SMALL = 1e-4;
+        if (dvd[2] > SMALL) count = true;
+        else if (fabs(dvd[2]) < SMALL) {
+          if (dvd[1] > SMALL) count = true;
+          else if (fabs(dvd[1]) < SMALL && dvd[0] > SMALL) count = true;
+        }
+      }
+    }
+    if (count) {
+      ev += static_cast<double>(e_vdW);
+      ee += static_cast<double>(e_ele);
+      ++counted;
+    }
+  }
+  gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); ev = warp_sum(ev); ee = warp_sum(ee);
+  for (int o = 16; o > 0; o >>= 1) counted += __shfl_xor_sync(0xffffffffu, counted, o);
+  if (lane == 0) {
+    d.fnb[i] = make_double4(gx, gy, gz, 0.0);
+    d.eatom[static_cast<size_t>(i) * kTerms + E_VDW] = ev;
+    d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] = ee;
+    const double chi = ff.sb[ti * SB_N + SB_CHI], eta = ff.sb[ti * SB_N + SB_ETA], qd = d.q[i];
+    d.eatom[static_cast<size_t>(i) * kTerms + E_POL] = 23.02 * (chi * qd + (eta / 2.) * (qd * qd));
+    d.census[4 * d.na + i] = counted;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ QEq CG
+// y = (diag(eta) + H) v for one row, both right-hand sides (s, t) at once; warp per row, lane-strided entries.
+__device__ inline double2 row_mv(const Dev& d, int i, double eta, const double2* v) {
+  const int cnt = min(d.nbr_cnt[i], d.ncap);
+  const int lane = threadIdx.x & 31;
+  double ys = 0.0, yt = 0.0;
+  const size_t base = static_cast<size_t>(i) * d.ncap;
+  for (int e = lane; e < cnt; e += 32) {
+    const double h = d.hval[base + e];
+    const int j = static_cast<int>(d.nbr[base + e] & d.amask);
+    const double2 vj = v[j];
+    ys += h * vj.x;
+    yt += h * vj.y;
+  }
+  ys = warp_sum(ys);
+  yt = warp_sum(yt);
+  const double2 vi = v[i];
+  return make_double2(eta * vi.x + __shfl_sync(0xffffffffu, ys, 0), eta * vi.y + __shfl_sync(0xffffffffu, yt, 0));
+}
+
+// deterministic block sum of NV doubles per thread into out[blockIdx.x * NV + k]
+template <int NV>
+__device__ inline void block_partials(const double* v, double* out, double* sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = 0; k < NV; ++k) {
+    double x = v[k];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[wid * NV + k] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += sh[w * NV + threadIdx.x];
+    out[blockIdx.x * NV + threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+// sum of the per-block partials in block order (every block computes the same value)
+template <int NV>
+__device__ inline void grid_totals(const double* part, int nblocks, double* tot, double* sh) {
+  if (threadIdx.x < NV) {
+    double t = 0.0;
+    for (int b = 0; b < nblocks; ++b) t += part[b * NV + threadIdx.x];
+    sh[threadIdx.x] = t;
+  }
+  __syncthreads();
+  for (int k = 0; k < NV; ++k) tot[k] = sh[k];
+  __syncthreads();
+}
+
+// Persistent cooperative Jacobi-PCG for one system, s and t solved together: the stock loop of fix qeq/reaxff as
+// reproduced in plugin/adapter/fix_qeq_reaxff_metal.cpp:89-123, in FP64, each system stopping on its own test
+// sqrt(r.M^-1 r)/|b| <= tol with at most imax-1 iterations. Then calculate_Q: q = s - (sum s / sum t) t.
+// Rows are distributed over all warps of the grid; reductions are fixed-order (per-block partials summed in block
+// order), so the result is bitwise reproducible. Only grid.sync() waits; the kernel is launched cooperatively.
+__global__ void k_cg_grid(Dev d, CgArgs a) {
+  cg::grid_group g = cg::this_grid();
+  __shared__ double sh[64 * 4];
+  __shared__ double tot_sh[8];
+  const int wpb = blockDim.x >> 5;
+  const int gw = blockIdx.x * wpb + (threadIdx.x >> 5);
+  const int nwarps = gridDim.x * wpb;
+  const int lane = threadIdx.x & 31;
+  const int i0 = a.begin, n = a.n;
+  double loc[4], tot[4];
+  int phase = 0;
+  auto partbuf = [&]() { return a.part + static_cast<size_t>(phase & 1) * gridDim.x * 4; };
+  // r = b - A x ; d = M^-1 r
+  loc[0] = loc[1] = loc[2] = loc[3] = 0.0;
+  for (int r = gw; r < n; r += nwarps) {
+    const int i = i0 + r;
+    const double eta = a.eta[i];
+    const double2 y = row_mv(d, i, eta, a.x);
+    if (lane == 0) {
+      const double2 b = a.b[i];
+      const double2 rr = make_double2(b.x - y.x, b.y - y.y);
+      a.r[i] = rr;
+      const double2 dd = make_double2(rr.x / eta, rr.y / eta);
+      a.d[i] = dd;
+      loc[0] += b.x * b.x; loc[1] += b.y * b.y; loc[2] += rr.x * dd.x; loc[3] += rr.y * dd.y;
+    }
+  }
+  block_partials<4>(loc, partbuf(), sh);
+  g.sync();
+  grid_totals<4>(partbuf(), gridDim.x, tot, tot_sh);
+  ++phase;
+  const double bnorm_s = sqrt(tot[0]), bnorm_t = sqrt(tot[1]);
+  double sig_s = tot[2], sig_t = tot[3];
+  bool act_s = true, act_t = true;
+  int it_s = 1, it_t = 1;
+  int it;
+  bool breakdown = false;
+  for (it = 1; it < a.imax; ++it) {
+    act_s = act_s && (sqrt(sig_s) / bnorm_s > a.tol);
+    act_t = act_t && (sqrt(sig_t) / bnorm_t > a.tol);
+    if (!act_s && !act_t) break;
+    // q = A d ; partial d.q
+    loc[0] = loc[1] = 0.0;
+    for (int r = gw; r < n; r += nwarps) {
+      const int i = i0 + r;
+      const double2 y = row_mv(d, i, a.eta[i], a.d);
+      if (lane == 0) {
+        a.q[i] = y;
+        const double2 dd = a.d[i];
+        loc[0] += dd.x * y.x; loc[1] += dd.y * y.y;
+      }
+    }
+    block_partials<2>(loc, partbuf(), sh);
+    g.sync();
+    grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
+    ++phase;
+    const double alpha_s = act_s ? sig_s / tot[0] : 0.0;
+    const double alpha_t = act_t ? sig_t / tot[1] : 0.0;
+    if (!(isfinite(alpha_s) && isfinite(alpha_t))) { breakdown = true; break; }
+    // x += alpha d ; r -= alpha q ; p = M^-1 r ; partial r.p
+    loc[0] = loc[1] = 0.0;
+    for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+      const int i = i0 + r;
+      const double2 dd = a.d[i], qq = a.q[i];
+      double2 xx = a.x[i], rr = a.r[i];
+      xx.x += alpha_s * dd.x; xx.y += alpha_t * dd.y;
+      rr.x -= alpha_s * qq.x; rr.y -= alpha_t * qq.y;
+      a.x[i] = xx;
+      a.r[i] = rr;
+      const double eta = a.eta[i];
+      const double2 pp = make_double2(rr.x / eta, rr.y / eta);
+      a.p[i] = pp;
+      loc[0] += rr.x * pp.x; loc[1] += rr.y * pp.y;
+    }
+    block_partials<2>(loc, partbuf(), sh);
+    g.sync();
+    grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
+    ++phase;
+    const double beta_s = act_s ? tot[0] / sig_s : 0.0;
+    const double beta_t = act_t ? tot[1] / sig_t : 0.0;
+    if (act_s) { sig_s = tot[0]; it_s = it + 1; }
+    if (act_t) { sig_t = tot[1]; it_t = it + 1; }
+    // d = p + beta d (only for the systems still iterating)
+    for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+      const int i = i0 + r;
+      const double2 pp = a.p[i];
+      double2 dd = a.d[i];
+      if (act_s) dd.x = pp.x + beta_s * dd.x;
+      if (act_t) dd.y = pp.y + beta_t * dd.y;
+      a.d[i] = dd;
+    }
+    g.sync();
+  }
+  // calculate_Q: q = s - (sum s / sum t) t
+  loc[0] = loc[1] = 0.0;
+  for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+    const double2 xx = a.x[i0 + r];
+    loc[0] += xx.x; loc[1] += xx.y;
+  }
+  block_partials<2>(loc, partbuf(), sh);
+  g.sync();
+  grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
+  ++phase;
+  const double u = tot[0] / tot[1];
+  for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+    const double2 xx = a.x[i0 + r];
+    d.q[i0 + r] = xx.x - u * xx.y;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out_iters[0] = it_s;
+    a.out_iters[1] = it_t;
+    a.out_rel[0] = sqrt(sig_s) / bnorm_s;
+    a.out_rel[1] = sqrt(sig_t) / bnorm_t;
+    if (breakdown) atomicOr(d.status, ST_CG_BREAKDOWN);
+  }
+}
+
+// One block per system: the same algorithm for many small systems at once (batched systems of a few hundred to a
+// few thousand atoms). Block-level reductions in fixed order; no grid-wide waits.
+__global__ void k_cg_block(Dev d, CgBatchArgs a) {
+  const int sidx = blockIdx.x;
+  if (sidx >= d.nsys) return;
+  const SysInfo s = d.sys[sidx];
+  const int i0 = s.begin, n = s.natoms;
+  __shared__ double sh[32 * 4];
+  __shared__ double tot[4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  auto reduce = [&](double* v, int nv) {
+    for (int k = 0; k < nv; ++k) {
+      double x = v[k];
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) sh[wid * 4 + k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+      double t = 0.0;
+      for (int w = 0; w < nw; ++w) t += sh[w * 4 + threadIdx.x];
+      tot[threadIdx.x] = t;
+    }
+    __syncthreads();
+    for (int k = 0; k < nv; ++k) v[k] = tot[k];
+    __syncthreads();
+  };
+  double loc[4];
+  loc[0] = loc[1] = loc[2] = loc[3] = 0.0;
+  for (int r = wid; r < n; r += nw) {
+    const int i = i0 + r;
+    const double eta = a.eta[i];
+    const double2 y = row_mv(d, i, eta, a.x);
+    if (lane == 0) {
+      const double2 b = a.b[i];
+      const double2 rr = make_double2(b.x - y.x, b.y - y.y);
+      a.r[i] = rr;
+      const double2 dd = make_double2(rr.x / eta, rr.y / eta);
+      a.d[i] = dd;
+      loc[0] += b.x * b.x; loc[1] += b.y * b.y; loc[2] += rr.x * dd.x; loc[3] += rr.y * dd.y;
+    }
+  }
+  reduce(loc, 4);
+  const double bnorm_s = sqrt(loc[0]), bnorm_t = sqrt(loc[1]);
+  double sig_s = loc[2], sig_t = loc[3];
+  bool act_s = true, act_t = true, breakdown = false;
+  int it_s = 1, it_t = 1;
+  for (int it = 1; it < a.imax; ++it) {
+    act_s = act_s && (sqrt(sig_s) / bnorm_s > a.tol);
+    act_t = act_t && (sqrt(sig_t) / bnorm_t > a.tol);
+    if (!act_s && !act_t) break;
+    loc[0] = loc[1] = 0.0;
+    for (int r = wid; r < n; r += nw) {
+      const int i = i0 + r;
+      const double2 y = row_mv(d, i, a.eta[i], a.d);
+      if (lane == 0) {
+        a.q[i] = y;
+        const double2 dd = a.d[i];
+        loc[0] += dd.x * y.x; loc[1] += dd.y * y.y;
+      }
+    }
+    reduce(loc, 2);
+    const double alpha_s = act_s ? sig_s / loc[0] : 0.0;
+    const double alpha_t = act_t ? sig_t / loc[1] : 0.0;
+    if (!(isfinite(alpha_s) && isfinite(alpha_t))) { breakdown = true; break; }
+    loc[0] = loc[1] = 0.0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+      const int i = i0 + r;
+      const double2 dd = a.d[i], qq = a.q[i];
+      double2 xx = a.x[i], rr = a.r[i];
+      xx.x += alpha_s * dd.x; xx.y += alpha_t * dd.y;
+      rr.x -= alpha_s * qq.x; rr.y -= alpha_t * qq.y;
+      a.x[i] = xx;
+      a.r[i] = rr;
+      const double eta = a.eta[i];
+      const double2 pp = make_double2(rr.x / eta, rr.y / eta);
+      a.p[i] = pp;
+      loc[0] += rr.x * pp.x; loc[1] += rr.y * pp.y;
+    }
+    reduce(loc, 2);
+    const double beta_s = act_s ? loc[0] / sig_s : 0.0;
+    const double beta_t = act_t ? loc[1] / sig_t : 0.0;
+    if (act_s) { sig_s = loc[0]; it_s = it + 1; }
+    if (act_t) { sig_t = loc[1]; it_t = it + 1; }
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+      const int i = i0 + r;
+      const double2 pp = a.p[i];
+      double2 dd = a.d[i];
+      if (act_s) dd.x = pp.x + beta_s * dd.x;
+      if (act_t) dd.y = pp.y + beta_t * dd.y;
+      a.d[i] = dd;
+    }
+    __syncthreads();
+  }
+  loc[0] = loc[1] = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const double2 xx = a.x[i0 + r];
+    loc[0] += xx.x; loc[1] += xx.y;
+  }
+  reduce(loc, 2);
+  const double u = loc[0] / loc[1];
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const double2 xx = a.x[i0 + r];
+    d.q[i0 + r] = xx.x - u * xx.y;
+  }
+  if (threadIdx.x == 0) {
+    a.out_iters[2 * sidx] = it_s;
+    a.out_iters[2 * sidx + 1] = it_t;
+    a.out_rel[2 * sidx] = sqrt(sig_s) / bnorm_s;
+    a.out_rel[2 * sidx + 1] = sqrt(sig_t) / bnorm_t;
+    if (breakdown) atomicOr(d.status, ST_CG_BREAKDOWN);
+  }
+}
+
+// Initial guesses from the histories (Q-23: s = 4(s0+s2) - (6 s1 + s3), t = t2 + 3(t0 - t1); index 0 = latest),
+// right-hand sides b_s = -chi, b_t = -1, and the diagonal eta.
+__global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, const double* t_hist) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.na) return;
+  const int t = d.type[i];
+  const double* sh = s_hist + 4 * static_cast<size_t>(i);
+  const double* th = t_hist + 4 * static_cast<size_t>(i);
+  a.x[i] = make_double2(4 * (sh[0] + sh[2]) - (6 * sh[1] + sh[3]), th[2] + 3 * (th[0] - th[1]));
+  a.b[i] = make_double2(-ff.sb[t * SB_N + SB_CHI], -1.0);
+  a.eta[i] = ff.sb[t * SB_N + SB_ETA];
+}
+
+__global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.na) return;
+  double* sh = s_hist + 4 * static_cast<size_t>(i);
+  double* th = t_hist + 4 * static_cast<size_t>(i);
+  for (int k = 3; k > 0; --k) { sh[k] = sh[k - 1]; th[k] = th[k - 1]; }
+  sh[0] = x[i].x;
+  th[0] = x[i].y;
+}
+
+// y = (diag(eta) + H) v, owned rows (mtl::Context::qeq_matvec)
+__global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (warp >= d.na) return;
+  const double eta = ff.sb[d.type[warp] * SB_N + SB_ETA];
+  const double2 r = row_mv(d, warp, eta, v);
+  if ((threadIdx.x & 31) == 0) y[warp] = r;
+}
+
+// ------------------------------------------------------------------------------------------------ energy sums
+// Per system, per term: fixed-order sum over the system's atoms (one block per system).
+__global__ void k_energy_sum(Dev d, double* out) {
+  const int sidx = blockIdx.x;
+  const SysInfo s = d.sys[sidx];
+  __shared__ double sh[256];
+  for (int t = 0; t < kTerms; ++t) {
+    double v = 0.0;
+    for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) v += d.eatom[static_cast<size_t>(s.begin + r) * kTerms + t];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[sidx * kTerms + t] = sh[0];
+    __syncthreads();
+  }
+}
+
+}  // namespace rx

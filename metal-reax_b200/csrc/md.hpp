@@ -1,0 +1,26 @@
+// Device state and kernels of the NVT integrator (md_kernels.cu).
+#pragma once
+#include "device.cuh"
+
+namespace rx {
+
+constexpr int kMaxChain = 8;
+
+struct MdDev {
+  double4* v;        // velocities (A/fs)
+  const double* mass;  // per force-field type (g/mol)
+  double* ke;        // per system (kcal/mol)
+  double* temp;      // per system (K)
+  double* scale;     // per system velocity scale of the last chain half-step
+  double* xi;        // nsys * kMaxChain chain positions
+  double* vxi;       // nsys * kMaxChain chain velocities
+  double dt, t_start, t_stop, t_damp;
+  int chain;
+};
+
+__global__ void k_md_kinetic(MdDev m, const SysInfo* sys, const int* type);
+__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys, double step_frac);
+__global__ void k_md_scale(MdDev m, const int* sys_of, int na);
+__global__ void k_md_kick(MdDev m, const int* type, const double4* grad, double4* x, int na, int drift);
+
+}  // namespace rx

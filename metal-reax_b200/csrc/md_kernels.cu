@@ -1,0 +1,101 @@
+// Velocity Verlet with a Nose-Hoover chain thermostat (NVT), per system.
+//
+// The reference leaves time integration to LAMMPS (`fix nvt temp Tstart Tstop Tdamp`). This is the
+// Martyna-Tuckerman-Klein chain (Mol. Phys. 87, 1117 (1996)) applied for dt/2 before the first velocity half-kick
+// and after the second, with chain masses Q_1 = Nf kT tau^2 and Q_k = kT tau^2 (tau = Tdamp), Nf = 3N - 3.
+// Units LAMMPS `real`: v in A/fs, forces kcal/mol/A, masses g/mol.
+#include "device.cuh"
+#include "md.hpp"
+
+namespace rx {
+
+namespace {
+constexpr double kFtm2v = 1.0 / 48.88821291 / 48.88821291;   // (kcal/mol/A)/(g/mol) -> A/fs^2
+constexpr double kMvv2e = 48.88821291 * 48.88821291;         // (g/mol) A^2/fs^2 -> kcal/mol
+constexpr double kBoltz = 0.0019872067;                      // kcal/mol/K
+}  // namespace
+
+// kinetic energy (kcal/mol) of every system, fixed-order block sums (one block per system)
+__global__ void k_md_kinetic(MdDev m, const SysInfo* sys, const int* type) {
+  const SysInfo s = sys[blockIdx.x];
+  __shared__ double sh[256];
+  double v2 = 0.0;
+  for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) {
+    const int a = s.begin + r;
+    const double4 v = m.v[a];
+    v2 += m.mass[type[a]] * (v.x * v.x + v.y * v.y + v.z * v.z);
+  }
+  sh[threadIdx.x] = v2;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) m.ke[blockIdx.x] = 0.5 * kMvv2e * sh[0];
+}
+
+// one thread per system: advance the chain by dt/2 and produce the velocity scale factor
+__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys, double step_frac) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  const int M = m.chain;
+  double* xi = m.xi + s * kMaxChain;
+  double* vx = m.vxi + s * kMaxChain;
+  const double T = m.t_start + step_frac * (m.t_stop - m.t_start);
+  const double kT = kBoltz * T;
+  const double nf = 3.0 * sys[s].natoms - 3.0;
+  const double tau2 = m.t_damp * m.t_damp;
+  double Q[kMaxChain];
+  Q[0] = nf * kT * tau2;
+  for (int k = 1; k < M; ++k) Q[k] = kT * tau2;
+  const double dt = m.dt, dt2 = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
+  double ke2 = 2.0 * m.ke[s];
+  auto G = [&](int k) { return k == 0 ? (ke2 - nf * kT) / Q[0] : (Q[k - 1] * vx[k - 1] * vx[k - 1] - kT) / Q[k]; };
+  vx[M - 1] += G(M - 1) * dt4;
+  for (int k = M - 2; k >= 0; --k) {
+    const double e = exp(-vx[k + 1] * dt8);
+    vx[k] *= e;
+    vx[k] += G(k) * dt4;
+    vx[k] *= e;
+  }
+  const double scale = exp(-vx[0] * dt2);
+  ke2 *= scale * scale;
+  for (int k = 0; k < M; ++k) xi[k] += vx[k] * dt2;
+  for (int k = 0; k < M - 1; ++k) {
+    const double e = exp(-vx[k + 1] * dt8);
+    vx[k] *= e;
+    vx[k] += G(k) * dt4;
+    vx[k] *= e;
+  }
+  vx[M - 1] += G(M - 1) * dt4;
+  m.scale[s] = scale;
+  m.ke[s] = 0.5 * ke2;
+  m.temp[s] = ke2 / (nf * kBoltz);
+}
+
+__global__ void k_md_scale(MdDev m, const int* sys_of, int na) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= na) return;
+  const double sc = m.scale[sys_of[a]];
+  double4 v = m.v[a];
+  v.x *= sc; v.y *= sc; v.z *= sc;
+  m.v[a] = v;
+}
+
+// v += dt/2 * F/m (F = -grad); with drift: x += dt * v
+__global__ void k_md_kick(MdDev m, const int* type, const double4* grad, double4* x, int na, int drift) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= na) return;
+  const double c = 0.5 * m.dt * kFtm2v / m.mass[type[a]];
+  const double4 g = grad[a];
+  double4 v = m.v[a];
+  v.x -= c * g.x; v.y -= c * g.y; v.z -= c * g.z;
+  m.v[a] = v;
+  if (drift) {
+    double4 p = x[a];
+    p.x += m.dt * v.x; p.y += m.dt * v.y; p.z += m.dt * v.z;
+    x[a] = p;
+  }
+}
+
+}  // namespace rx

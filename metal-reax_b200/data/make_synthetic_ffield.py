@@ -66,11 +66,11 @@ GENERAL = [
 # per element: four lines of values (after the symbol on the first line)
 ATOMS = [
     ("C", [1.38, 4.0, 12.0000, 1.95, 0.085, 0.90, 1.24, 4.0],
-          [9.8, 2.2, 4.0, 33.0, 0.0, 5.9, 3.6, 0.0],
+          [9.8, 2.2, 4.0, 33.0, 0.0, 5.9, 7.0, 0.0],
           [1.20, 0.0, 13.0, 30.0, 2.0, 8.0, 0.0, 0.0],
           [-4.0, 2.0, 1.0, 4.0, 2.9, 1.85, 0.05, 10.0]),
     ("H", [0.86, 1.0, 1.0080, 1.40, 0.090, 0.82, -0.10, 1.0],
-          [9.4, 5.0, 1.0, 0.0, 0.0, 3.7, 4.8, 1.0],
+          [9.4, 5.0, 1.0, 0.0, 0.0, 3.7, 9.6, 1.0],
           [-0.10, 0.0, 1.0, 3.0, 1.0, 4.0, 0.0, 0.0],
           [-15.0, 2.0, 1.0, 1.0, 2.9, 1.30, 0.02, 8.0]),
     ("O", [1.24, 2.0, 15.9990, 2.35, 0.100, 1.08, 1.05, 6.0],

@@ -1,0 +1,228 @@
+"""Python front end of librxcuda.so, the C ABI of the B200 ReaxFF engine (include/rxcuda.h).
+
+Mirrors the reference's plugin surface for the hot path:
+  ``Engine.set_forcefield``   pair_coeff * * ffield ... (parse_force_field, src/io/ffield_parser.cpp:91)
+  ``Engine.set_control``      ControlParams / pair_style keywords (bond_cut, hbond_cut, thb_cut, thb_cutsq, enobonds)
+  ``Engine.set_qeq``          fix qeq/reaxff/metal <nevery> <swa> <swb> <tol> reaxff maxiter <imax> [strict]
+  ``Engine.compute``          PairReaxFFMetal::compute (plugin/adapter/pair_reaxff_metal.cpp:412-524)
+  ``Engine.qeq_solve``        FixQEqReaxFFMetal resident CG (plugin/adapter/fix_qeq_reaxff_metal.cpp:65-124)
+  ``Engine.qeq_matvec``       FixQEqReaxFFMetal::sparse_matvec (:190-205)
+  ``Engine.md_*``             an NVT driver (the reference delegates integration to LAMMPS `fix nvt`)
+
+Errors are raised as ``RxError`` with the status code and the engine's message, as the reference's adapter turns
+engine exceptions into LAMMPS errors. There is no CPU fallback: without the built library or without a GPU every
+device call fails.
+"""
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "librxcuda.so"
+TERMS = ["bond", "over", "under", "lone_pair", "valence", "penalty", "coalition", "hbond", "torsion", "conjugation", "vdw",
+         "coulomb", "polarization"]
+CENSUS = ["bonds", "angle_sets", "torsions", "hbonds", "nonbonded", "sbo_region", "lp_trunc"]
+RX_COMPUTE_QEQ = 1
+RX_COMPUTE_CENSUS = 2
+STATUS = {0: "ok", 1: "invalid", 2: "ffield", 3: "capacity", 4: "cuda", 5: "not_converged", 6: "state", 7: "timeout"}
+EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_forcefield_dump", "rx_forcefield_params",
+           "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
+           "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
+           "rx_get_velocities", "rx_md_run", "rx_stream", "rx_set_timing", "rx_phase_times"]
+
+_V = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+_lib = None
+
+
+class RxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%s): %s" % (STATUS.get(code, code), code, msg))
+        self.code = code
+
+
+def load():
+    """Load librxcuda.so (built by metal-reax_b200/build.py). Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError("librxcuda.so is not built (%s); run metal-reax_b200/build.py" % LIB_PATH)
+    lib = ctypes.CDLL(str(LIB_PATH))
+    sig = {
+        "rx_create": (_V, [_I]), "rx_destroy": (None, [_V]), "rx_last_error": (ctypes.c_char_p, [_V]),
+        "rx_set_forcefield": (_I, [_V, ctypes.c_char_p, _I]),
+        "rx_forcefield_dump": (ctypes.c_long, [_V, _I, ctypes.c_char_p, ctypes.c_long]),
+        "rx_forcefield_params": (_I, [_V, _V, _V, _V, _V, _V]),
+        "rx_set_control": (_I, [_V, _D, _D, _D, _D, _I]),
+        "rx_set_systems": (_I, [_V, _I, _V, _V, _V, _V, _V, _V]), "rx_num_atoms": (_I, [_V]),
+        "rx_set_positions": (_I, [_V, _V]), "rx_get_positions": (_I, [_V, _V]),
+        "rx_set_charges": (_I, [_V, _V]), "rx_get_charges": (_I, [_V, _V]),
+        "rx_set_qeq": (_I, [_V, _D, _D, _D, _I, _I]), "rx_qeq_solve": (_I, [_V, _V, _V]), "rx_qeq_matvec": (_I, [_V, _V, _V]),
+        "rx_compute": (_I, [_V, _I, _V, _V, _V, _V]),
+        "rx_md_setup": (_I, [_V, _V, _D, _D, _D, _D, _I]), "rx_set_velocities": (_I, [_V, _V]),
+        "rx_get_velocities": (_I, [_V, _V]), "rx_md_run": (_I, [_V, _I, _V, _V]),
+        "rx_stream": (_V, [_V]), "rx_set_timing": (_I, [_V, _I]),
+        "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class Engine:
+    """One engine context: a force field and one or more independent periodic systems (a batch)."""
+
+    def __init__(self, device=0):
+        self.lib = load()
+        self.h = self.lib.rx_create(device)
+        if not self.h:
+            raise RxError(4, self.lib.rx_last_error(None).decode())
+        self.nsys = 0
+        self.natoms = None
+        self.na = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RxError(rc, self.lib.rx_last_error(self.h).decode())
+
+    # ---- configuration
+    def set_forcefield(self, text, lgvdw=False):
+        self._check(self.lib.rx_set_forcefield(self.h, text.encode(), 1 if lgvdw else 0))
+
+    def forcefield_dump(self, portable=False):
+        n = self.lib.rx_forcefield_dump(self.h, 1 if portable else 0, None, 0)
+        if n < 0:
+            raise RxError(6, self.lib.rx_last_error(self.h).decode())
+        buf = ctypes.create_string_buffer(n + 1)
+        self.lib.rx_forcefield_dump(self.h, 1 if portable else 0, buf, n + 1)
+        return buf.value.decode()
+
+    def forcefield_params(self):
+        nt = ctypes.c_int(0)
+        self._check(self.lib.rx_forcefield_params(self.h, ctypes.addressof(nt), None, None, None, None))
+        chi, eta, gamma, mass = (np.zeros(nt.value) for _ in range(4))
+        self._check(self.lib.rx_forcefield_params(self.h, ctypes.addressof(nt), _p(chi), _p(eta), _p(gamma), _p(mass)))
+        return {"chi": chi, "eta": eta, "gamma": gamma, "mass": mass}
+
+    def set_control(self, bond_cut=5.0, hbond_cut=7.5, thb_cut=0.001, thb_cutsq=0.00001, enobonds=True):
+        self._check(self.lib.rx_set_control(self.h, bond_cut, hbond_cut, thb_cut, thb_cutsq, 1 if enobonds else 0))
+
+    def set_qeq(self, swa=0.0, swb=10.0, tol=1e-6, imax=200, strict=False):
+        self._check(self.lib.rx_set_qeq(self.h, swa, swb, tol, imax, 1 if strict else 0))
+
+    def set_systems(self, systems):
+        """systems: list of dicts (origin, box, periodic, x, type, tag) as produced by systems.py."""
+        natoms = np.array([len(s["type"]) for s in systems], dtype=np.int32)
+        origin = np.ascontiguousarray(np.concatenate([np.asarray(s["origin"], dtype=np.float64) for s in systems]))
+        box = np.ascontiguousarray(np.concatenate([np.asarray(s["box"], dtype=np.float64).reshape(9) for s in systems]))
+        per = np.ascontiguousarray(np.concatenate([np.asarray(s["periodic"], dtype=np.int32) for s in systems]))
+        ty = np.ascontiguousarray(np.concatenate([np.asarray(s["type"], dtype=np.int32) for s in systems]))
+        tg = np.ascontiguousarray(np.concatenate([np.asarray(s["tag"], dtype=np.int64) for s in systems]))
+        self._check(self.lib.rx_set_systems(self.h, len(systems), _p(natoms), _p(origin), _p(box), _p(per), _p(ty), _p(tg)))
+        self.nsys = len(systems)
+        self.natoms = natoms
+        self.na = int(natoms.sum())
+        self.offsets = np.concatenate([[0], np.cumsum(natoms)])
+        x = np.ascontiguousarray(np.concatenate([np.asarray(s["x"], dtype=np.float64).reshape(-1, 3) for s in systems]))
+        self.set_positions(x)
+
+    def set_positions(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        if x.size != 3 * self.na:
+            raise ValueError("need 3 coordinates per atom")
+        self._check(self.lib.rx_set_positions(self.h, _p(x)))
+
+    def get_positions(self):
+        x = np.zeros(3 * self.na)
+        self._check(self.lib.rx_get_positions(self.h, _p(x)))
+        return x.reshape(-1, 3)
+
+    def set_charges(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        self._check(self.lib.rx_set_charges(self.h, _p(q)))
+
+    def get_charges(self):
+        q = np.zeros(self.na)
+        self._check(self.lib.rx_get_charges(self.h, _p(q)))
+        return q
+
+    # ---- evaluation
+    def compute(self, qeq=False, census=False, counts=False):
+        e = np.zeros(13 * self.nsys)
+        g = np.zeros(3 * self.na)
+        cen = np.zeros(7 * self.na, dtype=np.int32) if census else None
+        cnt = np.zeros(4, dtype=np.int64) if counts else None
+        flags = (RX_COMPUTE_QEQ if qeq else 0) | (RX_COMPUTE_CENSUS if census else 0)
+        self._check(self.lib.rx_compute(self.h, flags, _p(e), _p(g), _p(cen), _p(cnt)))
+        out = {"e": e.reshape(self.nsys, 13), "grad": g.reshape(-1, 3)}
+        if census:
+            out["census"] = cen.reshape(7, self.na)
+        if counts:
+            out["counts"] = cnt
+        return out
+
+    def qeq_solve(self):
+        it = np.zeros(2 * self.nsys, dtype=np.int32)
+        rel = np.zeros(2 * self.nsys)
+        self._check(self.lib.rx_qeq_solve(self.h, _p(it), _p(rel)))
+        return {"q": self.get_charges(), "iters": it.reshape(-1, 2), "rel": rel.reshape(-1, 2)}
+
+    def qeq_matvec(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        y = np.zeros(self.na)
+        self._check(self.lib.rx_qeq_matvec(self.h, _p(v), _p(y)))
+        return y
+
+    # ---- dynamics
+    def md_setup(self, mass_per_type, dt=0.25, t_start=300.0, t_stop=None, t_damp=25.0, chain=3):
+        m = np.ascontiguousarray(mass_per_type, dtype=np.float64)
+        self._check(self.lib.rx_md_setup(self.h, _p(m), dt, t_start, t_start if t_stop is None else t_stop, t_damp, chain))
+
+    def set_velocities(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        self._check(self.lib.rx_set_velocities(self.h, _p(v)))
+
+    def get_velocities(self):
+        v = np.zeros(3 * self.na)
+        self._check(self.lib.rx_get_velocities(self.h, _p(v)))
+        return v.reshape(-1, 3)
+
+    def md_run(self, nsteps):
+        e = np.zeros(13 * self.nsys)
+        t = np.zeros(self.nsys)
+        self._check(self.lib.rx_md_run(self.h, nsteps, _p(e), _p(t)))
+        return {"e": e.reshape(self.nsys, 13), "T": t}
+
+    def stream(self):
+        return self.lib.rx_stream(self.h)
+
+    def set_timing(self, on=True):
+        self._check(self.lib.rx_set_timing(self.h, 1 if on else 0))
+
+    def phase_times(self):
+        buf = ctypes.create_string_buffer(4096)
+        ms = np.zeros(32)
+        n = self.lib.rx_phase_times(self.h, buf, 4096, _p(ms), 32)
+        names = buf.value.decode().split("\n")[:n]
+        return dict(zip(names, ms[:n]))

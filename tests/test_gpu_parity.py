@@ -1,0 +1,130 @@
+"""GPU parity: the CUDA engine (through its C ABI) against the CPU oracle (the C restatement of the reference's cpu64
+engine, pinned against the reference itself in test_oracle.py).
+
+Bars (the reference's own acceptance of an FP32 GPU engine against cpu64, tolerances/tolerances.json "C3"):
+  energy  |dE_total| / N <= 1e-3 kcal/mol/atom
+  force   max |dF| <= 0.05, RMS <= 5e-3 kcal/mol/A
+  census  every discrete decision (bonds, angle sets, torsions, H-bonds, non-bonded pairs, SBO branch, lone-pair
+          truncation) identical atom by atom
+Tighter bars for the FP64 bond-order terms: every bonded term within 1e-7 relative (max(1, |E|)).
+"""
+import numpy as np
+import pytest
+
+from helpers import (C3_ENERGY_PER_ATOM, C3_FORCE_MAX, C3_FORCE_RMS, fixed_charges, ffield_text, force_metrics,
+                     small_systems)
+
+pytestmark = pytest.mark.gpu
+
+BONDED = slice(0, 10)
+
+
+@pytest.fixture(scope="module")
+def oracle():
+    from oracle.oracle import COracle
+    return COracle(ffield_text(), shell=15.0)
+
+
+@pytest.fixture(scope="module")
+def engine():
+    import rxcuda
+    e = rxcuda.Engine(0)
+    e.set_forcefield(ffield_text())
+    e.set_control()
+    yield e
+    e.close()
+
+
+@pytest.mark.parametrize("idx", range(5))
+def test_single_point_matches_oracle(engine, oracle, idx):
+    s = small_systems()[idx]
+    q = fixed_charges(s)
+    ref = oracle.single_point(s, q)
+    engine.set_systems([s])
+    engine.set_charges(q)
+    out = engine.compute(census=True, counts=True)
+    e, e_ref = out["e"][0], ref["e"]
+    n = len(s["type"])
+    # FP64 bond-order terms: tight
+    rel = np.abs(e[BONDED] - e_ref[BONDED]) / np.maximum(1.0, np.abs(e_ref[BONDED]))
+    assert rel.max() <= 1e-7, (s["name"], e[BONDED], e_ref[BONDED])
+    # total energy per atom (C3)
+    assert abs(e.sum() - e_ref.sum()) / n <= C3_ENERGY_PER_ATOM, (s["name"], e, e_ref)
+    fmax, frms = force_metrics(ref["grad"], out["grad"])
+    assert fmax <= C3_FORCE_MAX and frms <= C3_FORCE_RMS, (s["name"], fmax, frms)
+    # every discrete decision identical
+    for k, name in enumerate(["bonds", "angle_sets", "torsions", "hbonds", "nonbonded", "sbo_region", "lp_trunc"]):
+        assert np.array_equal(out["census"][k], ref["census"][k]), (s["name"], name)
+
+
+def test_bonded_gradient_tight(engine, oracle):
+    """Without charges the gradient is the FP64 bonded chain alone plus FP32 van der Waals: compare tightly."""
+    s = small_systems()[1]
+    q = np.zeros(len(s["type"]))
+    ref = oracle.single_point(s, q)
+    engine.set_systems([s])
+    engine.set_charges(q)
+    out = engine.compute()
+    fmax, frms = force_metrics(ref["grad"], out["grad"])
+    assert fmax <= 5e-3 and frms <= 1e-3, (fmax, frms)
+
+
+def test_bitwise_rerun(engine):
+    """FORCE-2 of the reference (tests/python/test_gpu_fixtures.py:58): two runs give identical bits."""
+    s = small_systems()[0]
+    engine.set_systems([s])
+    engine.set_charges(fixed_charges(s))
+    a = engine.compute()
+    engine.set_systems([s])
+    engine.set_charges(fixed_charges(s))
+    b = engine.compute()
+    assert np.array_equal(a["e"], b["e"]) and np.array_equal(a["grad"], b["grad"])
+
+
+def test_qeq_charges_match_oracle(engine, oracle):
+    s = small_systems()[0]
+    engine.set_systems([s])
+    engine.set_qeq(0.0, 10.0, 1e-12, 400)
+    got = engine.qeq_solve()
+    ref = oracle.qeq(s, tol=1e-12, imax=400)
+    assert np.abs(got["q"] - ref["q"]).max() <= 1e-10
+    assert abs(got["q"].sum()) <= 1e-9
+    engine.set_qeq()
+
+
+def test_qeq_tol_1e6_within_c3(engine, oracle):
+    s = small_systems()[0]
+    engine.set_systems([s])
+    engine.set_qeq(0.0, 10.0, 1e-6, 200)
+    got = engine.qeq_solve()
+    ref = oracle.qeq(s, tol=1e-6, imax=200)
+    assert np.abs(got["q"] - ref["q"]).max() <= 1e-4
+    assert tuple(got["iters"][0]) == tuple(ref["iters"])
+
+
+def test_qeq_matvec_matches_oracle(engine, oracle):
+    s = small_systems()[2]
+    engine.set_systems([s])
+    v = np.random.default_rng(5).normal(size=len(s["type"]))
+    y = engine.qeq_matvec(v)
+    y_ref = oracle.qeq_matvec(s, v)
+    assert np.abs(y - y_ref).max() <= 1e-10 * max(1.0, np.abs(y_ref).max())
+
+
+def test_batch_equals_alone(engine):
+    """Each system's result is the same alone and inside a batch (per-system reductions in fixed order)."""
+    ss = small_systems()[1:4]
+    alone = []
+    for s in ss:
+        engine.set_systems([s])
+        engine.set_charges(fixed_charges(s))
+        alone.append(engine.compute())
+    engine.set_systems(ss)
+    engine.set_charges(np.concatenate([fixed_charges(s) for s in ss]))
+    both = engine.compute()
+    off = 0
+    for k, s in enumerate(ss):
+        n = len(s["type"])
+        assert np.array_equal(both["e"][k], alone[k]["e"][0])
+        assert np.array_equal(both["grad"][off:off + n], alone[k]["grad"])
+        off += n
