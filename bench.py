@@ -1,0 +1,372 @@
+#!/usr/bin/env python3
+"""Benchmark of the ReaxFF force + charge-equilibration step on B200 (one JSON line on rank 0).
+
+Workload (the single-GPU configuration the headline metric is quoted on): 8000 H2O = 24,000 atoms in a 62.07 A
+periodic box (lattice of molecules, +-0.3 A jitter, random orientations, O-H 0.96 A, 104.5 deg), synthetic CHO
+force field (metal-reax_b200/data/ffield.synthetic.cho), NVT at 300 K, dt 0.25 fs, Tdamp 25 fs, chain 3, charge
+equilibration every step (taper 0-10 A, tol 1e-6, maxiter 200). One step = QEq + energy/forces + velocity Verlet.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+value: atom-steps/s of the whole job with the state resident in HBM (device-timed with CUDA events on the engine's
+stream, max over ranks). e2e: the same metric through the C ABI with host buffers (positions in, gradient and
+energies out every step, integration on the host, as the LAMMPS plugin drives the engine). N > 1: N independent
+replicas (one per GPU, no collective on the data path; the single-system step does not shard).
+--impl reference: the reference's own CPU engine (oracle/_ref, cpu64) plus the C restatement of the stock QEq CG on
+the host, same workload and metric.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+PKG = REPO / "metal-reax_b200"
+for p in (str(REPO), str(PKG)):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import systems  # noqa: E402
+
+METRIC = "atom-steps/s"
+UNIT = "atom-steps/s"
+WORKLOAD = "water24k_nvt_qeq"
+DT, TEMP, TDAMP, CHAIN = 0.25, 300.0, 25.0, 3
+QEQ = dict(swa=0.0, swb=10.0, tol=1e-6, imax=200)
+MASS = [12.0, 1.008, 15.999]
+KTERMS = 13
+
+
+def ffield_text():
+    return (PKG / "data" / "ffield.synthetic.cho").read_text()
+
+
+def workload(n_side=20):
+    s = systems.water_box(n_side)
+    v = systems.maxwell_velocities(s, TEMP, seed=20261203)
+    return s, v
+
+
+# ---------------------------------------------------------------------------------------------------- clocks
+class Clocks:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = Path("/tmp/rx_clocks_%d_%d.csv" % (os.getpid(), device))
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "200",
+                                          "-i", str(self.device)], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if parts[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------------- byte model
+def bytes_model(N, P, D, I, R):
+    """Algorithmic HBM bytes of one MD step: 128 N + 8 P + P (4 + 8 I) + 12 P R + 256 D (P = counted half pairs within
+    the non-bonded cut-off, D = directed bonds, I = fused s/t CG iterations, R = FP64 residual refinements)."""
+    return 128 * N + 8 * P + P * (4 + 8 * I) + 12 * P * R + 256 * D
+
+
+def phase_bytes(name, N, P, D, I, R):
+    """Algorithmic bytes of one launch of each timed phase, taken term by term from the step model."""
+    return {
+        "neighbors": 8 * P + 4 * P + 32 * N,       # pair list written + read once, H written once (FP32), positions
+        "qeq": P * 8 * I + 12 * P * R,              # H value + index per fused s/t iteration, FP64 refinement
+        "bond_orders": 128 * D,
+        "bonded_terms": 64 * D,
+        "torsion": 32 * D,
+        "nonbonded": 8 * P + 32 * N,                # list + positions/charges
+        "gather": 32 * D + 32 * N,
+    }.get(name, 0)
+
+
+def measured_peak():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            v = json.loads(p.read_text()).get("hbm_gbs")
+            if v:
+                return float(v), "measured"
+        except (ValueError, OSError):
+            pass
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------------------------------- engine arm
+def make_engine(device, s, v):
+    import rxcuda
+    e = rxcuda.Engine(device)
+    e.set_forcefield(ffield_text())
+    e.set_control()
+    e.set_qeq(QEQ["swa"], QEQ["swb"], QEQ["tol"], QEQ["imax"])
+    e.set_systems([s])
+    e.md_setup(MASS, dt=DT, t_start=TEMP, t_damp=TDAMP, chain=CHAIN)
+    e.set_velocities(v)
+    return e
+
+
+def cpu_baseline_sample(seconds=15.0):
+    """The reference's own cpu64 engine (oracle/_ref) + the C restatement of the stock QEq, one core, on 648-atom
+    water single points repeated for about `seconds`."""
+    from oracle.oracle import COracle, RefOracle
+    text = ffield_text()
+    s = systems.water_box(6)
+    n = len(s["type"])
+    co = COracle(text, shell=12.0)
+    kind = "reference" if RefOracle.available() else "port"
+    ref = RefOracle(text, shell=12.0) if kind == "reference" else co
+    count = 0
+    t0 = time.perf_counter()
+    while True:
+        qr = co.qeq(s, tol=QEQ["tol"], imax=QEQ["imax"])
+        ref.single_point(s, qr["q"])
+        count += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n * count / dt, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": "%d x (QEq + energy/forces) of 216 H2O (648 atoms), %.1f s, %s" % (count, dt,
+                      "reference cpu64 engine + C restatement of the stock QEq CG" if kind == "reference" else "C restatement")}
+
+
+def e2e_run(device, s, v, steps, warmup):
+    """Plugin-style loop through the C ABI: positions from host memory in, gradient + energies out, host integration."""
+    import torch
+    import rxcuda
+    e = rxcuda.Engine(device)
+    e.set_forcefield(ffield_text())
+    e.set_control()
+    e.set_qeq(QEQ["swa"], QEQ["swb"], QEQ["tol"], QEQ["imax"])
+    e.set_systems([s])
+    n = len(s["type"])
+    m = np.asarray(MASS)[s["type"]][:, None]
+    ftm2v = 1.0 / 48.88821291 / 48.88821291
+    x = np.ascontiguousarray(s["x"], dtype=np.float64).copy()
+    vel = v.copy()
+    stream = torch.cuda.ExternalStream(e.stream(), device=torch.device("cuda", device))
+    out = e.compute(qeq=True)
+    g = out["grad"]
+
+    def step():
+        nonlocal x, vel, g
+        vel -= 0.5 * DT * ftm2v * g / m
+        x += DT * vel
+        e.set_positions(x)
+        r = e.compute(qeq=True)
+        g = r["grad"]
+        vel -= 0.5 * DT * ftm2v * g / m
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize(device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        step()
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    e.close()
+    # the engine stages positions and gradients through pinned host buffers, 32 B per atom each way
+    return n * steps / (ms * 1e-3), {"h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": 32 * n + 8 * KTERMS}
+
+
+def run_engine(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+    s, v = workload()
+    n = len(s["type"])
+    eng = make_engine(local_rank, s, v)
+    stream = torch.cuda.ExternalStream(eng.stream(), device=torch.device("cuda", local_rank))
+    eng.md_run(max(args.warmup, 3))
+    clocks = Clocks(local_rank) if rank == 0 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(local_rank)
+    if clocks:
+        clocks.start()
+    launches0 = eng.kernel_launches()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    eng.md_run(args.steps)
+    b.record(stream)
+    b.synchronize()
+    torch.cuda.synchronize(local_rank)
+    launches = eng.kernel_launches() - launches0
+    ck = clocks.stop() if clocks else None
+    ms = a.elapsed_time(b)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * n * args.steps / (ms * 1e-3)
+
+    # per-phase device times (a separate short run with phase events on), sizes for the byte model
+    eng.set_timing(True)
+    prof_steps = 3
+    eng.md_run(prof_steps)
+    phases = {k: v_ / prof_steps for k, v_ in eng.phase_times().items()}
+    eng.set_timing(False)
+    out = eng.compute(qeq=True, counts=True)
+    qr = eng.qeq_solve()
+    P = int(out["counts"][1])
+    D = int(out["counts"][0]) * 2
+    I = int(qr["iters"].max())
+    R = 0
+    peak, peak_kind = measured_peak()
+    dom = max(phases, key=phases.get) if phases else "qeq"
+    dom_bytes = phase_bytes(dom, n, P, D, I, R)
+    achieved = dom_bytes / (phases[dom] * 1e-3) / 1e9 if phases.get(dom) else None
+    step_bytes = bytes_model(n, P, D, I, R)
+    step_achieved = step_bytes / (ms_step * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+        "data": "synthetic (seeded water box, synthetic CHO force field)",
+        "config": {"workload": WORKLOAD, "atoms_per_gpu": n, "systems_per_gpu": 1, "qeq_tol": QEQ["tol"], "dt_fs": DT,
+                   "T_K": TEMP, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "per-step working set larger than L2 (neighbor rows + charge matrix ~160 MB)"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None, "peak_kind": peak_kind,
+                     "phase_ms_per_step": phases},
+        "step_roofline": {"bytes_alg": step_bytes, "achieved": step_achieved, "peak": peak, "unit": "GB/s",
+                          "frac": step_achieved / peak, "N": n, "P": P, "D": D, "I": I, "R": R},
+        "clocks": ck,
+    }
+    eng.close()
+    if world == 1 and rank == 0:
+        e2e_value, e2e_bytes = e2e_run(local_rank, s, v, max(2, args.steps // 2), 2)
+        line["e2e"] = {"value": e2e_value, "unit": UNIT, **e2e_bytes}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_sample(args.cpu_seconds)
+    elif rank == 0:
+        line["e2e"] = None
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------------- reference arm
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from oracle.oracle import COracle, RefOracle
+    text = ffield_text()
+    s, v = workload()
+    n = len(s["type"])
+    co = COracle(text, shell=12.0)
+    kind = "reference" if RefOracle.available() else "port"
+    ref = RefOracle(text, shell=12.0) if kind == "reference" else co
+    m = np.asarray(MASS)[s["type"]][:, None]
+    ftm2v = 1.0 / 48.88821291 / 48.88821291
+    x = s["x"].copy()
+    vel = v.copy()
+    sq, tq = np.zeros(n), np.zeros(n)
+
+    def forces(xx):
+        nonlocal sq, tq
+        sys_ = dict(s, x=xx)
+        qr = co.qeq(sys_, tol=QEQ["tol"], imax=QEQ["imax"], s0=sq, t0=tq)
+        sq, tq = qr["s"], qr["t"]
+        return ref.single_point(sys_, qr["q"])["grad"]
+
+    g = forces(x)
+
+    def step():
+        nonlocal x, vel, g
+        vel -= 0.5 * DT * ftm2v * g / m
+        x = x + DT * vel
+        g = forces(x)
+        vel -= 0.5 * DT * ftm2v * g / m
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = n * args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water box, synthetic CHO force field)",
+            "config": {"workload": WORKLOAD, "atoms_per_gpu": n, "systems_per_gpu": 1, "qeq_tol": QEQ["tol"], "dt_fs": DT,
+                       "T_K": TEMP},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
+                             "sample": "full 24,000-atom steps (QEq + energy/forces + host velocity Verlet); the cpu64 engine is "
+                                       "single-threaded by design"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_engine(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

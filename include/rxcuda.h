@@ -95,6 +95,9 @@ int rx_get_velocities(rx_context* ctx, double* v);
 /* nsteps steps of every system; energies (13*nsys, last step) and temperature (nsys) may be NULL */
 int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature);
 
+/* Number of this engine's own kernels launched on the context so far (library kernels, e.g. the radix sort of the cell
+ * lists, are not counted). */
+int64_t rx_kernel_launches(const rx_context* ctx);
 /* The CUDA stream the context launches on (a cudaStream_t), for callers that time or order work around it. */
 void* rx_stream(rx_context* ctx);
 /* Per-phase device time of the last rx_compute / rx_md_run (milliseconds, summed over the call) when timing is on:

@@ -29,6 +29,7 @@ enum Status : int {
   ST_SHIFT_RANGE = 8,
   ST_CG_BREAKDOWN = 16,
   ST_NONFINITE = 32,
+  ST_NEAR_OVERFLOW = 64,
 };
 
 struct SysInfo {
@@ -39,6 +40,7 @@ struct SysInfo {
   int nc[3];      // cells per lattice direction
   int cell_begin;
   int range[3];   // cell search range per direction
+  int shift_base; // first entry of this system's lattice-shift table (S^3 entries)
 };
 
 struct DevFF {
@@ -53,6 +55,8 @@ struct DevFF {
   const double* fb;
   const int* hb_on;
   const double* hb;
+  const double* shld;    // nt x nt: (gamma_i gamma_j)^-1.5, the charge-matrix shielding
+  const float* nbf;      // nt x nt x 12: single-precision pair parameters of the non-bonded kernel
   double tap[8];   // taper coefficients on [nonb_low, nonb_cut] (include/reaxmetal/terms_host.hpp:16-29)
 };
 
@@ -76,6 +80,7 @@ struct Dev {
   // cells
   int* cell_key;         // global cell of every atom (sort key)
   int* cell_atoms;       // atoms sorted by cell
+  double4* xs;           // positions in cell order (w = type), so candidate loads are contiguous
   int* cell_start;       // ncell_total + 1
   int ncell_total;
   // neighbor rows (full: both directions, every image within nonb_cut)
@@ -86,6 +91,12 @@ struct Dev {
   int abits;
   unsigned amask;
   int smax, S;
+  const double4* shifts; // per system and shift index: L.s (xyz), summed as the reference sums lattice shifts
+  // near rows: the entries of the full row within max(bond_cut, hbond_cut), in the same order
+  int ncap_near;
+  unsigned* near;
+  int* near_cnt;
+  double rnear2;
   // bonds
   int bcap;
   unsigned* bcode;
@@ -128,39 +139,28 @@ __device__ inline void decode_shift(int sidx, int S, int smax, int& sx, int& sy,
   sx = sidx / (S * S) - smax;
 }
 
-// Lattice shift L.s summed in the reference's order (src/core/system.cpp:52-57: r[c] += s[k] * vectors[k][c]).
-__device__ inline void lattice_shift(const SysInfo& s, int sx, int sy, int sz, double* sh) {
-  for (int c = 0; c < 3; ++c) {
-    double r = 0.0;
-    r += static_cast<double>(sx) * s.L[0 + c];
-    r += static_cast<double>(sy) * s.L[3 + c];
-    r += static_cast<double>(sz) * s.L[6 + c];
-    sh[c] = r;
-  }
-}
-
 // Canonical separation vector of the entry (i -> j at shift s): computed from the lower-index end (for i == j from the
 // positive shift) and negated for the other direction, so both directions of a pair see bitwise-negated vectors and
-// identical distances; every cut-off decision is therefore symmetric.
-__device__ inline void pair_dvec(const Dev& d, const SysInfo& s, int i, int j, int sidx, double* dv) {
-  int sx, sy, sz;
-  decode_shift(sidx, d.S, d.smax, sx, sy, sz);
-  const int center = (d.S * d.S * d.S - 1) / 2;
-  const bool fwd = (j > i) || (j == i && sidx > center);
-  double sh[3];
+// identical distances; every cut-off decision is therefore symmetric. The lattice shifts come from a per-system
+// table built on the host (the same double-precision sum the reference uses, src/core/system.cpp:52-57).
+__device__ inline void pair_dvec_x(const Dev& d, const SysInfo& s, int i, int j, int sidx, const double4& xi, const double4& xj,
+                                   double* dv) {
+  const int S3 = d.S * d.S * d.S;
+  const bool fwd = (j > i) || (j == i && 2 * sidx > S3 - 1);
   if (fwd) {
-    lattice_shift(s, sx, sy, sz, sh);
-    const double4 xi = d.x[i], xj = d.x[j];
-    dv[0] = (xj.x + sh[0]) - xi.x;
-    dv[1] = (xj.y + sh[1]) - xi.y;
-    dv[2] = (xj.z + sh[2]) - xi.z;
+    const double4 sh = d.shifts[s.shift_base + sidx];
+    dv[0] = (xj.x + sh.x) - xi.x;
+    dv[1] = (xj.y + sh.y) - xi.y;
+    dv[2] = (xj.z + sh.z) - xi.z;
   } else {
-    lattice_shift(s, -sx, -sy, -sz, sh);
-    const double4 xi = d.x[i], xj = d.x[j];
-    dv[0] = -((xi.x + sh[0]) - xj.x);
-    dv[1] = -((xi.y + sh[1]) - xj.y);
-    dv[2] = -((xi.z + sh[2]) - xj.z);
+    const double4 sh = d.shifts[s.shift_base + (S3 - 1 - sidx)];
+    dv[0] = -((xi.x + sh.x) - xj.x);
+    dv[1] = -((xi.y + sh.y) - xj.y);
+    dv[2] = -((xi.z + sh.z) - xj.z);
   }
+}
+__device__ inline void pair_dvec(const Dev& d, const SysInfo& s, int i, int j, int sidx, double* dv) {
+  pair_dvec_x(d, s, i, j, sidx, d.x[i], d.x[j], dv);
 }
 
 __device__ inline double safe_exp(double v) { return exp(v > 700.0 ? 700.0 : v); }

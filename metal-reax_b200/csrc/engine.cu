@@ -93,6 +93,7 @@ struct Context {
   std::vector<int> hsys_of;
   DBuf<SysInfo> sys;
   DBuf<int> sys_of, type, cell_key, cell_key_sorted, cell_atoms, atom_iota, cell_start;
+  DBuf<double4> xs;
   DBuf<long long> tag;
   DBuf<double4> x;
   DBuf<double> q;
@@ -102,9 +103,10 @@ struct Context {
   bool have_pos = false;
 
   // lists
-  int ncap = 0, bcap = 0;
-  DBuf<unsigned> nbr, bcode;
-  DBuf<int> nbr_cnt, bsym, bcnt;
+  int ncap = 0, bcap = 0, ncap_near = 0;
+  DBuf<unsigned> nbr, bcode, near;
+  DBuf<int> nbr_cnt, bsym, bcnt, near_cnt;
+  DBuf<double4> shifts;
   DBuf<double> hval;
   DBuf<double4> bdv, bBO, bdBOp, bdlnpi, bdlnpi2, bC0, bC1, bC2, bacc, bfn, Tl;
   // atoms
@@ -126,6 +128,22 @@ struct Context {
   DBuf<double> mass, ke, temp, scale, xi, vxi;
   MdDev md{};
   long long md_step = 0;
+  // pinned host staging for per-step positions in and gradients out
+  double4* pinned = nullptr;
+  size_t pinned_n = 0;
+  double4* stage(size_t n) {
+    if (pinned_n < n) {
+      if (pinned) cudaFreeHost(pinned);
+      pinned = nullptr;
+      pinned_n = 0;
+      RXCU(cudaMallocHost(&pinned, n * sizeof(double4)));
+      pinned_n = n;
+    }
+    return pinned;
+  }
+  // kernels of this engine launched so far (library kernels such as the radix sort are not counted)
+  long long launches = 0;
+  int key_bits = 32;
   // timing
   bool timing = false;
   std::vector<Phase> phases;
@@ -150,6 +168,7 @@ struct Context {
   }
   ~Context() {
     if (host_only) return;
+    if (pinned) cudaFreeHost(pinned);
     for (auto& p : phases) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     if (stream) cudaStreamDestroy(stream);
   }
@@ -165,14 +184,38 @@ struct Context {
     const size_t nsb = ff.sb.size(), ntb = ff.tb.size(), nthb = ff.thb.size(), nfb = ff.fb.size(), nhb = ff.hb.size();
     const size_t nthn = ff.thb_n.size(), nfo = ff.fb_on.size(), nho = ff.hb_on.size();
     // ints are stored in the same buffer as doubles (one double slot per int)
-    const size_t total = 64 + nsb + ntb + nthb + nfb + nhb + nthn + nfo + nho;
+    std::vector<double> shld(static_cast<size_t>(ff.nt) * ff.nt);
+    for (int a = 0; a < ff.nt; ++a)
+      for (int b = 0; b < ff.nt; ++b) shld[static_cast<size_t>(a) * ff.nt + b] = std::pow(ff.s(a, SB_GAMMA) * ff.s(b, SB_GAMMA), -1.5);
+    // single-precision pair table of the non-bonded kernel: alpha, D, r_vdW, (1/gamma_w)^p_vdW1, ecore, acore, rcore,
+    // gamma (Coulomb shielding), lgcij, lgre^6 (12 floats per type pair)
+    std::vector<float> nbf(static_cast<size_t>(ff.nt) * ff.nt * 12, 0.0f);
+    for (int a = 0; a < ff.nt; ++a)
+      for (int b = 0; b < ff.nt; ++b) {
+        float* o = nbf.data() + (static_cast<size_t>(a) * ff.nt + b) * 12;
+        o[0] = static_cast<float>(ff.p(a, b, TB_ALPHA));
+        o[1] = static_cast<float>(ff.p(a, b, TB_D));
+        o[2] = static_cast<float>(ff.p(a, b, TB_R_VDW));
+        o[3] = static_cast<float>(std::pow(1.0 / ff.p(a, b, TB_GAMMA_W), ff.gp[28]));
+        o[4] = static_cast<float>(ff.p(a, b, TB_ECORE));
+        o[5] = static_cast<float>(ff.p(a, b, TB_ACORE));
+        o[6] = static_cast<float>(ff.p(a, b, TB_RCORE));
+        o[7] = static_cast<float>(ff.p(a, b, TB_GAMMA));
+        o[8] = static_cast<float>(ff.p(a, b, TB_LGCIJ));
+        o[9] = static_cast<float>(std::pow(ff.p(a, b, TB_LGRE), 6.0));
+      }
+    const size_t nbf_d = nbf.size() / 2;
+    const size_t total = 64 + nsb + ntb + nthb + nfb + nhb + nthn + nfo + nho + shld.size() + nbf_d;
     std::vector<double> h(total, 0.0);
     size_t off = 0;
     auto put = [&](const double* src, size_t n) { std::memcpy(h.data() + off, src, n * sizeof(double)); size_t o = off; off += n; return o; };
     std::vector<double> gp(64, 0.0);
     std::copy(ff.gp.begin(), ff.gp.end(), gp.begin());
     const size_t o_gp = put(gp.data(), 64), o_sb = put(ff.sb.data(), nsb), o_tb = put(ff.tb.data(), ntb), o_thb = put(ff.thb.data(), nthb);
-    const size_t o_fb = put(ff.fb.data(), nfb), o_hb = put(ff.hb.data(), nhb);
+    const size_t o_fb = put(ff.fb.data(), nfb), o_hb = put(ff.hb.data(), nhb), o_shld = put(shld.data(), shld.size());
+    const size_t o_nbf = off;
+    std::memcpy(h.data() + off, nbf.data(), nbf.size() * sizeof(float));
+    off += nbf_d;
     auto put_int = [&](const std::vector<int>& v) {
       const size_t o = off;
       std::memcpy(reinterpret_cast<int*>(h.data() + off), v.data(), v.size() * sizeof(int));
@@ -198,6 +241,8 @@ struct Context {
     dff.thb = ff_buf.p + o_thb;
     dff.fb = ff_buf.p + o_fb;
     dff.hb = ff_buf.p + o_hb;
+    dff.shld = ff_buf.p + o_shld;
+    dff.nbf = reinterpret_cast<const float*>(ff_buf.p + o_nbf);
     dff.thb_n = reinterpret_cast<const int*>(ff_buf.p + o_thn);
     dff.fb_on = reinterpret_cast<const int*>(ff_buf.p + o_fo);
     dff.hb_on = reinterpret_cast<const int*>(ff_buf.p + o_ho);
@@ -311,6 +356,7 @@ struct Context {
         ncell *= n;
       }
       si.cell_begin = cell_begin;
+      si.shift_base = 0;
       cell_begin += static_cast<int>(ncell);
       max_density = std::max(max_density, si.natoms / det);
     }
@@ -323,11 +369,29 @@ struct Context {
     if (static_cast<long long>(na) >= (1LL << abits))
       throw Error(RX_ERR_INVALID, "too many atoms for the periodic-image encoding of these boxes");
     ncell_total = cell_begin;
+    {  // lattice shift table: for every system and shift index, L.s summed in the reference's order
+      const int S3 = S * S * S;
+      std::vector<double4> tab(static_cast<size_t>(nsys) * S3);
+      for (int si = 0; si < nsys; ++si) {
+        SysInfo& sy = hsys[static_cast<size_t>(si)];
+        sy.shift_base = si * S3;
+        for (int idx = 0; idx < S3; ++idx) {
+          const int sv[3] = {idx / (S * S) - smax, (idx / S) % S - smax, idx % S - smax};
+          double r[3] = {0.0, 0.0, 0.0};
+          for (int k = 0; k < 3; ++k)
+            for (int c = 0; c < 3; ++c) r[c] += static_cast<double>(sv[k]) * sy.L[3 * k + c];
+          tab[static_cast<size_t>(si) * S3 + idx] = make_double4(r[0], r[1], r[2], 0.0);
+        }
+      }
+      shifts.ensure(tab.size());
+      RXCU(cudaMemcpy(shifts.p, tab.data(), sizeof(double4) * tab.size(), cudaMemcpyHostToDevice));
+    }
     sys.ensure(static_cast<size_t>(nsys));
     RXCU(cudaMemcpy(sys.p, hsys.data(), sizeof(SysInfo) * nsys, cudaMemcpyHostToDevice));
     cell_key.ensure(static_cast<size_t>(na));
     cell_key_sorted.ensure(static_cast<size_t>(na));
     cell_atoms.ensure(static_cast<size_t>(na));
+    xs.ensure(static_cast<size_t>(na));
     atom_iota.ensure(static_cast<size_t>(na));
     cell_start.ensure(static_cast<size_t>(ncell_total) + 1);
     {
@@ -335,12 +399,17 @@ struct Context {
       for (int a = 0; a < na; ++a) io[static_cast<size_t>(a)] = a;
       RXCU(cudaMemcpy(atom_iota.p, io.data(), sizeof(int) * na, cudaMemcpyHostToDevice));
     }
+    key_bits = 1;
+    while ((1LL << key_bits) <= ncell_total) ++key_bits;
     size_t tmp = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, 32, stream);
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, key_bits, stream);
     cub_tmp.ensure(tmp);
     const double expect = 4.0 / 3.0 * M_PI * rc * rc * rc * max_density;
     const int want_ncap = static_cast<int>(std::ceil((expect * 1.3 + 32) / 32.0)) * 32;
     if (ncap < want_ncap) ncap = want_ncap;
+    const double rn = std::max(ctl.bond_cut, ctl.hbond_cut);
+    const int want_near = static_cast<int>(std::ceil((4.0 / 3.0 * M_PI * rn * rn * rn * max_density * 1.3 + 32) / 32.0)) * 32;
+    if (ncap_near < want_near) ncap_near = want_near;
     if (bcap < 8) bcap = 8;
     alloc_atoms();
     alloc_lists();
@@ -351,7 +420,7 @@ struct Context {
     Deltap.ensure(n); Deltap_boc.ensure(n); cdtot.ensure(n); W.ensure(n); eatom.ensure(n * kTerms);
     dDp_self.ensure(n); fown.ensure(n); fdb.ensure(n); fnb.ensure(n); grad.ensure(n);
     aq.ensure(n); census.ensure(n * kCensus);
-    nbr_cnt.ensure(n); bcnt.ensure(n);
+    nbr_cnt.ensure(n); bcnt.ensure(n); near_cnt.ensure(n);
     energies.ensure(static_cast<size_t>(nsys) * kTerms);
     cg_x.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
@@ -362,6 +431,7 @@ struct Context {
     const size_t n = static_cast<size_t>(na);
     nbr.ensure(n * ncap);
     hval.ensure(n * ncap);
+    near.ensure(n * ncap_near);
     const size_t nb = n * bcap;
     bcode.ensure(nb); bsym.ensure(nb);
     bdv.ensure(nb); bBO.ensure(nb); bdBOp.ensure(nb); bdlnpi.ensure(nb); bdlnpi2.ensure(nb);
@@ -372,9 +442,14 @@ struct Context {
   Dev dev() {
     Dev d{};
     d.na = na; d.nsys = nsys; d.sys = sys.p; d.sys_of = sys_of.p; d.x = x.p; d.type = type.p; d.tag = tag.p; d.q = q.p;
-    d.cell_key = cell_key.p; d.cell_atoms = cell_atoms.p; d.cell_start = cell_start.p; d.ncell_total = ncell_total;
+    d.cell_key = cell_key.p; d.cell_atoms = cell_atoms.p; d.xs = xs.p; d.cell_start = cell_start.p; d.ncell_total = ncell_total;
     d.ncap = ncap; d.nbr = nbr.p; d.nbr_cnt = nbr_cnt.p; d.hval = hval.p;
     d.abits = abits; d.amask = (abits >= 32) ? 0xffffffffu : ((1u << abits) - 1u); d.smax = smax; d.S = S;
+    d.shifts = shifts.p; d.ncap_near = ncap_near; d.near = near.p; d.near_cnt = near_cnt.p;
+    {  // a superset of every consumer's sqrt(r2) <= cut test
+      const double rn = std::max(ctl.bond_cut, ctl.hbond_cut) * (1.0 + 1e-9);
+      d.rnear2 = rn * rn;
+    }
     d.bcap = bcap; d.bcode = bcode.p; d.bsym = bsym.p; d.bcnt = bcnt.p; d.bdv = bdv.p; d.bBO = bBO.p; d.bdBOp = bdBOp.p;
     d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p;
     d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
@@ -412,10 +487,13 @@ struct Context {
 
   void build_lists(const Dev& d) {
     tic(0, "neighbors");
+    ++launches;
     k_wrap_bin<<<blocks(na, 256), 256, 0, stream>>>(d);
     size_t tmp = cub_tmp.n;
-    RXCU(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, 32, stream));
+    RXCU(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, key_bits, stream));
+    ++launches;
     k_cell_start<<<blocks(na + 1, 256), 256, 0, stream>>>(d, cell_key_sorted.p);
+    ++launches;
     k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, qp);
     toc(0);
   }
@@ -431,6 +509,7 @@ struct Context {
   void launch_qeq(const Dev& d) {
     tic(1, "qeq");
     CgArgs a = cg_args();
+    ++launches;
     k_qeq_prepare<<<blocks(na, 256), 256, 0, stream>>>(d, dff, a, s_hist.p, t_hist.p);
     if (nsys == 1 && na > 4096) {
       const int threads = 256;
@@ -441,8 +520,10 @@ struct Context {
       a.begin = 0;
       a.n = na;
       void* args[] = {const_cast<Dev*>(&d), &a};
-      RXCU(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_grid), dim3(grid), dim3(threads), args, 0, stream));
+      ++launches;
+    RXCU(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_grid), dim3(grid), dim3(threads), args, 0, stream));
     } else {
+      ++launches;
       k_cg_block<<<nsys, 512, 0, stream>>>(d, a);
     }
     toc(1);
@@ -450,30 +531,43 @@ struct Context {
 
   void launch_bonded(const Dev& d) {
     tic(2, "bond_orders");
+    ++launches;
     k_bonds<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, ctl);
+    ++launches;
     k_bond_sym<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d);
+    ++launches;
     k_bo_correct<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d, dff);
+    ++launches;
     k_atom_quantities<<<blocks(na, 128), 128, 0, stream>>>(d, dff);
     toc(2);
     tic(3, "bonded_terms");
+    ++launches;
     k_bonded_atom<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
-    k_hbond_acceptor<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
+    ++launches;
+    k_hbond<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, ctl);
+    ++launches;
+    k_hbond_acceptor<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, ctl);
     toc(3);
     tic(4, "torsion");
+    ++launches;
     k_torsion<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
     toc(4);
   }
 
   void launch_nonbonded(const Dev& d) {
     tic(5, "nonbonded");
+    ++launches;
     k_nonbonded<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff);
     toc(5);
   }
 
   void launch_gather(const Dev& d) {
     tic(6, "gather");
+    ++launches;
     k_fold<<<blocks(na, 128), 128, 0, stream>>>(d);
+    ++launches;
     k_dbond<<<blocks(na, 128), 128, 0, stream>>>(d);
+    ++launches;
     k_force_final<<<blocks(na, 128), 128, 0, stream>>>(d);
     toc(6);
   }
@@ -496,9 +590,10 @@ struct Context {
       RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaStreamSynchronize(stream));
       RXCU(cudaGetLastError());
-      if (st[0] & (ST_NBR_OVERFLOW | ST_BOND_OVERFLOW)) {
+      if (st[0] & (ST_NBR_OVERFLOW | ST_BOND_OVERFLOW | ST_NEAR_OVERFLOW)) {
         if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "list capacity still exceeded after 4 grow attempts");
         if (st[0] & ST_NBR_OVERFLOW) ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
+        if (st[0] & ST_NEAR_OVERFLOW) ncap_near = ((st[3] * 5 / 4) + 31) / 32 * 32;
         if (st[0] & ST_BOND_OVERFLOW) bcap = std::max(bcap, ((st[2] * 5 / 4) + 3) / 4 * 4);
         alloc_lists();
         continue;
@@ -520,6 +615,7 @@ struct Context {
     last_rel.resize(2 * static_cast<size_t>(nsys));
     RXCU(cudaMemcpy(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost));
     RXCU(cudaMemcpy(last_rel.data(), cg_rel.p, sizeof(double) * 2 * nsys, cudaMemcpyDeviceToHost));
+    ++launches;
     k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(dev(), cg_x.p, s_hist.p, t_hist.p);
     RXCU(cudaStreamSynchronize(stream));
     if (qeq_strict)
@@ -530,15 +626,16 @@ struct Context {
   }
 
   void energy_sums() {
-    k_energy_sum<<<nsys, 256, 0, stream>>>(dev(), energies.p);
+    ++launches;
+    k_energy_sum<<<dim3(nsys, kTerms), 256, 0, stream>>>(dev(), energies.p);
   }
 
   // ------------------------------------------------------------------ state I/O
   void set_positions(const double* xin) {
     require_sys();
-    std::vector<double4> h(static_cast<size_t>(na));
-    for (int a = 0; a < na; ++a) h[static_cast<size_t>(a)] = make_double4(xin[3 * a], xin[3 * a + 1], xin[3 * a + 2], 0.0);
-    RXCU(cudaMemcpyAsync(x.p, h.data(), sizeof(double4) * na, cudaMemcpyHostToDevice, stream));
+    double4* h = stage(static_cast<size_t>(na));
+    for (int a = 0; a < na; ++a) h[a] = make_double4(xin[3 * a], xin[3 * a + 1], xin[3 * a + 2], 0.0);
+    RXCU(cudaMemcpyAsync(x.p, h, sizeof(double4) * na, cudaMemcpyHostToDevice, stream));
     RXCU(cudaStreamSynchronize(stream));
     have_pos = true;
   }
@@ -554,10 +651,10 @@ struct Context {
     evaluate((flags & RX_COMPUTE_QEQ) != 0);
     energy_sums();
     if (e_out) RXCU(cudaMemcpyAsync(e_out, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
-    std::vector<double4> g;
+    double4* g = nullptr;
     if (g_out) {
-      g.resize(static_cast<size_t>(na));
-      RXCU(cudaMemcpyAsync(g.data(), grad.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, stream));
+      g = stage(static_cast<size_t>(na));
+      RXCU(cudaMemcpyAsync(g, grad.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, stream));
     }
     if (cen_out) RXCU(cudaMemcpyAsync(cen_out, census.p, sizeof(int) * kCensus * na, cudaMemcpyDeviceToHost, stream));
     std::vector<int> nb, bc;
@@ -597,9 +694,10 @@ struct Context {
       RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaStreamSynchronize(stream));
       RXCU(cudaGetLastError());
-      if (st[0] & ST_NBR_OVERFLOW) {
+      if (st[0] & (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW)) {
         if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "neighbor capacity still exceeded after 4 grow attempts");
-        ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
+        if (st[0] & ST_NBR_OVERFLOW) ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
+        if (st[0] & ST_NEAR_OVERFLOW) ncap_near = ((st[3] * 5 / 4) + 31) / 32 * 32;
         alloc_lists();
         continue;
       }
@@ -623,9 +721,10 @@ struct Context {
       int st[4];
       RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaStreamSynchronize(stream));
-      if (st[0] & ST_NBR_OVERFLOW) {
+      if (st[0] & (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW)) {
         if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "neighbor capacity still exceeded after 4 grow attempts");
-        ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
+        if (st[0] & ST_NBR_OVERFLOW) ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
+        if (st[0] & ST_NEAR_OVERFLOW) ncap_near = ((st[3] * 5 / 4) + 31) / 32 * 32;
         alloc_lists();
         continue;
       }
@@ -634,6 +733,7 @@ struct Context {
     std::vector<double2> h(static_cast<size_t>(na));
     for (int a = 0; a < na; ++a) h[static_cast<size_t>(a)] = make_double2(vin[a], 0.0);
     RXCU(cudaMemcpy(cg_d.p, h.data(), sizeof(double2) * na, cudaMemcpyHostToDevice));
+    ++launches;
     k_qeq_matvec<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(dev(), dff, cg_d.p, cg_q.p);
     RXCU(cudaMemcpyAsync(h.data(), cg_q.p, sizeof(double2) * na, cudaMemcpyDeviceToHost, stream));
     RXCU(cudaStreamSynchronize(stream));
@@ -673,8 +773,11 @@ struct Context {
   }
 
   void thermostat_half(double frac) {
+    ++launches;
     k_md_kinetic<<<nsys, 256, 0, stream>>>(md, sys.p, type.p);
+    ++launches;
     k_md_chain<<<blocks(nsys, 64), 64, 0, stream>>>(md, sys.p, nsys, frac);
+    ++launches;
     k_md_scale<<<blocks(na, 256), 256, 0, stream>>>(md, sys_of.p, na);
   }
 
@@ -685,8 +788,10 @@ struct Context {
     for (int s = 0; s < nsteps; ++s) {
       const double frac = span > 0 ? static_cast<double>(s) / static_cast<double>(span) : 0.0;
       thermostat_half(frac);
+      ++launches;
       k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 1);
       evaluate(true);
+      ++launches;
       k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 0);
       thermostat_half(frac);
       ++md_step;
@@ -694,6 +799,7 @@ struct Context {
     energy_sums();
     if (e_out) RXCU(cudaMemcpyAsync(e_out, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
     if (t_out) {
+      ++launches;
       k_md_kinetic<<<nsys, 256, 0, stream>>>(md, sys.p, type.p);
       std::vector<double> kk(static_cast<size_t>(nsys));
       RXCU(cudaMemcpyAsync(kk.data(), ke.p, sizeof(double) * nsys, cudaMemcpyDeviceToHost, stream));
@@ -836,6 +942,8 @@ int rx_get_velocities(rx_context* ctx, double* v) { return guarded(ctx, [&](rx::
 int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature) {
   return guarded(ctx, [&](rx::Context& c) { c.md_run(nsteps, energies, temperature, 0); });
 }
+
+int64_t rx_kernel_launches(const rx_context* ctx) { return (ctx && ctx->c) ? ctx->c->launches : 0; }
 
 void* rx_stream(rx_context* ctx) { return (ctx && ctx->c) ? reinterpret_cast<void*>(ctx->c->stream) : nullptr; }
 

@@ -75,7 +75,7 @@ __global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl) {
   const SysInfo s = d.sys[d.sys_of[i]];
   const int ti = d.type[i];
   const double* si = SBp(ff, ti);
-  const int cnt = min(d.nbr_cnt[i], d.ncap);
+  const int cnt = min(d.near_cnt[i], d.ncap_near);
   const unsigned lt = (1u << lane) - 1u;
   const double bo_cut = ff.bo_cut;
   int nb = 0;
@@ -87,7 +87,7 @@ __global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl) {
     double dv[3] = {0, 0, 0}, dd = 0, BOt = 0, BO_s = 0, BO_pi = 0, BO_pi2 = 0, C12 = 0, C34 = 0, C56 = 0;
     const double* tb = nullptr;
     if (e < cnt) {
-      code = d.nbr[static_cast<size_t>(i) * d.ncap + e];
+      code = d.near[static_cast<size_t>(i) * d.ncap_near + e];
       const int j = static_cast<int>(code & d.amask);
       const int sidx = static_cast<int>(code >> d.abits);
       pair_dvec(d, s, i, j, sidx, dv);
@@ -271,8 +271,7 @@ __global__ void k_atom_quantities(Dev d, DevFF ff) {
 
 // ------------------------------------------------------------------------------------------------ per-centre terms
 // One thread per atom j: bond energy + triple-bond stabilisation (src/cpu/bonded.cpp:219-253), lone pair + C2
-// (:255-281), over/under coordination (:282-318), valence angle + penalty + coalition centred at j (:321-474) and the
-// H-bonds of hydrogen j (:654-715). Coefficients of j's own bonds go to j's slots; contributions to a bond partner
+// (:255-281), over/under coordination (:282-318), valence angle + penalty + coalition centred at j (:321-474). Coefficients of j's own bonds go to j's slots; contributions to a bond partner
 // (its CdDelta, its gradient) go to the slot naming it, for the partner to gather.
 __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -288,7 +287,7 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
     d.bfn[base + k] = make_double4(0, 0, 0, 0);
   }
   double fj[3] = {0, 0, 0}, cdd = 0.0;
-  double e_bond = 0, e_lp = 0, e_ov = 0, e_un = 0, e_ang = 0, e_pen = 0, e_coa = 0, e_hb = 0;
+  double e_bond = 0, e_lp = 0, e_ov = 0, e_un = 0, e_ang = 0, e_pen = 0, e_coa = 0;
 
   // ---- bond energy (owned end chosen by tag order)
   {
@@ -545,14 +544,79 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
     }
     d.census[1 * d.na + j] = nsets;
   }
-  // ---- hydrogen bonds of hydrogen j
-  int nhb = 0;
-  if (ctl.hbond_cut > 0 && static_cast<int>(sj[SB_P_HBOND]) == 1) {
-    const SysInfo s = d.sys[d.sys_of[j]];
-    const int cnt = min(d.nbr_cnt[j], d.ncap);
-    const double hc2 = ctl.hbond_cut * ctl.hbond_cut;
-    for (int e = 0; e < cnt; ++e) {
-      const unsigned code = d.nbr[static_cast<size_t>(j) * d.ncap + e];
+  d.fown[j] = make_double4(fj[0], fj[1], fj[2], cdd);
+  double* ea = d.eatom + static_cast<size_t>(j) * kTerms;
+  ea[E_BOND] = e_bond; ea[E_OV] = e_ov; ea[E_UN] = e_un; ea[E_LP] = e_lp;
+  ea[E_ANG] = e_ang; ea[E_PEN] = e_pen; ea[E_COA] = e_coa;
+}
+
+// Hydrogen bonds (src/cpu/bonded.cpp:654-715) of one triple: donor bond slot bi of hydrogen j, acceptor k at the
+// canonical vector dvjk (x_k - x_j) and distance r_jk. Returns false when a gate of the reference rejects it.
+struct HbOut { double e, CEhb1, CEhb2, CEhb3, dti[3], dtj[3], dtk[3]; };
+__device__ inline bool hbond_triple(const Dev& d, const DevFF& ff, int tj, int type_k, long long tag_k, size_t bi,
+                                    const double* dvjk, double r_jk, HbOut& o) {
+  const int ia = static_cast<int>(d.bcode[bi] & d.amask);
+  const int type_i = d.type[ia];
+  if (static_cast<int>(SBp(ff, type_i)[SB_P_HBOND]) != 2) return false;
+  const double BO = d.bBO[bi].x;
+  if (!(BO >= kHbThreshold)) return false;
+  if (d.tag[ia] == tag_k) return false;
+  const size_t key = (static_cast<size_t>(type_i) * ff.nt + tj) * ff.nt + type_k;
+  if (!ff.hb_on[key]) return false;
+  const double* hb = ff.hb + key * HB_NFIELDS;
+  if (hb[HB_R0] <= 0.0) return false;
+  const double4 dvi = d.bdv[bi];
+  const double vi[3] = {dvi.x, dvi.y, dvi.z};
+  double theta, cos_theta;
+  calc_theta(vi, dvi.w, dvjk, r_jk, theta, cos_theta);
+  calc_dcos(vi, dvi.w, dvjk, r_jk, o.dti, o.dtj, o.dtk);
+  const double sin_theta2 = sin(theta / 2.0);
+  double sin_xhz4 = sin_theta2 * sin_theta2;
+  sin_xhz4 *= sin_xhz4;
+  const double cos_xhz1 = (1.0 - cos_theta);
+  const double exp_hb2 = exp(-hb[HB_P_HB2] * BO);
+  const double exp_hb3 = exp(-hb[HB_P_HB3] * (hb[HB_R0] / r_jk + r_jk / hb[HB_R0] - 2.0));
+  o.e = hb[HB_P_HB1] * (1.0 - exp_hb2) * exp_hb3 * sin_xhz4;
+  o.CEhb1 = hb[HB_P_HB1] * hb[HB_P_HB2] * exp_hb2 * exp_hb3 * sin_xhz4;
+  o.CEhb2 = -hb[HB_P_HB1] / 2.0 * (1.0 - exp_hb2) * exp_hb3 * cos_xhz1;
+  o.CEhb3 = -hb[HB_P_HB3] * (-hb[HB_R0] / (r_jk * r_jk) + 1.0 / hb[HB_R0]) * o.e;
+  return true;
+}
+
+// One warp per hydrogen j (p_hbond = 1): for every donor bond of j, the lanes walk j's near row for acceptors
+// (p_hbond = 2, r <= hbond_cut). Energy, the gradient of j and the coefficient / gradient of the donor bond are
+// reduced over the warp in fixed order; the donor's share goes to j's slot for the donor to gather.
+__global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= d.na) return;
+  const int j = warp;
+  const int tj = d.type[j];
+  if (!(ctl.hbond_cut > 0) || static_cast<int>(SBp(ff, tj)[SB_P_HBOND]) != 1) {
+    if (lane == 0) {
+      d.eatom[static_cast<size_t>(j) * kTerms + E_HB] = 0.0;
+      d.census[3 * d.na + j] = 0;
+    }
+    return;
+  }
+  const SysInfo s = d.sys[d.sys_of[j]];
+  const int cnt = min(d.near_cnt[j], d.ncap_near);
+  const int nb = min(d.bcnt[j], d.bcap);
+  const double hc2 = ctl.hbond_cut * ctl.hbond_cut;
+  const size_t base = static_cast<size_t>(j) * d.bcap;
+  double e = 0.0, fj0 = 0.0, fj1 = 0.0, fj2 = 0.0;
+  int ntrip = 0;
+  for (int pi = 0; pi < nb; ++pi) {
+    const size_t bi = base + pi;
+    {  // donor gates that do not depend on the acceptor (warp-uniform)
+      const int ia = static_cast<int>(d.bcode[bi] & d.amask);
+      if (static_cast<int>(SBp(ff, d.type[ia])[SB_P_HBOND]) != 2 || !(d.bBO[bi].x >= kHbThreshold)) continue;
+    }
+    double c1 = 0.0, fi0 = 0.0, fi1 = 0.0, fi2 = 0.0;
+    for (int e0 = 0; e0 < cnt; e0 += 32) {
+      const int ee = e0 + lane;
+      if (ee >= cnt) continue;
+      const unsigned code = d.near[static_cast<size_t>(j) * d.ncap_near + ee];
       const int ka = static_cast<int>(code & d.amask);
       const int type_k = d.type[ka];
       if (static_cast<int>(SBp(ff, type_k)[SB_P_HBOND]) != 2) continue;
@@ -562,63 +626,53 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
       if (!(r2 <= hc2)) continue;
       const double r_jk = sqrt(r2);
       if (!(r_jk <= ctl.hbond_cut)) continue;
-      for (int pi = 0; pi < nb; ++pi) {
-        const size_t bi = base + pi;
-        const int ia = static_cast<int>(d.bcode[bi] & d.amask);
-        const int type_i = d.type[ia];
-        if (static_cast<int>(SBp(ff, type_i)[SB_P_HBOND]) != 2) continue;
-        const double4 boi = d.bBO[bi];
-        if (!(boi.x >= kHbThreshold)) continue;
-        if (d.tag[ia] == d.tag[ka]) continue;
-        const size_t key = (static_cast<size_t>(type_i) * ff.nt + tj) * ff.nt + type_k;
-        if (!ff.hb_on[key]) continue;
-        const double* hb = ff.hb + key * HB_NFIELDS;
-        if (hb[HB_R0] <= 0.0) continue;
-        ++nhb;
-        const double4 dvi = d.bdv[bi];
-        const double vi[3] = {dvi.x, dvi.y, dvi.z};
-        double theta, cos_theta, dti[3], dtj[3], dtk[3];
-        calc_theta(vi, dvi.w, dvjk, r_jk, theta, cos_theta);
-        calc_dcos(vi, dvi.w, dvjk, r_jk, dti, dtj, dtk);
-        const double sin_theta2 = sin(theta / 2.0);
-        double sin_xhz4 = sin_theta2 * sin_theta2;
-        sin_xhz4 *= sin_xhz4;
-        const double cos_xhz1 = (1.0 - cos_theta);
-        const double exp_hb2 = exp(-hb[HB_P_HB2] * boi.x);
-        const double exp_hb3 = exp(-hb[HB_P_HB3] * (hb[HB_R0] / r_jk + r_jk / hb[HB_R0] - 2.0));
-        const double e_hb_t = hb[HB_P_HB1] * (1.0 - exp_hb2) * exp_hb3 * sin_xhz4;
-        e_hb += e_hb_t;
-        const double CEhb1 = hb[HB_P_HB1] * hb[HB_P_HB2] * exp_hb2 * exp_hb3 * sin_xhz4;
-        const double CEhb2 = -hb[HB_P_HB1] / 2.0 * (1.0 - exp_hb2) * exp_hb3 * cos_xhz1;
-        const double CEhb3 = -hb[HB_P_HB3] * (-hb[HB_R0] / (r_jk * r_jk) + 1.0 / hb[HB_R0]) * e_hb_t;
-        d.bacc[bi].x += CEhb1;
-        add3(d.bfn[bi], CEhb2, dti);
-        for (int c = 0; c < 3; ++c) fj[c] += CEhb2 * dtj[c];
-        for (int c = 0; c < 3; ++c) fj[c] += -CEhb3 / r_jk * dvjk[c];
-      }
+      HbOut o;
+      if (!hbond_triple(d, ff, tj, type_k, d.tag[ka], bi, dvjk, r_jk, o)) continue;
+      ++ntrip;
+      e += o.e;
+      c1 += o.CEhb1;
+      fi0 += o.CEhb2 * o.dti[0]; fi1 += o.CEhb2 * o.dti[1]; fi2 += o.CEhb2 * o.dti[2];
+      fj0 += o.CEhb2 * o.dtj[0] + -o.CEhb3 / r_jk * dvjk[0];
+      fj1 += o.CEhb2 * o.dtj[1] + -o.CEhb3 / r_jk * dvjk[1];
+      fj2 += o.CEhb2 * o.dtj[2] + -o.CEhb3 / r_jk * dvjk[2];
     }
+    c1 = warp_sum(c1); fi0 = warp_sum(fi0); fi1 = warp_sum(fi1); fi2 = warp_sum(fi2);
+    if (lane == 0) {
+      d.bacc[bi].x += c1;
+      double4 fn = d.bfn[bi];
+      fn.x += fi0; fn.y += fi1; fn.z += fi2;
+      d.bfn[bi] = fn;
+    }
+    __syncwarp();
   }
-  d.census[3 * d.na + j] = nhb;
-  d.fown[j] = make_double4(fj[0], fj[1], fj[2], cdd);
-  double* ea = d.eatom + static_cast<size_t>(j) * kTerms;
-  ea[E_BOND] = e_bond; ea[E_OV] = e_ov; ea[E_UN] = e_un; ea[E_LP] = e_lp;
-  ea[E_ANG] = e_ang; ea[E_PEN] = e_pen; ea[E_COA] = e_coa; ea[E_HB] = e_hb;
+  e = warp_sum(e); fj0 = warp_sum(fj0); fj1 = warp_sum(fj1); fj2 = warp_sum(fj2);
+  for (int o = 16; o > 0; o >>= 1) ntrip += __shfl_xor_sync(0xffffffffu, ntrip, o);
+  if (lane == 0) {
+    double4 f = d.fown[j];
+    f.x += fj0; f.y += fj1; f.z += fj2;
+    d.fown[j] = f;
+    d.eatom[static_cast<size_t>(j) * kTerms + E_HB] = e;
+    d.census[3 * d.na + j] = ntrip;
+  }
 }
 
-// The gradient on the acceptor k of every H-bond triple (i, j, k): each triple is evaluated again from the acceptor's
-// side, with bitwise the same inputs (the H's bond slot, the canonical j -> k vector), so the acceptor gathers its own
-// gradient without any write to another atom.
-__global__ void k_hbond_acceptor(Dev d, DevFF ff, DevCtl ctl) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= d.na) return;
+// The gradient on the acceptor k of every H-bond triple: each triple is evaluated again from the acceptor's side
+// (one warp per acceptor, lanes over its near row), with bitwise the same inputs (the hydrogen's bond slot, the
+// canonical j -> k vector), so the acceptor gathers its own gradient without writing to any other atom.
+__global__ void __launch_bounds__(128) k_hbond_acceptor(Dev d, DevFF ff, DevCtl ctl) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= d.na) return;
+  const int k = warp;
   const int type_k = d.type[k];
   if (!(ctl.hbond_cut > 0) || static_cast<int>(SBp(ff, type_k)[SB_P_HBOND]) != 2) return;
   const SysInfo s = d.sys[d.sys_of[k]];
-  const int cnt = min(d.nbr_cnt[k], d.ncap);
+  const int cnt = min(d.near_cnt[k], d.ncap_near);
   const double hc2 = ctl.hbond_cut * ctl.hbond_cut;
-  double fk[3] = {0, 0, 0};
-  for (int e = 0; e < cnt; ++e) {
-    const unsigned code = d.nbr[static_cast<size_t>(k) * d.ncap + e];
+  const long long tag_k = d.tag[k];
+  double f0 = 0, f1 = 0, f2 = 0;
+  for (int e = lane; e < cnt; e += 32) {
+    const unsigned code = d.near[static_cast<size_t>(k) * d.ncap_near + e];
     const int h = static_cast<int>(code & d.amask);
     const int tj = d.type[h];
     if (static_cast<int>(SBp(ff, tj)[SB_P_HBOND]) != 1) continue;
@@ -631,38 +685,19 @@ __global__ void k_hbond_acceptor(Dev d, DevFF ff, DevCtl ctl) {
     if (!(r_jk <= ctl.hbond_cut)) continue;
     const int nb = min(d.bcnt[h], d.bcap);
     for (int pi = 0; pi < nb; ++pi) {
-      const size_t bi = static_cast<size_t>(h) * d.bcap + pi;
-      const int ia = static_cast<int>(d.bcode[bi] & d.amask);
-      const int type_i = d.type[ia];
-      if (static_cast<int>(SBp(ff, type_i)[SB_P_HBOND]) != 2) continue;
-      const double4 boi = d.bBO[bi];
-      if (!(boi.x >= kHbThreshold)) continue;
-      if (d.tag[ia] == d.tag[k]) continue;
-      const size_t key = (static_cast<size_t>(type_i) * ff.nt + tj) * ff.nt + type_k;
-      if (!ff.hb_on[key]) continue;
-      const double* hb = ff.hb + key * HB_NFIELDS;
-      if (hb[HB_R0] <= 0.0) continue;
-      const double4 dvi = d.bdv[bi];
-      const double vi[3] = {dvi.x, dvi.y, dvi.z};
-      double theta, cos_theta, dti[3], dtj[3], dtk[3];
-      calc_theta(vi, dvi.w, dvjk, r_jk, theta, cos_theta);
-      calc_dcos(vi, dvi.w, dvjk, r_jk, dti, dtj, dtk);
-      const double sin_theta2 = sin(theta / 2.0);
-      double sin_xhz4 = sin_theta2 * sin_theta2;
-      sin_xhz4 *= sin_xhz4;
-      const double cos_xhz1 = (1.0 - cos_theta);
-      const double exp_hb2 = exp(-hb[HB_P_HB2] * boi.x);
-      const double exp_hb3 = exp(-hb[HB_P_HB3] * (hb[HB_R0] / r_jk + r_jk / hb[HB_R0] - 2.0));
-      const double e_hb_t = hb[HB_P_HB1] * (1.0 - exp_hb2) * exp_hb3 * sin_xhz4;
-      const double CEhb2 = -hb[HB_P_HB1] / 2.0 * (1.0 - exp_hb2) * exp_hb3 * cos_xhz1;
-      const double CEhb3 = -hb[HB_P_HB3] * (-hb[HB_R0] / (r_jk * r_jk) + 1.0 / hb[HB_R0]) * e_hb_t;
-      for (int c = 0; c < 3; ++c) fk[c] += CEhb2 * dtk[c];
-      for (int c = 0; c < 3; ++c) fk[c] += CEhb3 / r_jk * dvjk[c];
+      HbOut o;
+      if (!hbond_triple(d, ff, tj, type_k, tag_k, static_cast<size_t>(h) * d.bcap + pi, dvjk, r_jk, o)) continue;
+      f0 += o.CEhb2 * o.dtk[0] + o.CEhb3 / r_jk * dvjk[0];
+      f1 += o.CEhb2 * o.dtk[1] + o.CEhb3 / r_jk * dvjk[1];
+      f2 += o.CEhb2 * o.dtk[2] + o.CEhb3 / r_jk * dvjk[2];
     }
   }
-  double4 f = d.fown[k];
-  f.x += fk[0]; f.y += fk[1]; f.z += fk[2];
-  d.fown[k] = f;
+  f0 = warp_sum(f0); f1 = warp_sum(f1); f2 = warp_sum(f2);
+  if (lane == 0) {
+    double4 f = d.fown[k];
+    f.x += f0; f.y += f1; f.z += f2;
+    d.fown[k] = f;
+  }
 }
 
 // ------------------------------------------------------------------------------------------------ torsion

@@ -42,13 +42,19 @@ __global__ void k_wrap_bin(Dev d) {
   d.cell_key[a] = s.cell_begin + (c[2] * s.nc[1] + c[1]) * s.nc[0] + c[0];
 }
 
-// cell_start[c] = first position in the sorted order whose key is >= c
+// cell_start[c] = first position in the sorted order whose key is >= c; positions gathered into cell order
 __global__ void k_cell_start(Dev d, const int* sorted_keys) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p > d.na) return;
   const int prev = p == 0 ? -1 : sorted_keys[p - 1];
   const int cur = p == d.na ? d.ncell_total : sorted_keys[p];
   for (int c = prev + 1; c <= cur; ++c) d.cell_start[c] = p;
+  if (p < d.na) {
+    const int a = d.cell_atoms[p];
+    double4 x = d.x[a];
+    x.w = static_cast<double>(d.type[a]);
+    d.xs[p] = x;
+  }
 }
 
 // ------------------------------------------------------------------------------------------------ neighbor rows
@@ -63,10 +69,12 @@ __device__ inline void taper_horner(const double* c, double r, double& Tap, doub
 }
 
 // One warp per atom: every image of every atom within nonb_cut (the owned-row cut-off of build_far_list,
-// src/neighbor/neighbor.cpp:180-212), found through the cells within `range` of the atom's cell, periodic images
-// included. Entries are written in cell-scan order through a warp ballot (deterministic). Fused: the charge-matrix
-// entry H = 14.4 Tap(r) / cbrt(r^3 + (gamma_i gamma_j)^-1.5) for r <= swb (ENGINE_SPEC 7; fix_qeq_reaxff compute_H).
-__global__ void k_neighbors(Dev d, DevFF ff, QeqParams qp) {
+// src/neighbor/neighbor.cpp:180-212). The cells within `range` of the atom's cell are visited as runs of consecutive
+// cells along x (one contiguous range of the cell-ordered atoms per run and periodic image), so the candidate loads are
+// coalesced. Entries are written through a warp ballot in visiting order (deterministic). Fused: the charge-matrix
+// entry H = 14.4 Tap(r) / cbrt(r^3 + (gamma_i gamma_j)^-1.5) for r <= swb (ENGINE_SPEC 7; fix_qeq_reaxff compute_H),
+// and the near row (entries within max(bond_cut, hbond_cut)) the bond and H-bond kernels scan.
+__global__ void __launch_bounds__(128) k_neighbors(Dev d, DevFF ff, QeqParams qp) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
@@ -75,53 +83,68 @@ __global__ void k_neighbors(Dev d, DevFF ff, QeqParams qp) {
   const int key = d.cell_key[i] - s.cell_begin;
   const int cx = key % s.nc[0], cy = (key / s.nc[0]) % s.nc[1], cz = key / (s.nc[0] * s.nc[1]);
   const double rc2 = ff.nonb_cut * ff.nonb_cut;
+  const double4 xi = d.x[i];
   const int ti = d.type[i];
-  const double gi = ff.sb[ti * SB_N + SB_GAMMA];
-  int count = 0;
+  const double* shld_i = ff.shld + static_cast<size_t>(ti) * ff.nt;
+  int count = 0, count_near = 0;
   const unsigned lt = (1u << lane) - 1u;
   const int center = (d.S * d.S * d.S - 1) / 2;
+  const size_t rowbase = static_cast<size_t>(i) * d.ncap;
   for (int oz = -s.range[2]; oz <= s.range[2]; ++oz) {
     const int zz = cz + oz, shz = floor_div(zz, s.nc[2]), wz = zz - shz * s.nc[2];
     for (int oy = -s.range[1]; oy <= s.range[1]; ++oy) {
       const int yy = cy + oy, shy = floor_div(yy, s.nc[1]), wy = yy - shy * s.nc[1];
-      for (int ox = -s.range[0]; ox <= s.range[0]; ++ox) {
-        const int xx = cx + ox, shx = floor_div(xx, s.nc[0]), wx = xx - shx * s.nc[0];
+      const int rowcell = s.cell_begin + (wz * s.nc[1] + wy) * s.nc[0];
+      int xx = cx - s.range[0];
+      const int xend = cx + s.range[0];
+      while (xx <= xend) {
+        const int shx = floor_div(xx, s.nc[0]);
+        const int wx0 = xx - shx * s.nc[0];
+        const int len = min(s.nc[0] - wx0, xend - xx + 1);
+        xx += len;
         if (shx < -d.smax || shx > d.smax || shy < -d.smax || shy > d.smax || shz < -d.smax || shz > d.smax) {
           if (lane == 0) atomicOr(d.status, ST_SHIFT_RANGE);
           continue;
         }
         const int sidx = ((shx + d.smax) * d.S + (shy + d.smax)) * d.S + (shz + d.smax);
-        const int cell = s.cell_begin + (wz * s.nc[1] + wy) * s.nc[0] + wx;
-        const int c0 = d.cell_start[cell], c1 = d.cell_start[cell + 1];
+        const int c0 = d.cell_start[rowcell + wx0], c1 = d.cell_start[rowcell + wx0 + len];
         for (int base = c0; base < c1; base += 32) {
           const int p = base + lane;
           bool ok = false;
           int j = 0;
           double r2 = 0.0;
+          double4 xj = make_double4(0, 0, 0, 0);
           if (p < c1) {
             j = d.cell_atoms[p];
+            xj = d.xs[p];
             if (!(j == i && sidx == center)) {
               double dv[3];
-              pair_dvec(d, s, i, j, sidx, dv);
+              pair_dvec_x(d, s, i, j, sidx, xi, xj, dv);
               r2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
               ok = r2 <= rc2;
             }
           }
           const unsigned m = __ballot_sync(0xffffffffu, ok);
+          const bool nr = ok && r2 <= d.rnear2;
+          const unsigned mn = __ballot_sync(0xffffffffu, nr);
+          if (nr) {
+            const int posn = count_near + __popc(mn & lt);
+            if (posn < d.ncap_near)
+              d.near[static_cast<size_t>(i) * d.ncap_near + posn] = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
+          }
+          count_near += __popc(mn);
           if (ok) {
             const int pos = count + __popc(m & lt);
             if (pos < d.ncap) {
-              const size_t e = static_cast<size_t>(i) * d.ncap + pos;
-              d.nbr[e] = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
+              d.nbr[rowbase + pos] = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
               const double r = sqrt(r2);
               double h = 0.0;
               if (r <= qp.swb) {
                 double Tap, dTap;
                 taper_horner(qp.tap, r, Tap, dTap);
-                const double shld = pow(gi * ff.sb[d.type[j] * SB_N + SB_GAMMA], -1.5);
-                h = Tap * 14.4 / cbrt(r * r * r + shld);
+                h = Tap * 14.4 / cbrt(r * r * r + shld_i[static_cast<int>(xj.w)]);
               }
-              d.hval[e] = h;
+              d.hval[rowbase + pos] = h;
             }
           }
           count += __popc(m);
@@ -131,9 +154,14 @@ __global__ void k_neighbors(Dev d, DevFF ff, QeqParams qp) {
   }
   if (lane == 0) {
     d.nbr_cnt[i] = count;
+    d.near_cnt[i] = count_near;
     if (count > d.ncap) {
       atomicOr(d.status, ST_NBR_OVERFLOW);
       atomicMax(d.status + 1, count);
+    }
+    if (count_near > d.ncap_near) {
+      atomicOr(d.status, ST_NEAR_OVERFLOW);
+      atomicMax(d.status + 3, count_near);
     }
   }
 }
@@ -175,20 +203,21 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     const float dx = static_cast<float>(dvd[0]), dy = static_cast<float>(dvd[1]), dz = static_cast<float>(dvd[2]);
     const float r = static_cast<float>(sqrt(dvd[0] * dvd[0] + dvd[1] * dvd[1] + dvd[2] * dvd[2]));
     const int tj = d.type[j];
-    const double* tb = ff.tb + (static_cast<size_t>(ti) * ff.nt + tj) * TB_N;
+    const float* pp = ff.nbf + (static_cast<size_t>(ti) * ff.nt + tj) * 12;
     float Tap, dTap;
     taper_stable_f(swa, swb, r, Tap, dTap);
-    const float alpha = static_cast<float>(tb[TB_ALPHA]), D = static_cast<float>(tb[TB_D]), r_vdW = static_cast<float>(tb[TB_R_VDW]);
+    const float alpha = pp[0], D = pp[1], r_vdW = pp[2];
     float e_vdW = 0.f, CEvd;
     if (ff.vdw_type == 1 || ff.vdw_type == 3) {
       const float powr_vdW1 = powf(r, p_vdW1);
-      const float powgi_vdW1 = powf(1.f / static_cast<float>(tb[TB_GAMMA_W]), p_vdW1);
-      const float fn13 = powf(powr_vdW1 + powgi_vdW1, p_vdW1i);
+      const float sum = powr_vdW1 + pp[3];
+      const float fn13 = powf(sum, p_vdW1i);
       const float exp1 = __expf(alpha * (1.f - fn13 / r_vdW));
       const float exp2 = __expf(0.5f * alpha * (1.f - fn13 / r_vdW));
       const float evd = D * (exp1 - 2.f * exp2);
       e_vdW += Tap * evd;
-      const float dfn13 = powf(powr_vdW1 + powgi_vdW1, p_vdW1i - 1.f) * powf(r, p_vdW1 - 2.f);
+      // (sum)^(1/p - 1) r^(p - 2) = fn13 / sum * powr / r^2
+      const float dfn13 = (fn13 / sum) * (powr_vdW1 / (r * r));
       CEvd = dTap * evd - Tap * D * (alpha / r_vdW) * (exp1 - exp2) * dfn13;
     } else {
       const float exp1 = __expf(alpha * (1.f - r / r_vdW));
@@ -198,21 +227,21 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
       CEvd = dTap * evd - Tap * D * (alpha / r_vdW) * (exp1 - exp2) / r;
     }
     if (ff.vdw_type == 2 || ff.vdw_type == 3) {
-      const float ecore = static_cast<float>(tb[TB_ECORE]), acore = static_cast<float>(tb[TB_ACORE]), rcore = static_cast<float>(tb[TB_RCORE]);
+      const float ecore = pp[4], acore = pp[5], rcore = pp[6];
       const float e_core = ecore * __expf(acore * (1.f - (r / rcore)));
       e_vdW += Tap * e_core;
       const float de_core = -(acore / rcore) * e_core;
       CEvd += dTap * e_core + Tap * de_core / r;
       if (ff.lg) {
-        const float r5 = powf(r, 5.f), r6 = powf(r, 6.f), re6 = powf(static_cast<float>(tb[TB_LGRE]), 6.f);
-        const float e_lg = -(static_cast<float>(tb[TB_LGCIJ]) / (r6 + re6));
+        const float r2f = r * r, r4 = r2f * r2f, r5 = r4 * r, r6 = r4 * r2f, re6 = pp[9];
+        const float e_lg = -(pp[8] / (r6 + re6));
         e_vdW += Tap * e_lg;
         const float de_lg = -6.f * e_lg * r5 / (r6 + re6);
         CEvd += dTap * e_lg + Tap * de_lg / r;
       }
     }
     const float qj = static_cast<float>(d.q[j]);
-    const float dr3gamij_1 = r * r * r + static_cast<float>(tb[TB_GAMMA]);
+    const float dr3gamij_1 = r * r * r + pp[7];
     const float dr3gamij_3 = cbrtf(dr3gamij_1);
     const float e_ele = 332.06371f * qi * qj * (Tap / dr3gamij_3);
     const float CEclmb = 332.06371f * qi * qj * (dTap - Tap * r / dr3gamij_1) / dr3gamij_3;
@@ -260,6 +289,7 @@ __device__ inline double2 row_mv(const Dev& d, int i, double eta, const double2*
   const int lane = threadIdx.x & 31;
   double ys = 0.0, yt = 0.0;
   const size_t base = static_cast<size_t>(i) * d.ncap;
+#pragma unroll 4
   for (int e = lane; e < cnt; e += 32) {
     const double h = d.hval[base + e];
     const int j = static_cast<int>(d.nbr[base + e] & d.amask);
@@ -291,16 +321,23 @@ __device__ inline void block_partials(const double* v, double* out, double* sh) 
   __syncthreads();
 }
 
-// sum of the per-block partials in block order (every block computes the same value)
+// Sum of the per-block partials, identical in every block: each thread loads a strided subset in order, then a
+// fixed-shape shuffle tree and a fixed-order sum over the warps (the tree depends only on gridDim and blockDim).
 template <int NV>
 __device__ inline void grid_totals(const double* part, int nblocks, double* tot, double* sh) {
-  if (threadIdx.x < NV) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = 0; k < NV; ++k) {
     double t = 0.0;
-    for (int b = 0; b < nblocks; ++b) t += part[b * NV + threadIdx.x];
-    sh[threadIdx.x] = t;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) t += part[b * NV + k];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) sh[wid * NV + k] = t;
   }
   __syncthreads();
-  for (int k = 0; k < NV; ++k) tot[k] = sh[k];
+  for (int k = 0; k < NV; ++k) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += sh[w * NV + k];
+    tot[k] = t;
+  }
   __syncthreads();
 }
 
@@ -309,10 +346,10 @@ __device__ inline void grid_totals(const double* part, int nblocks, double* tot,
 // sqrt(r.M^-1 r)/|b| <= tol with at most imax-1 iterations. Then calculate_Q: q = s - (sum s / sum t) t.
 // Rows are distributed over all warps of the grid; reductions are fixed-order (per-block partials summed in block
 // order), so the result is bitwise reproducible. Only grid.sync() waits; the kernel is launched cooperatively.
-__global__ void k_cg_grid(Dev d, CgArgs a) {
+__global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   cg::grid_group g = cg::this_grid();
   __shared__ double sh[64 * 4];
-  __shared__ double tot_sh[8];
+  __shared__ double tot_sh[64 * 4];
   const int wpb = blockDim.x >> 5;
   const int gw = blockIdx.x * wpb + (threadIdx.x >> 5);
   const int nwarps = gridDim.x * wpb;
@@ -572,23 +609,20 @@ __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y) {
 }
 
 // ------------------------------------------------------------------------------------------------ energy sums
-// Per system, per term: fixed-order sum over the system's atoms (one block per system).
+// Per system, per term: fixed-order sum over the system's atoms (one block per system and term).
 __global__ void k_energy_sum(Dev d, double* out) {
-  const int sidx = blockIdx.x;
+  const int sidx = blockIdx.x, t = blockIdx.y;
   const SysInfo s = d.sys[sidx];
   __shared__ double sh[256];
-  for (int t = 0; t < kTerms; ++t) {
-    double v = 0.0;
-    for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) v += d.eatom[static_cast<size_t>(s.begin + r) * kTerms + t];
-    sh[threadIdx.x] = v;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-      if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) out[sidx * kTerms + t] = sh[0];
+  double v = 0.0;
+  for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) v += d.eatom[static_cast<size_t>(s.begin + r) * kTerms + t];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
+  if (threadIdx.x == 0) out[sidx * kTerms + t] = sh[0];
 }
 
 }  // namespace rx

@@ -29,7 +29,7 @@ STATUS = {0: "ok", 1: "invalid", 2: "ffield", 3: "capacity", 4: "cuda", 5: "not_
 EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_forcefield_dump", "rx_forcefield_params",
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
-           "rx_get_velocities", "rx_md_run", "rx_stream", "rx_set_timing", "rx_phase_times"]
+           "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -64,7 +64,7 @@ def load():
         "rx_compute": (_I, [_V, _I, _V, _V, _V, _V]),
         "rx_md_setup": (_I, [_V, _V, _D, _D, _D, _D, _I]), "rx_set_velocities": (_I, [_V, _V]),
         "rx_get_velocities": (_I, [_V, _V]), "rx_md_run": (_I, [_V, _I, _V, _V]),
-        "rx_stream": (_V, [_V]), "rx_set_timing": (_I, [_V, _I]),
+        "rx_stream": (_V, [_V]), "rx_set_timing": (_I, [_V, _I]), "rx_kernel_launches": (ctypes.c_int64, [_V]),
         "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
     }
     for name, (res, args) in sig.items():
@@ -213,6 +213,9 @@ class Engine:
         t = np.zeros(self.nsys)
         self._check(self.lib.rx_md_run(self.h, nsteps, _p(e), _p(t)))
         return {"e": e.reshape(self.nsys, 13), "T": t}
+
+    def kernel_launches(self):
+        return int(self.lib.rx_kernel_launches(self.h))
 
     def stream(self):
         return self.lib.rx_stream(self.h)
