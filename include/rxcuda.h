@@ -95,6 +95,26 @@ int rx_get_velocities(rx_context* ctx, double* v);
 /* nsteps steps of every system; energies (13*nsys, last step) and temperature (nsys) may be NULL */
 int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature);
 
+/* Charge equilibration without any device allocation (this entry point has no counterpart in the reference).
+ * For callers that cannot let a library call cudaMalloc: codes that own all device memory through their own pooled
+ * allocator or fixed budget, and codes running where an allocation and its implicit device synchronisation are not
+ * allowed. It solves (diag(eta) + H) s = -chi and (diag(eta) + H) t = -1 with the engine's Jacobi-preconditioned CG
+ * (the stopping rule of fix qeq/reaxff: sqrt(r.M^-1 r)/|b| <= tol, at most imax - 1 iterations) and writes
+ * q = s - (sum s / sum t) t. Every pointer is a device pointer on the current device, owned by the caller:
+ * H as CSR (row_start[n+1], col[nnz], val[nnz]; every periodic image of a pair summed into its entry), eta[n] and
+ * chi[n] per atom, s[n] and t[n] the initial guesses on entry and the solutions on return, q[n] the charges,
+ * iters[2] and rel[2] (s then t; may be NULL). The call is asynchronous on `stream` (a cudaStream_t, NULL = default).
+ * The CG work vectors live in one fixed device array of RX_QEQ_STATIC_MAX_ATOMS * 8 doubles (2 MiB) that every GPU
+ * loading the library holds until the process exits; larger n is rejected with RX_ERR_INVALID. All calls share that
+ * array: calls whose kernels overlap on the GPU (other streams, other threads) race, so serialise them. The array keeps
+ * the last call's contents; nothing in it needs to start at zero, since every work vector is written before it is
+ * read. The first call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current, so make that first call before any stream capture. err/errlen (may be NULL) receive a message. */
+#define RX_QEQ_STATIC_MAX_ATOMS 32768
+int rx_qeq_solve_static(int n, const int* row_start, const int* col, const double* val, const double* eta, const double* chi,
+                        double* s, double* t, double* q, double tol, int imax, int* iters, double* rel, void* stream,
+                        char* err, int errlen);
+
 /* Number of this engine's own kernels launched on the context so far (library kernels, e.g. the radix sort of the cell
  * lists, are not counted). */
 int64_t rx_kernel_launches(const rx_context* ctx);

@@ -15,7 +15,7 @@ REPO = PKG.parent
 SRC = PKG / "csrc"
 OUT = PKG / "librxcuda.so"
 BUILD = REPO / "_build"
-SOURCES = ["engine.cu", "kernels_nb.cu", "kernels_bonded.cu", "md_kernels.cu", "ffield.cpp"]
+SOURCES = ["engine.cu", "kernels_nb.cu", "kernels_bonded.cu", "md_kernels.cu", "ffield.cpp", "noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-I" + str(REPO / "include")]

@@ -29,7 +29,8 @@ STATUS = {0: "ok", 1: "invalid", 2: "ffield", 3: "capacity", 4: "cuda", 5: "not_
 EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_forcefield_dump", "rx_forcefield_params",
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
-           "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times"]
+           "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
+           "rx_qeq_solve_static"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -66,6 +67,7 @@ def load():
         "rx_get_velocities": (_I, [_V, _V]), "rx_md_run": (_I, [_V, _I, _V, _V]),
         "rx_stream": (_V, [_V]), "rx_set_timing": (_I, [_V, _I]), "rx_kernel_launches": (ctypes.c_int64, [_V]),
         "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
+        "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
