@@ -41,6 +41,8 @@ struct SysInfo {
   int cell_begin;
   int range[3];   // cell search range per direction
   int shift_base; // first entry of this system's lattice-shift table (S^3 entries)
+  double h[3];    // distances between opposite faces (heights) along each lattice direction
+  int ortho;      // lattice vectors mutually orthogonal
 };
 
 struct DevFF {

@@ -344,6 +344,11 @@ struct Context {
       const double h[3] = {det / std::sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]), det / std::sqrt(ca[0] * ca[0] + ca[1] * ca[1] + ca[2] * ca[2]),
                            det / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2])};
       long long ncell = 1;
+      for (int k = 0; k < 3; ++k) si.h[k] = h[k];
+      {
+        auto dotp = [](const double* u, const double* w) { return u[0] * w[0] + u[1] * w[1] + u[2] * w[2]; };
+        si.ortho = (dotp(a, b) == 0.0 && dotp(a, c) == 0.0 && dotp(b, c) == 0.0) ? 1 : 0;
+      }
       for (int k = 0; k < 3; ++k) {
         int n = static_cast<int>(std::floor(h[k] * 2.0 / rc));
         n = std::max(1, std::min(n, 512));

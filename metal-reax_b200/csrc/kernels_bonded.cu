@@ -551,35 +551,49 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
 }
 
 // Hydrogen bonds (src/cpu/bonded.cpp:654-715) of one triple: donor bond slot bi of hydrogen j, acceptor k at the
-// canonical vector dvjk (x_k - x_j) and distance r_jk. Returns false when a gate of the reference rejects it.
-struct HbOut { double e, CEhb1, CEhb2, CEhb3, dti[3], dtj[3], dtk[3]; };
+// canonical vector dvjk (x_k - x_j) and distance r_jk. Every gate of the reference is taken in FP64 (types, tags,
+// BO >= HB_THRESHOLD, parameters present, r_jk <= hbond_cut by the caller); the term itself is FP32. sin^4(theta/2)
+// is formed as ((1 - cos theta) / 2)^2, the same quantity as the reference's sin(acos(c) / 2)^4.
+struct HbOut { float e, CEhb1, CEhb2, CEhb3, dti[3], dtj[3], dtk[3]; };
 __device__ inline bool hbond_triple(const Dev& d, const DevFF& ff, int tj, int type_k, long long tag_k, size_t bi,
-                                    const double* dvjk, double r_jk, HbOut& o) {
+                                    const float* vk, float r_jk, HbOut& o) {
   const int ia = static_cast<int>(d.bcode[bi] & d.amask);
   const int type_i = d.type[ia];
   if (static_cast<int>(SBp(ff, type_i)[SB_P_HBOND]) != 2) return false;
-  const double BO = d.bBO[bi].x;
-  if (!(BO >= kHbThreshold)) return false;
+  const double BOd = d.bBO[bi].x;
+  if (!(BOd >= kHbThreshold)) return false;
   if (d.tag[ia] == tag_k) return false;
   const size_t key = (static_cast<size_t>(type_i) * ff.nt + tj) * ff.nt + type_k;
   if (!ff.hb_on[key]) return false;
   const double* hb = ff.hb + key * HB_NFIELDS;
   if (hb[HB_R0] <= 0.0) return false;
+  const float r0 = static_cast<float>(hb[HB_R0]), p1 = static_cast<float>(hb[HB_P_HB1]);
+  const float p2 = static_cast<float>(hb[HB_P_HB2]), p3 = static_cast<float>(hb[HB_P_HB3]);
+  const float BO = static_cast<float>(BOd);
   const double4 dvi = d.bdv[bi];
-  const double vi[3] = {dvi.x, dvi.y, dvi.z};
-  double theta, cos_theta;
-  calc_theta(vi, dvi.w, dvjk, r_jk, theta, cos_theta);
-  calc_dcos(vi, dvi.w, dvjk, r_jk, o.dti, o.dtj, o.dtk);
-  const double sin_theta2 = sin(theta / 2.0);
-  double sin_xhz4 = sin_theta2 * sin_theta2;
-  sin_xhz4 *= sin_xhz4;
-  const double cos_xhz1 = (1.0 - cos_theta);
-  const double exp_hb2 = exp(-hb[HB_P_HB2] * BO);
-  const double exp_hb3 = exp(-hb[HB_P_HB3] * (hb[HB_R0] / r_jk + r_jk / hb[HB_R0] - 2.0));
-  o.e = hb[HB_P_HB1] * (1.0 - exp_hb2) * exp_hb3 * sin_xhz4;
-  o.CEhb1 = hb[HB_P_HB1] * hb[HB_P_HB2] * exp_hb2 * exp_hb3 * sin_xhz4;
-  o.CEhb2 = -hb[HB_P_HB1] / 2.0 * (1.0 - exp_hb2) * exp_hb3 * cos_xhz1;
-  o.CEhb3 = -hb[HB_P_HB3] * (-hb[HB_R0] / (r_jk * r_jk) + 1.0 / hb[HB_R0]) * o.e;
+  const float vi[3] = {static_cast<float>(dvi.x), static_cast<float>(dvi.y), static_cast<float>(dvi.z)};
+  const float d_ji = static_cast<float>(dvi.w);
+  // reaxff_valence_angles.cpp:36-70 (calculate_theta / calculate_dcos_theta) in FP32
+  const float inv = 1.0f / (d_ji * r_jk);
+  const float dotv = vi[0] * vk[0] + vi[1] * vk[1] + vi[2] * vk[2];
+  float c = dotv * inv;
+  c = fminf(1.0f, fmaxf(-1.0f, c));
+  const float Cdot = dotv * inv * inv * inv;
+  const float sq_ji = d_ji * d_ji, sq_jk = r_jk * r_jk;
+  for (int t = 0; t < 3; ++t) {
+    o.dti[t] = vk[t] * inv - Cdot * sq_jk * vi[t];
+    o.dtj[t] = -(vk[t] + vi[t]) * inv + Cdot * (sq_jk * vi[t] + sq_ji * vk[t]);
+    o.dtk[t] = vi[t] * inv - Cdot * sq_ji * vk[t];
+  }
+  const float half = 0.5f * (1.0f - c);
+  const float sin_xhz4 = half * half;
+  const float cos_xhz1 = 1.0f - c;
+  const float exp_hb2 = __expf(-p2 * BO);
+  const float exp_hb3 = __expf(-p3 * (r0 / r_jk + r_jk / r0 - 2.0f));
+  o.e = p1 * (1.0f - exp_hb2) * exp_hb3 * sin_xhz4;
+  o.CEhb1 = p1 * p2 * exp_hb2 * exp_hb3 * sin_xhz4;
+  o.CEhb2 = -p1 / 2.0f * (1.0f - exp_hb2) * exp_hb3 * cos_xhz1;
+  o.CEhb3 = -p3 * (-r0 / (r_jk * r_jk) + 1.0f / r0) * o.e;
   return true;
 }
 
@@ -624,17 +638,20 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
       pair_dvec(d, s, j, ka, static_cast<int>(code >> d.abits), dvjk);
       const double r2 = dot3(dvjk, dvjk);
       if (!(r2 <= hc2)) continue;
-      const double r_jk = sqrt(r2);
-      if (!(r_jk <= ctl.hbond_cut)) continue;
+      const double r_jkd = sqrt(r2);
+      if (!(r_jkd <= ctl.hbond_cut)) continue;
+      const float vk[3] = {static_cast<float>(dvjk[0]), static_cast<float>(dvjk[1]), static_cast<float>(dvjk[2])};
+      const float r_jk = static_cast<float>(r_jkd);
       HbOut o;
-      if (!hbond_triple(d, ff, tj, type_k, d.tag[ka], bi, dvjk, r_jk, o)) continue;
+      if (!hbond_triple(d, ff, tj, type_k, d.tag[ka], bi, vk, r_jk, o)) continue;
       ++ntrip;
       e += o.e;
       c1 += o.CEhb1;
       fi0 += o.CEhb2 * o.dti[0]; fi1 += o.CEhb2 * o.dti[1]; fi2 += o.CEhb2 * o.dti[2];
-      fj0 += o.CEhb2 * o.dtj[0] + -o.CEhb3 / r_jk * dvjk[0];
-      fj1 += o.CEhb2 * o.dtj[1] + -o.CEhb3 / r_jk * dvjk[1];
-      fj2 += o.CEhb2 * o.dtj[2] + -o.CEhb3 / r_jk * dvjk[2];
+      const float c3 = -o.CEhb3 / r_jk;
+      fj0 += o.CEhb2 * o.dtj[0] + c3 * vk[0];
+      fj1 += o.CEhb2 * o.dtj[1] + c3 * vk[1];
+      fj2 += o.CEhb2 * o.dtj[2] + c3 * vk[2];
     }
     c1 = warp_sum(c1); fi0 = warp_sum(fi0); fi1 = warp_sum(fi1); fi2 = warp_sum(fi2);
     if (lane == 0) {
@@ -681,15 +698,18 @@ __global__ void __launch_bounds__(128) k_hbond_acceptor(Dev d, DevFF ff, DevCtl 
     const double dvjk[3] = {-dkh[0], -dkh[1], -dkh[2]};
     const double r2 = dot3(dvjk, dvjk);
     if (!(r2 <= hc2)) continue;
-    const double r_jk = sqrt(r2);
-    if (!(r_jk <= ctl.hbond_cut)) continue;
+    const double r_jkd = sqrt(r2);
+    if (!(r_jkd <= ctl.hbond_cut)) continue;
+    const float vk[3] = {static_cast<float>(dvjk[0]), static_cast<float>(dvjk[1]), static_cast<float>(dvjk[2])};
+    const float r_jk = static_cast<float>(r_jkd);
     const int nb = min(d.bcnt[h], d.bcap);
     for (int pi = 0; pi < nb; ++pi) {
       HbOut o;
-      if (!hbond_triple(d, ff, tj, type_k, tag_k, static_cast<size_t>(h) * d.bcap + pi, dvjk, r_jk, o)) continue;
-      f0 += o.CEhb2 * o.dtk[0] + o.CEhb3 / r_jk * dvjk[0];
-      f1 += o.CEhb2 * o.dtk[1] + o.CEhb3 / r_jk * dvjk[1];
-      f2 += o.CEhb2 * o.dtk[2] + o.CEhb3 / r_jk * dvjk[2];
+      if (!hbond_triple(d, ff, tj, type_k, tag_k, static_cast<size_t>(h) * d.bcap + pi, vk, r_jk, o)) continue;
+      const float c3 = o.CEhb3 / r_jk;
+      f0 += o.CEhb2 * o.dtk[0] + c3 * vk[0];
+      f1 += o.CEhb2 * o.dtk[1] + c3 * vk[1];
+      f2 += o.CEhb2 * o.dtk[2] + c3 * vk[2];
     }
   }
   f0 = warp_sum(f0); f1 = warp_sum(f1); f2 = warp_sum(f2);

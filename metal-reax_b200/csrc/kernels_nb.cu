@@ -90,13 +90,36 @@ __global__ void __launch_bounds__(128) k_neighbors(Dev d, DevFF ff, QeqParams qp
   const unsigned lt = (1u << lane) - 1u;
   const int center = (d.S * d.S * d.S - 1) / 2;
   const size_t rowbase = static_cast<size_t>(i) * d.ncap;
+  // fractional coordinates of i: lower bounds of the distance to a cell slab prune whole runs and clip the x range
+  double fi[3];
+  for (int k = 0; k < 3; ++k)
+    fi[k] = s.R[3 * k] * (xi.x - s.origin[0]) + s.R[3 * k + 1] * (xi.y - s.origin[1]) + s.R[3 * k + 2] * (xi.z - s.origin[2]);
+  const double rc = ff.nonb_cut * (1.0 + 1e-9) + 1e-9;
+  auto slab_gap = [&](int k, int c) {   // distance from i to the slab of cell index c (unwrapped) along direction k
+    const double lo = static_cast<double>(c) / s.nc[k], hi = static_cast<double>(c + 1) / s.nc[k];
+    const double g = fmax(0.0, fmax(lo - fi[k], fi[k] - hi));
+    return fmax(0.0, g * s.h[k] - 1e-9 * s.h[k]);
+  };
   for (int oz = -s.range[2]; oz <= s.range[2]; ++oz) {
     const int zz = cz + oz, shz = floor_div(zz, s.nc[2]), wz = zz - shz * s.nc[2];
+    const double gz = slab_gap(2, zz);
+    if (gz > rc) continue;
     for (int oy = -s.range[1]; oy <= s.range[1]; ++oy) {
       const int yy = cy + oy, shy = floor_div(yy, s.nc[1]), wy = yy - shy * s.nc[1];
+      const double gy = slab_gap(1, yy);
+      double rx;
+      if (s.ortho) {
+        const double g2 = gy * gy + gz * gz;
+        if (g2 > rc * rc) continue;
+        rx = sqrt(rc * rc - g2);
+      } else {
+        if (gy > rc) continue;
+        rx = rc;
+      }
       const int rowcell = s.cell_begin + (wz * s.nc[1] + wy) * s.nc[0];
-      int xx = cx - s.range[0];
-      const int xend = cx + s.range[0];
+      const double fx_lo = fi[0] - rx / s.h[0], fx_hi = fi[0] + rx / s.h[0];
+      int xx = max(cx - s.range[0], static_cast<int>(floor(fx_lo * s.nc[0])));
+      const int xend = min(cx + s.range[0], static_cast<int>(floor(fx_hi * s.nc[0])));
       while (xx <= xend) {
         const int shx = floor_div(xx, s.nc[0]);
         const int wx0 = xx - shx * s.nc[0];
@@ -142,7 +165,10 @@ __global__ void __launch_bounds__(128) k_neighbors(Dev d, DevFF ff, QeqParams qp
               if (r <= qp.swb) {
                 double Tap, dTap;
                 taper_horner(qp.tap, r, Tap, dTap);
-                h = Tap * 14.4 / cbrt(r * r * r + shld_i[static_cast<int>(xj.w)]);
+                const double a3 = r * r * r + shld_i[static_cast<int>(xj.w)];
+                double y = static_cast<double>(cbrtf(static_cast<float>(a3)));
+                y = y - (y * y * y - a3) / (3.0 * y * y);   // one Newton step: relative error ~1e-14
+                h = Tap * 14.4 / y;
               }
               d.hval[rowbase + pos] = h;
             }

@@ -6,7 +6,8 @@ Bars (the reference's own acceptance of an FP32 GPU engine against cpu64, tolera
   force   max |dF| <= 0.05, RMS <= 5e-3 kcal/mol/A
   census  every discrete decision (bonds, angle sets, torsions, H-bonds, non-bonded pairs, SBO branch, lone-pair
           truncation) identical atom by atom
-Tighter bars for the FP64 bond-order terms: every bonded term within 1e-7 relative (max(1, |E|)).
+Tighter bars for the terms computed in FP64 (bond, over/under, lone pair, valence, penalty, coalition, torsion,
+conjugation): within 1e-7 relative (max(1, |E|)); the FP32 H-bond term within 2e-5 relative.
 """
 import numpy as np
 import pytest
@@ -16,7 +17,8 @@ from helpers import (C3_ENERGY_PER_ATOM, C3_FORCE_MAX, C3_FORCE_RMS, fixed_charg
 
 pytestmark = pytest.mark.gpu
 
-BONDED = slice(0, 10)
+FP64_TERMS = [0, 1, 2, 3, 4, 5, 6, 8, 9]
+HBOND = 7
 
 
 @pytest.fixture(scope="module")
@@ -45,9 +47,10 @@ def test_single_point_matches_oracle(engine, oracle, idx):
     out = engine.compute(census=True, counts=True)
     e, e_ref = out["e"][0], ref["e"]
     n = len(s["type"])
-    # FP64 bond-order terms: tight
-    rel = np.abs(e[BONDED] - e_ref[BONDED]) / np.maximum(1.0, np.abs(e_ref[BONDED]))
-    assert rel.max() <= 1e-7, (s["name"], e[BONDED], e_ref[BONDED])
+    # FP64 bond-order terms: tight; FP32 H-bonds: FP32 level
+    rel = np.abs(e[FP64_TERMS] - e_ref[FP64_TERMS]) / np.maximum(1.0, np.abs(e_ref[FP64_TERMS]))
+    assert rel.max() <= 1e-7, (s["name"], e[FP64_TERMS], e_ref[FP64_TERMS])
+    assert abs(e[HBOND] - e_ref[HBOND]) <= 2e-5 * max(1.0, abs(e_ref[HBOND])), (s["name"], e[HBOND], e_ref[HBOND])
     # total energy per atom (C3)
     assert abs(e.sum() - e_ref.sum()) / n <= C3_ENERGY_PER_ATOM, (s["name"], e, e_ref)
     fmax, frms = force_metrics(ref["grad"], out["grad"])
