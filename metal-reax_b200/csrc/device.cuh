@@ -165,6 +165,11 @@ __device__ inline void pair_dvec(const Dev& d, const SysInfo& s, int i, int j, i
   pair_dvec_x(d, s, i, j, sidx, d.x[i], d.x[j], dv);
 }
 
+// A list of this evaluation overflowed (the host grows it and repeats the evaluation): later kernels skip their work.
+__device__ inline bool lists_failed(const Dev& d) {
+  return (*reinterpret_cast<volatile const int*>(d.status) & (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW | ST_BOND_OVERFLOW | ST_SHIFT_RANGE)) != 0;
+}
+
 __device__ inline double safe_exp(double v) { return exp(v > 700.0 ? 700.0 : v); }
 __device__ inline float safe_expf(float v) { return __expf(v > 40.f ? 40.f : v); }
 

@@ -415,7 +415,7 @@ struct Context {
     const double rn = std::max(ctl.bond_cut, ctl.hbond_cut);
     const int want_near = static_cast<int>(std::ceil((4.0 / 3.0 * M_PI * rn * rn * rn * max_density * 1.3 + 32) / 32.0)) * 32;
     if (ncap_near < want_near) ncap_near = want_near;
-    if (bcap < 8) bcap = 8;
+    if (bcap < 16) bcap = 16;
     alloc_atoms();
     alloc_lists();
   }
@@ -516,7 +516,7 @@ struct Context {
     CgArgs a = cg_args();
     ++launches;
     k_qeq_prepare<<<blocks(na, 256), 256, 0, stream>>>(d, dff, a, s_hist.p, t_hist.p);
-    if (nsys == 1 && na > 4096) {
+    if (nsys == 1) {   // one system: all SMs on it (a single block per system is latency-bound)
       const int threads = 256;
       int per_sm = 0;
       RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_grid, threads, 0));

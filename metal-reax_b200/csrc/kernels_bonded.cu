@@ -68,6 +68,7 @@ __device__ inline void add3(double4& a, double s, const double* v) { a.x += s * 
 // One warp per atom over its neighbor row: entries within bond_cut whose uncorrected bond order passes bo_cut
 // (terms::bo_prime, terms.hpp:50-56; gate src/cpu/bonded.cpp:130) become bond slots, in row order.
 __global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl) {
+  if (lists_failed(d)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
@@ -138,6 +139,7 @@ __global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl) {
 }
 
 __global__ void k_bond_sym(Dev d) {
+  if (lists_failed(d)) return;
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= static_cast<long long>(d.na) * d.bcap) return;
   const int a = static_cast<int>(t / d.bcap), k = static_cast<int>(t % d.bcap);
@@ -160,6 +162,7 @@ __global__ void k_bond_sym(Dev d) {
 // terms::bo_correct (include/reaxmetal/terms.hpp:66-132) for every slot, the slot's atom as "i". The corrected bond
 // orders are symmetric in (i, j) bit for bit, so both slots of a bond hold the same values.
 __global__ void k_bo_correct(Dev d, DevFF ff) {
+  if (lists_failed(d)) return;
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= static_cast<long long>(d.na) * d.bcap) return;
   const int a = static_cast<int>(t / d.bcap), k = static_cast<int>(t % d.bcap);
@@ -241,6 +244,7 @@ __global__ void k_bo_correct(Dev d, DevFF ff) {
 }
 
 __global__ void k_atom_quantities(Dev d, DevFF ff) {
+  if (lists_failed(d)) return;
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= d.na) return;
   const int t = d.type[a];
@@ -274,6 +278,7 @@ __global__ void k_atom_quantities(Dev d, DevFF ff) {
 // (:255-281), over/under coordination (:282-318), valence angle + penalty + coalition centred at j (:321-474). Coefficients of j's own bonds go to j's slots; contributions to a bond partner
 // (its CdDelta, its gradient) go to the slot naming it, for the partner to gather.
 __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
+  if (lists_failed(d)) return;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.na) return;
   const int tj = d.type[j];
@@ -601,6 +606,7 @@ __device__ inline bool hbond_triple(const Dev& d, const DevFF& ff, int tj, int t
 // (p_hbond = 2, r <= hbond_cut). Energy, the gradient of j and the coefficient / gradient of the donor bond are
 // reduced over the warp in fixed order; the donor's share goes to j's slot for the donor to gather.
 __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
+  if (lists_failed(d)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
@@ -677,6 +683,7 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
 // (one warp per acceptor, lanes over its near row), with bitwise the same inputs (the hydrogen's bond slot, the
 // canonical j -> k vector), so the acceptor gathers its own gradient without writing to any other atom.
 __global__ void __launch_bounds__(128) k_hbond_acceptor(Dev d, DevFF ff, DevCtl ctl) {
+  if (lists_failed(d)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
@@ -726,6 +733,7 @@ __global__ void __launch_bounds__(128) k_hbond_acceptor(Dev d, DevFF ff, DevCtl 
 // (ti, tj, tk, tl), BO_kl > thb_cut, BO_ij BO_jk BO_kl > thb_cut). Contributions to the bond k-l and to the atom l
 // are written to Tl[(slot j->k) * bcap + (position of l in k's slots)], gathered by k in k_fold.
 __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
+  if (lists_failed(d)) return;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.na) return;
   const int type_j = d.type[j];
@@ -927,6 +935,7 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
 // k folds the torsion contributions written for its bonds (Tl of every central bond j -> k) into its own slots, and
 // sums its total CdDelta: own part + the parts its partners wrote into their slots naming k.
 __global__ void k_fold(Dev d) {
+  if (lists_failed(d)) return;
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= d.na) return;
   const int nb = min(d.bcnt[a], d.bcap);
@@ -953,6 +962,7 @@ __global__ void k_fold(Dev d) {
 // dBOp(a->p), of dln_BOp_pi/pi2(a->p) and of dDeltap_self[a]; W[a] = sum of the dDeltap_self coefficients, which the
 // bond partners apply to their own dBOp in k_force_final.
 __global__ void k_dbond(Dev d) {
+  if (lists_failed(d)) return;
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= d.na) return;
   const int nb = min(d.bcnt[a], d.bcap);
@@ -982,6 +992,7 @@ __global__ void k_dbond(Dev d) {
 }
 
 __global__ void k_force_final(Dev d) {
+  if (lists_failed(d)) return;
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= d.na) return;
   const int nb = min(d.bcnt[a], d.bcap);

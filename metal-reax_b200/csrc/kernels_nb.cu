@@ -206,6 +206,7 @@ __device__ inline void taper_stable_f(float swa, float swb, float r, float& Tap,
 // at i if it is owned-owned with j > i, or a periodic image with tag_i < tag_j or, for an image of i itself, the
 // positive direction; each counted entry contributes its full pair energy (terms::nonbonded_pair, terms.hpp:282-323).
 __global__ void k_nonbonded(Dev d, DevFF ff) {
+  if (lists_failed(d)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
