@@ -65,6 +65,13 @@ int rx_set_control(rx_context* ctx, double bond_cut, double hbond_cut, double th
 int rx_set_systems(rx_context* ctx, int nsys, const int* natoms, const double* origin, const double* box, const int* periodic,
                    const int* type, const int64_t* tag);
 int rx_num_atoms(const rx_context* ctx);
+
+/* Per-atom list capacities: neighbor-row entries, bond slots, near-row entries (in that order). The engine sizes them
+ * from the densest system at rx_set_systems and grows them on overflow, repeating the evaluation (neighbor.cpp:362-374);
+ * rx_set_capacities replaces the current values (nbr and near are rounded up to multiples of 32), e.g. to start a
+ * serving context from capacities measured earlier. Values below 1 are rejected with RX_ERR_INVALID. */
+int rx_set_capacities(rx_context* ctx, int nbr, int bonds, int near_entries);
+int rx_get_capacities(const rx_context* ctx, int* out3);
 int rx_set_positions(rx_context* ctx, const double* x);   /* x[3*NA] */
 int rx_get_positions(rx_context* ctx, double* x);         /* positions as held (wrapped into the primary cell) */
 int rx_set_charges(rx_context* ctx, const double* q);     /* q[NA] */

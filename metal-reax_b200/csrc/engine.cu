@@ -119,7 +119,9 @@ struct Context {
   // QEq
   DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
   DBuf<double> cg_eta, cg_part, s_hist, t_hist, cg_rel;
-  DBuf<int> cg_iters;
+  DBuf<int> cg_iters, cg_nlive;
+  DBuf<SysCg> cg_sys;
+  DBuf<double2> cg_rb0, cg_rb1;
   std::vector<int> last_iters;
   std::vector<double> last_rel;
   // MD
@@ -429,6 +431,7 @@ struct Context {
     energies.ensure(static_cast<size_t>(nsys) * kTerms);
     cg_x.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
+    cg_sys.ensure(nsys); cg_rb0.ensure(n); cg_rb1.ensure(n); cg_nlive.ensure(2);
     cg_part.ensure(8 * static_cast<size_t>(std::max(nsm, 1)) * 32);
   }
 
@@ -516,7 +519,7 @@ struct Context {
     CgArgs a = cg_args();
     ++launches;
     k_qeq_prepare<<<blocks(na, 256), 256, 0, stream>>>(d, dff, a, s_hist.p, t_hist.p);
-    if (nsys == 1) {   // one system: all SMs on it (a single block per system is latency-bound)
+    if (nsys == 1 && na > 4096) {   // one large system: all SMs on its rows, block partials summed in block order
       const int threads = 256;
       int per_sm = 0;
       RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_grid, threads, 0));
@@ -527,9 +530,18 @@ struct Context {
       void* args[] = {const_cast<Dev*>(&d), &a};
       ++launches;
     RXCU(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_grid), dim3(grid), dim3(threads), args, 0, stream));
-    } else {
+    } else {   // a batch (or one small system): every row of every system on all SMs, per-system fixed-order sums
+      const int threads = 256;
+      int per_sm = 0;
+      RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_seg, threads, 0));
+      int grid = std::max(1, std::min(per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
+      grid = std::min(grid, nsm * 32);
+      a.sc = cg_sys.p; a.rb0 = cg_rb0.p; a.rb1 = cg_rb1.p; a.nlive = cg_nlive.p;
+      RXCU(cudaMemsetAsync(cg_sys.p, 0, sizeof(SysCg) * nsys, stream));
+      RXCU(cudaMemsetAsync(cg_nlive.p, 0, 2 * sizeof(int), stream));
+      void* args[] = {const_cast<Dev*>(&d), &a};
       ++launches;
-      k_cg_block<<<nsys, 512, 0, stream>>>(d, a);
+      RXCU(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_seg), dim3(grid), dim3(threads), args, 0, stream));
     }
     toc(1);
   }
@@ -904,6 +916,25 @@ int rx_set_systems(rx_context* ctx, int nsys, const int* natoms, const double* o
 }
 
 int rx_num_atoms(const rx_context* ctx) { return (ctx && ctx->c) ? ctx->c->na : 0; }
+
+int rx_set_capacities(rx_context* ctx, int nbr_entries, int bonds, int near_entries) {
+  return guarded(ctx, [&](rx::Context& c) {
+    c.require_sys();
+    if (nbr_entries < 1 || bonds < 1 || near_entries < 1) throw rx::Error(RX_ERR_INVALID, "capacities must be >= 1");
+    c.ncap = (nbr_entries + 31) / 32 * 32;
+    c.bcap = bonds;
+    c.ncap_near = (near_entries + 31) / 32 * 32;
+    c.alloc_lists();
+  });
+}
+
+int rx_get_capacities(const rx_context* ctx, int* out3) {
+  if (!ctx || !ctx->c || !out3) return RX_ERR_INVALID;
+  out3[0] = ctx->c->ncap;
+  out3[1] = ctx->c->bcap;
+  out3[2] = ctx->c->ncap_near;
+  return RX_OK;
+}
 
 int rx_set_positions(rx_context* ctx, const double* x) {
   return guarded(ctx, [&](rx::Context& c) {

@@ -13,6 +13,13 @@ struct QeqParams {
   double tap[8];   // taper coefficients on [swa, swb]
 };
 
+// per-system state of the segmented (batched) CG
+struct SysCg {
+  double sig_s, sig_t, bnorm_s, bnorm_t, alpha_s, alpha_t, beta_s, beta_t;
+  int act_s, act_t, it_s, it_t, live, breakdown;
+  unsigned counter;   // rows of this system that have arrived in the current pass
+};
+
 struct CgArgs {
   int begin, n, imax;
   double tol;
@@ -26,15 +33,19 @@ struct CgArgs {
   double* part;    // 2 * 4 * gridDim.x partial sums (double-buffered)
   int* out_iters;
   double* out_rel;
+  // segmented CG only
+  SysCg* sc;       // nsys
+  double2* rb0;    // per-row dot-product terms (fixed-order per-system sums)
+  double2* rb1;
+  int* nlive;      // [2]: systems still iterating, by iteration parity
 };
-using CgBatchArgs = CgArgs;
 
 __global__ void k_wrap_bin(Dev d);
 __global__ void k_cell_start(Dev d, const int* sorted_keys);
 __global__ void k_neighbors(Dev d, DevFF ff, QeqParams qp);
 __global__ void k_nonbonded(Dev d, DevFF ff);
 __global__ void k_cg_grid(Dev d, CgArgs a);
-__global__ void k_cg_block(Dev d, CgBatchArgs a);
+__global__ void k_cg_seg(Dev d, CgArgs a);
 __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, const double* t_hist);
 __global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist);
 __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y);

@@ -490,118 +490,229 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   }
 }
 
-// One block per system: the same algorithm for many small systems at once (batched systems of a few hundred to a
-// few thousand atoms). Block-level reductions in fixed order; no grid-wide waits.
-__global__ void k_cg_block(Dev d, CgBatchArgs a) {
-  const int sidx = blockIdx.x;
-  if (sidx >= d.nsys) return;
-  const SysInfo s = d.sys[sidx];
-  const int i0 = s.begin, n = s.natoms;
-  __shared__ double sh[32 * 4];
-  __shared__ double tot[4];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  auto reduce = [&](double* v, int nv) {
-    for (int k = 0; k < nv; ++k) {
-      double x = v[k];
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-      if (lane == 0) sh[wid * 4 + k] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x < nv) {
-      double t = 0.0;
-      for (int w = 0; w < nw; ++w) t += sh[w * 4 + threadIdx.x];
-      tot[threadIdx.x] = t;
-    }
-    __syncthreads();
-    for (int k = 0; k < nv; ++k) v[k] = tot[k];
-    __syncthreads();
-  };
-  double loc[4];
-  loc[0] = loc[1] = loc[2] = loc[3] = 0.0;
-  for (int r = wid; r < n; r += nw) {
-    const int i = i0 + r;
-    const double eta = a.eta[i];
-    const double2 y = row_mv(d, i, eta, a.x);
-    if (lane == 0) {
-      const double2 b = a.b[i];
-      const double2 rr = make_double2(b.x - y.x, b.y - y.y);
-      a.r[i] = rr;
-      const double2 dd = make_double2(rr.x / eta, rr.y / eta);
-      a.d[i] = dd;
-      loc[0] += b.x * b.x; loc[1] += b.y * b.y; loc[2] += rr.x * dd.x; loc[3] += rr.y * dd.y;
-    }
+// Segmented Jacobi-PCG: every system of the batch at once on one cooperative grid, the same algorithm (and the same
+// stopping rule per system, s and t separately) as the stock loop of fix qeq/reaxff (fix_qeq_reaxff_metal.cpp:89-123).
+// Rows of all systems are spread over all warps of the GPU, so one small system no longer runs on a single block.
+// Every dot product is a per-row term written to rb0/rb1; the warp that brings the last row of a system to a pass
+// sums that system's terms in row order (lane-strided, then a butterfly), so a system's result depends only on its
+// own rows: it is bitwise the same alone and inside any batch. The iteration loop ends when no system is live; the
+// live count is kept per iteration parity so that no block can see it change before every block has read it.
+__device__ inline double2 sys_sum2(const double2* v, int i0, int n) {
+  const int lane = threadIdx.x & 31;
+  double sx = 0.0, sy = 0.0;
+#pragma unroll 8
+  for (int k = lane; k < n; k += 32) {
+    const double2 t = __ldcg(v + i0 + k);
+    sx += t.x;
+    sy += t.y;
   }
-  reduce(loc, 4);
-  const double bnorm_s = sqrt(loc[0]), bnorm_t = sqrt(loc[1]);
-  double sig_s = loc[2], sig_t = loc[3];
-  bool act_s = true, act_t = true, breakdown = false;
-  int it_s = 1, it_t = 1;
-  for (int it = 1; it < a.imax; ++it) {
-    act_s = act_s && (sqrt(sig_s) / bnorm_s > a.tol);
-    act_t = act_t && (sqrt(sig_t) / bnorm_t > a.tol);
-    if (!act_s && !act_t) break;
-    loc[0] = loc[1] = 0.0;
-    for (int r = wid; r < n; r += nw) {
-      const int i = i0 + r;
-      const double2 y = row_mv(d, i, a.eta[i], a.d);
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+  }
+  return make_double2(sx, sy);
+}
+
+// lane 0 counts cnt rows of the system in (after every lane's writes are fenced); true in every lane of the warp that
+// brought the system's last rows
+__device__ inline bool arrive_last(SysCg* sc, int n, int cnt) {
+  __threadfence();
+  __syncwarp();
+  bool last = false;
+  if ((threadIdx.x & 31) == 0) last = atomicAdd(&sc->counter, static_cast<unsigned>(cnt)) == static_cast<unsigned>(n - cnt);
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (last) __threadfence();
+  return last;
+}
+
+__global__ void __launch_bounds__(256, 4) k_cg_seg(Dev d, CgArgs a) {
+  if (lists_failed(d)) return;
+  cg::grid_group g = cg::this_grid();
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  const int na = d.na;
+  const double tol = a.tol;
+  // matrix passes: warp per row, rows dealt round-robin over all warps (a system that is still iterating when most
+  // have stopped keeps many warps busy); a warp counts its rows of one system in when it meets a different system
+  // ---- r = b - A x, d = M^-1 r; |b|^2 and r.d per system; first stop test
+  {
+    int cur = -1, cnt = 0;
+    auto finish = [&](int s, int c) {
+      const SysInfo& si = d.sys[s];
+      if (!arrive_last(a.sc + s, si.natoms, c)) return;
+      const double2 bb = sys_sum2(a.rb0, si.begin, si.natoms);
+      const double2 rd = sys_sum2(a.rb1, si.begin, si.natoms);
       if (lane == 0) {
-        a.q[i] = y;
-        const double2 dd = a.d[i];
-        loc[0] += dd.x * y.x; loc[1] += dd.y * y.y;
+        SysCg& c2 = a.sc[s];
+        c2.counter = 0;
+        c2.bnorm_s = sqrt(bb.x);
+        c2.bnorm_t = sqrt(bb.y);
+        c2.sig_s = rd.x;
+        c2.sig_t = rd.y;
+        c2.it_s = c2.it_t = 1;
+        c2.breakdown = 0;
+        c2.act_s = sqrt(c2.sig_s) / c2.bnorm_s > tol;
+        c2.act_t = sqrt(c2.sig_t) / c2.bnorm_t > tol;
+        c2.live = (c2.act_s || c2.act_t) && a.imax > 1;
+        if (c2.live) atomicAdd(a.nlive + 1, 1);
+      }
+    };
+    for (int i = gw; i < na; i += nw) {
+      const int s = d.sys_of[i];
+      if (s != cur) {
+        if (cnt > 0) finish(cur, cnt);
+        cur = s;
+        cnt = 0;
+      }
+      const double eta = a.eta[i];
+      const double2 y = row_mv(d, i, eta, a.x);
+      if (lane == 0) {
+        const double2 b = a.b[i];
+        const double2 rr = make_double2(b.x - y.x, b.y - y.y);
+        a.r[i] = rr;
+        const double2 dd = make_double2(rr.x / eta, rr.y / eta);
+        a.d[i] = dd;
+        a.rb0[i] = make_double2(b.x * b.x, b.y * b.y);
+        a.rb1[i] = make_double2(rr.x * dd.x, rr.y * dd.y);
+      }
+      ++cnt;
+    }
+    if (cnt > 0) finish(cur, cnt);
+  }
+  g.sync();
+  for (int it = 1; it < a.imax; ++it) {
+    if (__ldcg(a.nlive + (it & 1)) == 0) break;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.nlive[(it + 1) & 1] = 0;
+    // ---- q = A d, d.q; alpha (or a breakdown, which ends this system)
+    {
+      int cur = -1, cnt = 0;
+      bool live = false;
+      auto finish = [&](int s, int c) {
+        const SysInfo& si = d.sys[s];
+        if (!arrive_last(a.sc + s, si.natoms, c)) return;
+        const double2 dq = sys_sum2(a.rb0, si.begin, si.natoms);
+        if (lane == 0) {
+          SysCg& c2 = a.sc[s];
+          c2.counter = 0;
+          c2.alpha_s = c2.act_s ? c2.sig_s / dq.x : 0.0;
+          c2.alpha_t = c2.act_t ? c2.sig_t / dq.y : 0.0;
+          if (!(isfinite(c2.alpha_s) && isfinite(c2.alpha_t))) {
+            c2.breakdown = 1;
+            c2.live = 0;
+          }
+        }
+      };
+      for (int i = gw; i < na; i += nw) {
+        const int s = d.sys_of[i];
+        if (s != cur) {
+          if (cnt > 0) finish(cur, cnt);
+          cur = s;
+          cnt = 0;
+          live = __ldcg(&a.sc[s].live) != 0;
+        }
+        if (!live) continue;
+        const double2 y = row_mv(d, i, a.eta[i], a.d);
+        if (lane == 0) {
+          a.q[i] = y;
+          const double2 dd = a.d[i];
+          a.rb0[i] = make_double2(dd.x * y.x, dd.y * y.y);
+        }
+        ++cnt;
+      }
+      if (cnt > 0) finish(cur, cnt);
+    }
+    g.sync();
+    // ---- x += alpha d, r -= alpha q, p = M^-1 r, r.p; beta, the counts and the next stop test
+    for (int i0 = gw * 32; i0 < na; i0 += nw * 32) {
+      const int i = i0 + lane;
+      int s = -1;
+      bool on = false;
+      if (i < na) {
+        s = d.sys_of[i];
+        on = __ldcg(&a.sc[s].live) != 0;
+      }
+      if (on) {
+        const double alpha_s = __ldcg(&a.sc[s].alpha_s), alpha_t = __ldcg(&a.sc[s].alpha_t);
+        const double2 dd = a.d[i], qq = a.q[i];
+        double2 xx = a.x[i], rr = a.r[i];
+        xx.x += alpha_s * dd.x; xx.y += alpha_t * dd.y;
+        rr.x -= alpha_s * qq.x; rr.y -= alpha_t * qq.y;
+        a.x[i] = xx;
+        a.r[i] = rr;
+        const double eta = a.eta[i];
+        const double2 pp = make_double2(rr.x / eta, rr.y / eta);
+        a.p[i] = pp;
+        a.rb0[i] = make_double2(rr.x * pp.x, rr.y * pp.y);
+      }
+      __threadfence();
+      __syncwarp();
+      // one arrival per system present in this warp's 32 rows, by the lowest lane of that system
+      const unsigned on_mask = __ballot_sync(0xffffffffu, on);
+      const unsigned same = __match_any_sync(0xffffffffu, s) & on_mask;
+      bool last = false;
+      if (on && (__ffs(same) - 1) == lane) {
+        const unsigned c = __popc(same);
+        last = atomicAdd(&a.sc[s].counter, c) == static_cast<unsigned>(d.sys[s].natoms) - c;
+      }
+      unsigned m = __ballot_sync(0xffffffffu, last);
+      if (m) __threadfence();
+      while (m) {
+        const int l = __ffs(m) - 1;
+        m &= m - 1;
+        const int ss = __shfl_sync(0xffffffffu, s, l);
+        const SysInfo& si = d.sys[ss];
+        const double2 rp = sys_sum2(a.rb0, si.begin, si.natoms);
+        if (lane == 0) {
+          SysCg& c = a.sc[ss];
+          c.counter = 0;
+          c.beta_s = c.act_s ? rp.x / c.sig_s : 0.0;
+          c.beta_t = c.act_t ? rp.y / c.sig_t : 0.0;
+          if (c.act_s) { c.sig_s = rp.x; c.it_s = it + 1; }
+          if (c.act_t) { c.sig_t = rp.y; c.it_t = it + 1; }
+          // the stop test of the next iteration; d below is updated only for the right-hand sides still active
+          c.act_s = c.act_s && (sqrt(c.sig_s) / c.bnorm_s > tol);
+          c.act_t = c.act_t && (sqrt(c.sig_t) / c.bnorm_t > tol);
+          c.live = (c.act_s || c.act_t) && it + 1 < a.imax;
+          if (c.live) atomicAdd(a.nlive + ((it + 1) & 1), 1);
+        }
       }
     }
-    reduce(loc, 2);
-    const double alpha_s = act_s ? sig_s / loc[0] : 0.0;
-    const double alpha_t = act_t ? sig_t / loc[1] : 0.0;
-    if (!(isfinite(alpha_s) && isfinite(alpha_t))) { breakdown = true; break; }
-    loc[0] = loc[1] = 0.0;
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-      const int i = i0 + r;
-      const double2 dd = a.d[i], qq = a.q[i];
-      double2 xx = a.x[i], rr = a.r[i];
-      xx.x += alpha_s * dd.x; xx.y += alpha_t * dd.y;
-      rr.x -= alpha_s * qq.x; rr.y -= alpha_t * qq.y;
-      a.x[i] = xx;
-      a.r[i] = rr;
-      const double eta = a.eta[i];
-      const double2 pp = make_double2(rr.x / eta, rr.y / eta);
-      a.p[i] = pp;
-      loc[0] += rr.x * pp.x; loc[1] += rr.y * pp.y;
-    }
-    reduce(loc, 2);
-    const double beta_s = act_s ? loc[0] / sig_s : 0.0;
-    const double beta_t = act_t ? loc[1] / sig_t : 0.0;
-    if (act_s) { sig_s = loc[0]; it_s = it + 1; }
-    if (act_t) { sig_t = loc[1]; it_t = it + 1; }
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-      const int i = i0 + r;
+    g.sync();
+    // ---- d = p + beta d
+    for (int i = gw * 32 + lane; i < na; i += nw * 32) {
+      const int s = d.sys_of[i];
+      if (!__ldcg(&a.sc[s].live)) continue;
+      const double beta_s = __ldcg(&a.sc[s].beta_s), beta_t = __ldcg(&a.sc[s].beta_t);
+      const int act_s = __ldcg(&a.sc[s].act_s), act_t = __ldcg(&a.sc[s].act_t);
       const double2 pp = a.p[i];
       double2 dd = a.d[i];
       if (act_s) dd.x = pp.x + beta_s * dd.x;
       if (act_t) dd.y = pp.y + beta_t * dd.y;
       a.d[i] = dd;
     }
-    __syncthreads();
+    g.sync();
   }
-  loc[0] = loc[1] = 0.0;
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
-    const double2 xx = a.x[i0 + r];
-    loc[0] += xx.x; loc[1] += xx.y;
-  }
-  reduce(loc, 2);
-  const double u = loc[0] / loc[1];
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
-    const double2 xx = a.x[i0 + r];
-    d.q[i0 + r] = xx.x - u * xx.y;
-  }
-  if (threadIdx.x == 0) {
-    a.out_iters[2 * sidx] = it_s;
-    a.out_iters[2 * sidx + 1] = it_t;
-    a.out_rel[2 * sidx] = sqrt(sig_s) / bnorm_s;
-    a.out_rel[2 * sidx + 1] = sqrt(sig_t) / bnorm_t;
-    if (breakdown) atomicOr(d.status, ST_CG_BREAKDOWN);
+// ---- calculate_Q per system (warp per system): q = s - (sum s / sum t) t, the counts and residuals
+  for (int s = gw; s < d.nsys; s += nw) {
+    const SysInfo& si = d.sys[s];
+    const double2 sum = sys_sum2(a.x, si.begin, si.natoms);
+    const double u = sum.x / sum.y;
+    for (int k = lane; k < si.natoms; k += 32) {
+      const double2 xx = a.x[si.begin + k];
+      d.q[si.begin + k] = xx.x - u * xx.y;
+    }
+    if (lane == 0) {
+      const SysCg& c = a.sc[s];
+      a.out_iters[2 * s] = c.it_s;
+      a.out_iters[2 * s + 1] = c.it_t;
+      a.out_rel[2 * s] = sqrt(c.sig_s) / c.bnorm_s;
+      a.out_rel[2 * s + 1] = sqrt(c.sig_t) / c.bnorm_t;
+      if (c.breakdown) atomicOr(d.status, ST_CG_BREAKDOWN);
+    }
   }
 }
+
 
 // Initial guesses from the histories (Q-23: s = 4(s0+s2) - (6 s1 + s3), t = t2 + 3(t0 - t1); index 0 = latest),
 // right-hand sides b_s = -chi, b_t = -1, and the diagonal eta.

@@ -51,7 +51,7 @@ __device__ inline double2 csr_row_mv(int i, const int* rs, const int* col, const
   return make_double2(eta * vi.x + __shfl_sync(0xffffffffu, ys, 0), eta * vi.y + __shfl_sync(0xffffffffu, yt, 0));
 }
 
-// The block-per-system Jacobi-PCG of the engine (k_cg_block) for one system held as a CSR matrix: solves
+// A single-block Jacobi-PCG for one system held as a CSR matrix: solves
 // (diag(eta) + H) s = -chi and (diag(eta) + H) t = -1 with the stopping rule of the stock fix (sqrt(r.M^-1 r)/|b| <=
 // tol, at most imax - 1 iterations per system), then q = s - (sum s / sum t) t. Every work vector is written before
 // it is read, so the previous call's contents of the scratch array never reach the result.

@@ -30,7 +30,7 @@ EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
-           "rx_qeq_solve_static"]
+           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -68,6 +68,7 @@ def load():
         "rx_stream": (_V, [_V]), "rx_set_timing": (_I, [_V, _I]), "rx_kernel_launches": (ctypes.c_int64, [_V]),
         "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
+        "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -221,6 +222,14 @@ class Engine:
 
     def stream(self):
         return self.lib.rx_stream(self.h)
+
+    def set_capacities(self, nbr, bonds, near):
+        self._check(self.lib.rx_set_capacities(self.h, int(nbr), int(bonds), int(near)))
+
+    def capacities(self):
+        out = np.zeros(3, dtype=np.int32)
+        self._check(self.lib.rx_get_capacities(self.h, _p(out)))
+        return tuple(int(v) for v in out)
 
     def set_timing(self, on=True):
         self._check(self.lib.rx_set_timing(self.h, 1 if on else 0))

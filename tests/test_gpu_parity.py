@@ -131,3 +131,80 @@ def test_batch_equals_alone(engine):
         assert np.array_equal(both["e"][k], alone[k]["e"][0])
         assert np.array_equal(both["grad"][off:off + n], alone[k]["grad"])
         off += n
+
+
+def test_batched_charges_equal_alone_and_oracle(engine, oracle):
+    """Batching form: the charge solve of a batch gives every system the same bits as its solve alone (per-system
+    fixed-order reductions), and the oracle's charges within 1e-10 e at tol 1e-12."""
+    import systems
+    ss = [systems.random_cho(k) for k in (0, 4, 9, 21, 33, 40)]
+    engine.set_qeq(0.0, 10.0, 1e-12, 400)
+    engine.set_systems(ss)
+    both = engine.qeq_solve()
+    off = 0
+    for k, s in enumerate(ss):
+        n = len(s["type"])
+        engine.set_systems([s])
+        alone = engine.qeq_solve()
+        assert np.array_equal(alone["q"], both["q"][off:off + n]), s["name"]
+        assert np.array_equal(alone["iters"][0], both["iters"][k])
+        ref = oracle.qeq(s, tol=1e-12, imax=400)
+        assert np.abs(alone["q"] - ref["q"]).max() <= 1e-10, s["name"]
+        assert abs(alone["q"].sum()) <= 1e-9
+        off += n
+    engine.set_qeq()
+
+
+def test_batch_of_mixed_systems_matches_oracle(engine, oracle):
+    """Eight systems of the 512-system batching workload (uneven sizes and compositions) in one batch, each against
+    the oracle under the same bars as the single-system test."""
+    import systems
+    ss = [systems.random_cho(k) for k in (1, 5, 12, 77, 130, 256, 300, 511)]
+    qs = [fixed_charges(s) for s in ss]
+    engine.set_systems(ss)
+    engine.set_charges(np.concatenate(qs))
+    out = engine.compute(census=True)
+    off = 0
+    for k, s in enumerate(ss):
+        n = len(s["type"])
+        ref = oracle.single_point(s, qs[k])
+        e = out["e"][k]
+        assert abs(e.sum() - ref["e"].sum()) / n <= C3_ENERGY_PER_ATOM, s["name"]
+        fmax, frms = force_metrics(ref["grad"], out["grad"][off:off + n])
+        assert fmax <= C3_FORCE_MAX and frms <= C3_FORCE_RMS, (s["name"], fmax, frms)
+        for c in range(7):
+            assert np.array_equal(out["census"][c][off:off + n], ref["census"][c]), (s["name"], c)
+        off += n
+
+
+def test_capacity_regrowth_gives_same_bits(engine):
+    """Failure detection on the host: lists started far too small overflow, the engine grows them from the counts the
+    kernels report and repeats the evaluation; the result is bitwise the one with ample capacities."""
+    s = small_systems()[2]
+    engine.set_systems([s])
+    engine.set_charges(fixed_charges(s))
+    ref = engine.compute()
+    ample = engine.capacities()
+    engine.set_capacities(32, 1, 32)
+    assert engine.capacities() == (32, 1, 32)
+    out = engine.compute()
+    grown = engine.capacities()
+    assert grown[0] > 32 and grown[1] > 1
+    assert np.array_equal(out["e"], ref["e"]) and np.array_equal(out["grad"], ref["grad"])
+    assert ample[0] >= 32
+
+
+def test_strict_qeq_reports_non_convergence(engine):
+    """fix qeq/reaxff/metal strict mode (fix_qeq_reaxff_metal.cpp:79-80): hitting imax is an error; otherwise the
+    iteration counts and residuals report it."""
+    import rxcuda
+    s = small_systems()[0]
+    engine.set_systems([s])
+    engine.set_qeq(0.0, 10.0, 1e-14, 3, strict=True)
+    with pytest.raises(rxcuda.RxError) as ei:
+        engine.qeq_solve()
+    assert ei.value.code == 5
+    engine.set_qeq(0.0, 10.0, 1e-14, 3, strict=False)
+    r = engine.qeq_solve()
+    assert r["iters"].max() <= 3 and r["rel"].max() > 1e-14
+    engine.set_qeq()
