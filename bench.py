@@ -12,6 +12,8 @@ value: atom-steps/s of the whole job with the state resident in HBM (device-time
 stream, max over ranks). e2e: the same metric through the C ABI with host buffers (positions in, gradient and
 energies out every step, integration on the host, as the LAMMPS plugin drives the engine). N > 1: N independent
 replicas (one per GPU, no collective on the data path; the single-system step does not shard).
+batch: the batching form on the same GPU, 512 mixed CHO systems evaluated as one batch versus one context per
+system (atom-evals/s of each, their ratio, p50/p99 latency of the batched evaluation).
 --impl reference: the reference's own CPU engine (oracle/_ref, cpu64) plus the C restatement of the stock QEq CG on
 the host, same workload and metric.
 """
@@ -102,23 +104,43 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------------------------------- byte model
-def bytes_model(N, P, D, I, R):
-    """Algorithmic HBM bytes of one MD step: 128 N + 8 P + P (4 + 8 I) + 12 P R + 256 D (P = counted half pairs within
-    the non-bonded cut-off, D = directed bonds, I = fused s/t CG iterations, R = FP64 residual refinements)."""
-    return 128 * N + 8 * P + P * (4 + 8 * I) + 12 * P * R + 256 * D
-
-
-def phase_bytes(name, N, P, D, I, R):
-    """Algorithmic bytes of one launch of each timed phase, taken term by term from the step model."""
+def phase_bytes(name, N, E, D, I):
+    """Algorithmic HBM bytes of one launch sequence of each timed phase (N atoms, E neighbor-row entries, D directed
+    bonds, I charge-matrix passes of the fused s/t CG = max iteration count of the solve, init pass included)."""
     return {
-        "neighbors": 8 * P + 4 * P + 32 * N,       # pair list written + read once, H written once (FP32), positions
-        "qeq": P * 8 * I + 12 * P * R,              # H value + index per fused s/t iteration, FP64 refinement
+        "neighbors": 12 * E + 64 * N,              # row entry (4 B) + FP64 charge-matrix value (8 B) written; positions
+        "qeq": I * (12 * E + 160 * N),             # per pass: every row entry and value read, ~10 vectors of 16 B/atom
         "bond_orders": 128 * D,
         "bonded_terms": 64 * D,
         "torsion": 32 * D,
-        "nonbonded": 8 * P + 32 * N,                # list + positions/charges
+        "nonbonded": 4 * E + 64 * N,               # row entries + positions/charges/types, gradient written
         "gather": 32 * D + 32 * N,
     }.get(name, 0)
+
+
+def bytes_model(N, E, D, I):
+    """Algorithmic HBM bytes of one MD step: the sum of the phases plus the integrator (2 kicks, 64 B/atom each)."""
+    return sum(phase_bytes(k, N, E, D, I) for k in
+               ("neighbors", "qeq", "bond_orders", "bonded_terms", "torsion", "nonbonded", "gather")) + 128 * N
+
+
+PHASE_KERNEL = {"neighbors": "k_neighbors", "qeq": "k_cg_grid", "bond_orders": "k_bonds", "bonded_terms": "k_bonded_atom",
+                "torsion": "k_torsion", "nonbonded": "k_nonbonded", "gather": "k_force_final"}
+
+
+def profiled_traffic(kernel, passes):
+    """DRAM bytes (read + write) per launch of `kernel` on this workload, from the committed ncu summary: a per-launch
+    figure, or a per-matrix-pass figure scaled by the passes of the measured launch. None without a summary."""
+    p = REPO / "profiles" / "dram_traffic_water24k.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        f = line.split()
+        if len(f) >= 3 and f[0] == kernel and f[1] == "dram_bytes_per_launch":
+            return float(f[2])
+        if len(f) >= 3 and f[0] == kernel and f[1] == "dram_bytes_per_pass":
+            return float(f[2]) * passes
+    return None
 
 
 def measured_peak():
@@ -225,6 +247,12 @@ def run_engine(args, rank, world, local_rank):
     eng = make_engine(local_rank, s, v)
     stream = torch.cuda.ExternalStream(eng.stream(), device=torch.device("cuda", local_rank))
     eng.md_run(max(args.warmup, 3))
+    if args.qeq_passes > 0:
+        eng.set_qeq(QEQ["swa"], QEQ["swb"], 1e-300, args.qeq_passes)
+        r = eng.qeq_solve()
+        print(json.dumps({"qeq_passes": int(r["iters"].max()), "atoms": n}), flush=True)
+        eng.close()
+        return
     clocks = Clocks(local_rank) if rank == 0 else None
     if dist:
         dist.barrier()
@@ -255,17 +283,15 @@ def run_engine(args, rank, world, local_rank):
     eng.md_run(prof_steps)
     phases = {k: v_ / prof_steps for k, v_ in eng.phase_times().items()}
     eng.set_timing(False)
-    out = eng.compute(qeq=True, counts=True)
-    qr = eng.qeq_solve()
-    P = int(out["counts"][1])
+    I = int(eng.qeq_last()["iters"].max())       # charge-matrix passes of the last MD step's solve
+    out = eng.compute(counts=True)
+    E = int(out["counts"][2])
     D = int(out["counts"][0]) * 2
-    I = int(qr["iters"].max())
-    R = 0
     peak, peak_kind = measured_peak()
     dom = max(phases, key=phases.get) if phases else "qeq"
-    dom_bytes = phase_bytes(dom, n, P, D, I, R)
+    dom_bytes = phase_bytes(dom, n, E, D, I)
     achieved = dom_bytes / (phases[dom] * 1e-3) / 1e9 if phases.get(dom) else None
-    step_bytes = bytes_model(n, P, D, I, R)
+    step_bytes = bytes_model(n, E, D, I)
     step_achieved = step_bytes / (ms_step * 1e-3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -275,17 +301,21 @@ def run_engine(args, rank, world, local_rank):
                    "T_K": TEMP, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "per-step working set larger than L2 (neighbor rows + charge matrix ~160 MB)"},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None, "peak_kind": peak_kind,
-                     "phase_ms_per_step": phases},
+        "roofline": {"bound": "hbm", "kernel": PHASE_KERNEL.get(dom, dom), "phase": dom, "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                     "traffic": profiled_traffic(PHASE_KERNEL.get(dom, dom), I), "bytes_alg": dom_bytes,
+                     "peak_kind": peak_kind, "phase_ms_per_step": phases},
         "step_roofline": {"bytes_alg": step_bytes, "achieved": step_achieved, "peak": peak, "unit": "GB/s",
-                          "frac": step_achieved / peak, "N": n, "P": P, "D": D, "I": I, "R": R},
+                          "frac": step_achieved / peak, "N": n, "E": E, "D": D, "I": I},
         "clocks": ck,
     }
     eng.close()
     if world == 1 and rank == 0:
-        e2e_value, e2e_bytes = e2e_run(local_rank, s, v, max(2, args.steps // 2), 2)
-        line["e2e"] = {"value": e2e_value, "unit": UNIT, **e2e_bytes}
+        if not args.no_e2e:
+            e2e_value, e2e_bytes = e2e_run(local_rank, s, v, max(2, args.steps // 2), 2)
+            line["e2e"] = {"value": e2e_value, "unit": UNIT, **e2e_bytes}
+        if not args.no_batch:
+            line["batch"] = batch_run(local_rank)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(args.cpu_seconds)
     elif rank == 0:
@@ -295,6 +325,65 @@ def run_engine(args, rank, world, local_rank):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------------- batching form
+BATCH_SYSTEMS = 512
+
+
+def batch_run(device, reps=20, world=1, rank=0):
+    """512 independent periodic CHO systems (log-uniform 64-1024 atoms, Dirichlet C/H/O, 0.5-1.2 g/cm3, seed per
+    system): one energy + forces + charges evaluation of all of them, as a fresh single point (CG from zero), through
+    the C ABI with host buffers out (energies, gradient). Batched: every system in one context and one launch sequence;
+    per-system: one context per system, evaluated one after the other. Latency percentiles are over `reps` batched
+    evaluations (host wall clock around the synchronous call). Under N ranks each rank takes its shard of the systems."""
+    import rxcuda
+    import batching
+    ss_all = [systems.random_cho(k) for k in range(BATCH_SYSTEMS)]
+    mine = batching.shard_systems([len(s["type"]) for s in ss_all], world, rank)
+    ss = [ss_all[k] for k in mine]
+    na = sum(len(s["type"]) for s in ss)
+    text = ffield_text()
+
+    def engine_for(group):
+        e = rxcuda.Engine(device)
+        e.set_forcefield(text)
+        e.set_control()
+        e.set_qeq(QEQ["swa"], QEQ["swb"], QEQ["tol"], QEQ["imax"])
+        e.set_systems(group)
+        return e
+
+    eng = engine_for(ss)
+    for _ in range(3):
+        eng.compute(qeq=True, cold=True)
+    lat = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        eng.compute(qeq=True, cold=True)
+        lat.append(time.perf_counter() - t)
+    it = np.asarray(eng.qeq_solve()["iters"])
+    eng.close()
+    lat_ms = np.array(lat) * 1e3
+    batched = na / (np.median(lat_ms) * 1e-3)
+    singles = [engine_for([s]) for s in ss]
+    for e in singles:
+        e.compute(qeq=True, cold=True)
+    best = None
+    for _ in range(2):
+        t = time.perf_counter()
+        for e in singles:
+            e.compute(qeq=True, cold=True)
+        dt = time.perf_counter() - t
+        best = dt if best is None else min(best, dt)
+    for e in singles:
+        e.close()
+    per_system = na / best
+    return {"workload": "cho512_single_point_qeq", "systems": len(ss), "atoms": na, "qeq_tol": QEQ["tol"],
+            "unit": "atom-evals/s", "batched": batched, "per_system": per_system, "speedup": batched / per_system,
+            "latency_ms": {"p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
+                           "reps": reps},
+            "qeq_iters_max": int(it.max()), "per_system_pass_ms": best * 1e3,
+            "note": "host wall clock through the C ABI (H2D of nothing, D2H of energies and gradient each evaluation)"}
 
 
 # ---------------------------------------------------------------------------------------------------- reference arm
@@ -357,6 +446,11 @@ def main():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (C ABI) run")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batching measurement")
+    ap.add_argument("--qeq-passes", type=int, default=0,
+                    help="profiling case: after the warm-up steps, one charge solve of exactly this many matrix passes "
+                         "(tolerance 0), then print the counts and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))

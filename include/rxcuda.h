@@ -37,6 +37,8 @@ extern "C" {
 /* rx_compute flags */
 #define RX_COMPUTE_QEQ 1        /* solve the charges (fix qeq/reaxff/metal resident) before the force evaluation */
 #define RX_COMPUTE_CENSUS 2     /* fill the decision census (include/reaxmetal/census.hpp:12-20) */
+#define RX_COMPUTE_QEQ_COLD 4     /* with RX_COMPUTE_QEQ: start the CG from s = t = 0 instead of the history extrapolation
+                                     (a fresh single point; the history is then restarted from this solve) */
 
 typedef struct rx_context rx_context;
 
@@ -86,6 +88,9 @@ int rx_set_qeq(rx_context* ctx, double swa, double swb, double tol, int imax, in
 int rx_qeq_solve(rx_context* ctx, int* iters, double* rel);
 /* mtl::Context::qeq_matvec (metal_backend.hpp:82): y = (diag(eta) + H) v over the owned atoms, v[NA], y[NA]. */
 int rx_qeq_matvec(rx_context* ctx, const double* v, double* y);
+/* CG iteration counts and final relative residuals (s, t per system, as rx_qeq_solve reports them) of the most recent
+ * charge solve of any entry point (rx_compute with RX_COMPUTE_QEQ, rx_md_run steps, rx_qeq_solve). */
+int rx_qeq_last(const rx_context* ctx, int32_t* iters, double* rel);
 
 /* PairReaxFFMetal::compute (pair_reaxff_metal.cpp:412-524) for every system: energies[13*nsys] in the reference's
  * EnergyTerm order (bond, over, under, lone_pair, valence, penalty, coalition, hbond, torsion, conjugation, vdw,

@@ -127,7 +127,8 @@ struct Context {
   // MD
   bool md_ready = false;
   DBuf<double4> v;
-  DBuf<double> mass, ke, temp, scale, xi, vxi;
+  DBuf<double> mass, ke, temp, scale, xi, vxi, kpart;
+  DBuf<int> kfirst, ksys;
   MdDev md{};
   long long md_step = 0;
   // pinned host staging for per-step positions in and gradients out
@@ -665,6 +666,10 @@ struct Context {
   }
 
   void compute(int flags, double* e_out, double* g_out, int32_t* cen_out, int64_t* counts) {
+    if ((flags & RX_COMPUTE_QEQ) && (flags & RX_COMPUTE_QEQ_COLD)) {   // a fresh single point: CG from s = t = 0
+      RXCU(cudaMemsetAsync(s_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
+      RXCU(cudaMemsetAsync(t_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
+    }
     evaluate((flags & RX_COMPUTE_QEQ) != 0);
     energy_sums();
     if (e_out) RXCU(cudaMemcpyAsync(e_out, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
@@ -771,7 +776,17 @@ struct Context {
     RXCU(cudaMemset(xi.p, 0, sizeof(double) * nsys * kMaxChain));
     RXCU(cudaMemset(vxi.p, 0, sizeof(double) * nsys * kMaxChain));
     RXCU(cudaMemset(v.p, 0, sizeof(double4) * na));
-    md = MdDev{v.p, mass.p, ke.p, temp.p, scale.p, xi.p, vxi.p, dt, t0, t1, tdamp, chain};
+    std::vector<int> first(static_cast<size_t>(nsys) + 1, 0), csys;
+    for (int s = 0; s < nsys; ++s) {
+      const int nc = (hsys[s].natoms + kKeChunk - 1) / kKeChunk;
+      first[s + 1] = first[s] + nc;
+      for (int k = 0; k < nc; ++k) csys.push_back(s);
+    }
+    const int nchunks = first[nsys];
+    kpart.ensure(std::max(nchunks, 1)); kfirst.ensure(first.size()); ksys.ensure(std::max(nchunks, 1));
+    RXCU(cudaMemcpy(kfirst.p, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
+    if (nchunks > 0) RXCU(cudaMemcpy(ksys.p, csys.data(), sizeof(int) * csys.size(), cudaMemcpyHostToDevice));
+    md = MdDev{v.p, mass.p, ke.p, temp.p, scale.p, xi.p, vxi.p, dt, t0, t1, tdamp, chain, kpart.p, kfirst.p, ksys.p, nchunks};
     md_ready = true;
     md_step = 0;
   }
@@ -791,7 +806,7 @@ struct Context {
 
   void thermostat_half(double frac) {
     ++launches;
-    k_md_kinetic<<<nsys, 256, 0, stream>>>(md, sys.p, type.p);
+    k_md_kinetic_part<<<md.nchunks, 256, 0, stream>>>(md, sys.p, type.p);
     ++launches;
     k_md_chain<<<blocks(nsys, 64), 64, 0, stream>>>(md, sys.p, nsys, frac);
     ++launches;
@@ -816,8 +831,9 @@ struct Context {
     energy_sums();
     if (e_out) RXCU(cudaMemcpyAsync(e_out, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
     if (t_out) {
-      ++launches;
-      k_md_kinetic<<<nsys, 256, 0, stream>>>(md, sys.p, type.p);
+      launches += 2;
+      k_md_kinetic_part<<<md.nchunks, 256, 0, stream>>>(md, sys.p, type.p);
+      k_md_kinetic_sum<<<blocks(nsys, 64), 64, 0, stream>>>(md, nsys);
       std::vector<double> kk(static_cast<size_t>(nsys));
       RXCU(cudaMemcpyAsync(kk.data(), ke.p, sizeof(double) * nsys, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaStreamSynchronize(stream));
@@ -916,6 +932,15 @@ int rx_set_systems(rx_context* ctx, int nsys, const int* natoms, const double* o
 }
 
 int rx_num_atoms(const rx_context* ctx) { return (ctx && ctx->c) ? ctx->c->na : 0; }
+
+int rx_qeq_last(const rx_context* ctx, int32_t* iters, double* rel) {
+  if (!ctx || !ctx->c) return RX_ERR_STATE;
+  const rx::Context& c = *ctx->c;
+  if (c.last_iters.empty()) return RX_ERR_STATE;
+  if (iters) std::copy(c.last_iters.begin(), c.last_iters.end(), iters);
+  if (rel) std::copy(c.last_rel.begin(), c.last_rel.end(), rel);
+  return RX_OK;
+}
 
 int rx_set_capacities(rx_context* ctx, int nbr_entries, int bonds, int near_entries) {
   return guarded(ctx, [&](rx::Context& c) {

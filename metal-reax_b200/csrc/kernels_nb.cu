@@ -166,9 +166,11 @@ __global__ void __launch_bounds__(128) k_neighbors(Dev d, DevFF ff, QeqParams qp
                 double Tap, dTap;
                 taper_horner(qp.tap, r, Tap, dTap);
                 const double a3 = r * r * r + shld_i[static_cast<int>(xj.w)];
-                double y = static_cast<double>(cbrtf(static_cast<float>(a3)));
-                y = y - (y * y * y - a3) / (3.0 * y * y);   // one Newton step: relative error ~1e-14
-                h = Tap * 14.4 / y;
+                // z = a3^(-1/3): single-precision seed, then two Newton steps z <- z + (z/3)(1 - a3 z^3), which
+                // square the relative error each (1e-7 -> 1e-14 -> rounding level); no division
+                double z = static_cast<double>(rcbrtf(static_cast<float>(a3)));
+                for (int k = 0; k < 2; ++k) z = fma(z * (1.0 / 3.0), fma(-a3 * z, z * z, 1.0), z);
+                h = Tap * 14.4 * z;
               }
               d.hval[rowbase + pos] = h;
             }

@@ -16,9 +16,17 @@ struct MdDev {
   double* vxi;       // nsys * kMaxChain chain velocities
   double dt, t_start, t_stop, t_damp;
   int chain;
+  // kinetic energy in fixed chunks of kKeChunk atoms per system (the sum of a system depends only on its atoms)
+  double* kpart;            // one partial per chunk
+  const int* kchunk_first;  // nsys + 1: first chunk of each system
+  const int* kchunk_sys;    // system of each chunk
+  int nchunks;
 };
 
-__global__ void k_md_kinetic(MdDev m, const SysInfo* sys, const int* type);
+constexpr int kKeChunk = 1024;
+
+__global__ void k_md_kinetic_part(MdDev m, const SysInfo* sys, const int* type);
+__global__ void k_md_kinetic_sum(MdDev m, int nsys);
 __global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys, double step_frac);
 __global__ void k_md_scale(MdDev m, const int* sys_of, int na);
 __global__ void k_md_kick(MdDev m, const int* type, const double4* grad, double4* x, int na, int drift);

@@ -15,13 +15,16 @@ constexpr double kMvv2e = 48.88821291 * 48.88821291;         // (g/mol) A^2/fs^2
 constexpr double kBoltz = 0.0019872067;                      // kcal/mol/K
 }  // namespace
 
-// kinetic energy (kcal/mol) of every system, fixed-order block sums (one block per system)
-__global__ void k_md_kinetic(MdDev m, const SysInfo* sys, const int* type) {
-  const SysInfo s = sys[blockIdx.x];
+// kinetic energy: one block per chunk of kKeChunk atoms of a system, a fixed-shape tree per chunk
+__global__ void k_md_kinetic_part(MdDev m, const SysInfo* sys, const int* type) {
+  const int c = blockIdx.x;
+  const int s = m.kchunk_sys[c];
+  const SysInfo& si = sys[s];
+  const int a0 = si.begin + (c - m.kchunk_first[s]) * kKeChunk;
+  const int a1 = min(a0 + kKeChunk, si.begin + si.natoms);
   __shared__ double sh[256];
   double v2 = 0.0;
-  for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) {
-    const int a = s.begin + r;
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const double4 v = m.v[a];
     v2 += m.mass[type[a]] * (v.x * v.x + v.y * v.y + v.z * v.z);
   }
@@ -31,7 +34,19 @@ __global__ void k_md_kinetic(MdDev m, const SysInfo* sys, const int* type) {
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) m.ke[blockIdx.x] = 0.5 * kMvv2e * sh[0];
+  if (threadIdx.x == 0) m.kpart[c] = sh[0];
+}
+
+// kinetic energy (kcal/mol) of a system from its chunk partials, in chunk order
+__device__ inline double system_ke(const MdDev& m, int s) {
+  double t = 0.0;
+  for (int c = m.kchunk_first[s]; c < m.kchunk_first[s + 1]; ++c) t += m.kpart[c];
+  return 0.5 * kMvv2e * t;
+}
+
+__global__ void k_md_kinetic_sum(MdDev m, int nsys) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nsys) m.ke[s] = system_ke(m, s);
 }
 
 // one thread per system: advance the chain by dt/2 and produce the velocity scale factor
@@ -49,7 +64,7 @@ __global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys, double step_fr
   Q[0] = nf * kT * tau2;
   for (int k = 1; k < M; ++k) Q[k] = kT * tau2;
   const double dt = m.dt, dt2 = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
-  double ke2 = 2.0 * m.ke[s];
+  double ke2 = 2.0 * system_ke(m, s);
   auto G = [&](int k) { return k == 0 ? (ke2 - nf * kT) / Q[0] : (Q[k - 1] * vx[k - 1] * vx[k - 1] - kT) / Q[k]; };
   vx[M - 1] += G(M - 1) * dt4;
   for (int k = M - 2; k >= 0; --k) {

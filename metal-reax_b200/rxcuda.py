@@ -25,12 +25,13 @@ TERMS = ["bond", "over", "under", "lone_pair", "valence", "penalty", "coalition"
 CENSUS = ["bonds", "angle_sets", "torsions", "hbonds", "nonbonded", "sbo_region", "lp_trunc"]
 RX_COMPUTE_QEQ = 1
 RX_COMPUTE_CENSUS = 2
+RX_COMPUTE_QEQ_COLD = 4
 STATUS = {0: "ok", 1: "invalid", 2: "ffield", 3: "capacity", 4: "cuda", 5: "not_converged", 6: "state", 7: "timeout"}
 EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_forcefield_dump", "rx_forcefield_params",
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
-           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities"]
+           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -69,6 +70,7 @@ def load():
         "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
         "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
+        "rx_qeq_last": (_I, [_V, _V, _V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -171,12 +173,12 @@ class Engine:
         return q
 
     # ---- evaluation
-    def compute(self, qeq=False, census=False, counts=False):
+    def compute(self, qeq=False, census=False, counts=False, cold=False):
         e = np.zeros(13 * self.nsys)
         g = np.zeros(3 * self.na)
         cen = np.zeros(7 * self.na, dtype=np.int32) if census else None
         cnt = np.zeros(4, dtype=np.int64) if counts else None
-        flags = (RX_COMPUTE_QEQ if qeq else 0) | (RX_COMPUTE_CENSUS if census else 0)
+        flags = (RX_COMPUTE_QEQ if qeq else 0) | (RX_COMPUTE_CENSUS if census else 0) | (RX_COMPUTE_QEQ_COLD if cold else 0)
         self._check(self.lib.rx_compute(self.h, flags, _p(e), _p(g), _p(cen), _p(cnt)))
         out = {"e": e.reshape(self.nsys, 13), "grad": g.reshape(-1, 3)}
         if census:
@@ -222,6 +224,12 @@ class Engine:
 
     def stream(self):
         return self.lib.rx_stream(self.h)
+
+    def qeq_last(self):
+        it = np.zeros(2 * self.nsys, dtype=np.int32)
+        rel = np.zeros(2 * self.nsys)
+        self._check(self.lib.rx_qeq_last(self.h, _p(it), _p(rel)))
+        return {"iters": it.reshape(-1, 2), "rel": rel.reshape(-1, 2)}
 
     def set_capacities(self, nbr, bonds, near):
         self._check(self.lib.rx_set_capacities(self.h, int(nbr), int(bonds), int(near)))

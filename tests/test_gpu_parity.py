@@ -208,3 +208,35 @@ def test_strict_qeq_reports_non_convergence(engine):
     r = engine.qeq_solve()
     assert r["iters"].max() <= 3 and r["rel"].max() > 1e-14
     engine.set_qeq()
+
+
+def test_nvt_batch_equals_alone_and_reruns_bitwise():
+    """NVT with charge equilibration every step: a system advanced inside a batch follows bitwise the trajectory it
+    follows alone (per-system thermostat sums in fixed chunks, per-system CG reductions), and a rerun repeats it."""
+    import rxcuda
+    import systems
+    mass = [12.0, 1.008, 15.999]
+    ss = [systems.random_cho(3), systems.water_box(4)]
+    vs = [systems.maxwell_velocities(s, 300.0, seed=7 + k) for k, s in enumerate(ss)]
+
+    def run(group, vel):
+        e = rxcuda.Engine(0)
+        e.set_forcefield(ffield_text())
+        e.set_control()
+        e.set_qeq(0.0, 10.0, 1e-6, 200)
+        e.set_systems(group)
+        e.md_setup(mass, dt=0.25, t_start=300.0, t_damp=25.0, chain=3)
+        e.set_velocities(np.concatenate(vel))
+        out = e.md_run(20)
+        x = e.get_positions()
+        e.close()
+        return out, x
+
+    alone = [run([s], [v]) for s, v in zip(ss, vs)]
+    both, xb = run(ss, vs)
+    again, xa = run(ss, vs)
+    assert np.array_equal(xb, xa)
+    n0 = len(ss[0]["type"])
+    assert np.array_equal(alone[0][1], xb[:n0]) and np.array_equal(alone[1][1], xb[n0:])
+    for k in range(2):
+        assert np.all(np.isfinite(alone[k][1]))
