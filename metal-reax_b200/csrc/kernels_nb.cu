@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
 __device__ inline double2 sys_sum2(const double2* v, int i0, int n) {
   const int lane = threadIdx.x & 31;
   double sx = 0.0, sy = 0.0;
-#pragma unroll 8
+#pragma unroll 4
   for (int k = lane; k < n; k += 32) {
     const double2 t = __ldcg(v + i0 + k);
     sx += t.x;
