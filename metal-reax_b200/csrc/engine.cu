@@ -604,6 +604,14 @@ struct Context {
       launch_bonded(d);
       launch_nonbonded(d);
       launch_gather(d);
+      if (do_qeq) {   // history shift and the solve's counts, in the same round trip as the status word
+        ++launches;
+        k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p);
+        last_iters.resize(2 * static_cast<size_t>(nsys));
+        last_rel.resize(2 * static_cast<size_t>(nsys));
+        RXCU(cudaMemcpyAsync(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
+        RXCU(cudaMemcpyAsync(last_rel.data(), cg_rel.p, sizeof(double) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
+      }
       int st[4];
       RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaStreamSynchronize(stream));
@@ -628,14 +636,7 @@ struct Context {
     collect_times();
   }
 
-  void finish_qeq() {
-    last_iters.resize(2 * static_cast<size_t>(nsys));
-    last_rel.resize(2 * static_cast<size_t>(nsys));
-    RXCU(cudaMemcpy(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost));
-    RXCU(cudaMemcpy(last_rel.data(), cg_rel.p, sizeof(double) * 2 * nsys, cudaMemcpyDeviceToHost));
-    ++launches;
-    k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(dev(), cg_x.p, s_hist.p, t_hist.p);
-    RXCU(cudaStreamSynchronize(stream));
+  void finish_qeq() {   // the counts were copied back with the status word
     if (qeq_strict)
       for (size_t k = 0; k < last_rel.size(); ++k)
         if (!(last_rel[k] <= qeq_tol))
@@ -712,6 +713,12 @@ struct Context {
       const Dev d = dev();
       build_lists(d);
       launch_qeq(d);
+      ++launches;
+      k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p);
+      last_iters.resize(2 * static_cast<size_t>(nsys));
+      last_rel.resize(2 * static_cast<size_t>(nsys));
+      RXCU(cudaMemcpyAsync(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
+      RXCU(cudaMemcpyAsync(last_rel.data(), cg_rel.p, sizeof(double) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
       int st[4];
       RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaStreamSynchronize(stream));

@@ -729,7 +729,9 @@ __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, c
   a.eta[i] = ff.sb[t * SB_N + SB_ETA];
 }
 
+// the solve just finished becomes the newest history entry (not after a list overflow: the evaluation is repeated)
 __global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist) {
+  if (lists_failed(d)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.na) return;
   double* sh = s_hist + 4 * static_cast<size_t>(i);

@@ -149,3 +149,17 @@ def maxwell_velocities(sys_, T, seed):
     p = (v * m[:, None]).sum(0) / m.sum()
     v -= p
     return v
+
+
+def triclinic(s, tilts=(0.12, -0.08, 0.05), name=None):
+    """A general triclinic version of a cubic system: box rows a = (L,0,0), b = (xy, L, 0), c = (xz, yz, L) with the
+    tilts given as fractions of L; atoms keep their fractional coordinates (molecules are sheared slightly)."""
+    L = float(s["box"][0][0])
+    xy, xz, yz = (t * L for t in tilts)
+    box = np.array([[L, 0.0, 0.0], [xy, L, 0.0], [xz, yz, L]])
+    f = s["x"] / L
+    out = dict(s)
+    out["box"] = box
+    out["x"] = np.ascontiguousarray(f @ box)
+    out["name"] = name or (s["name"] + "_tri")
+    return out

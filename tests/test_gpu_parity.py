@@ -240,3 +240,40 @@ def test_nvt_batch_equals_alone_and_reruns_bitwise():
     assert np.array_equal(alone[0][1], xb[:n0]) and np.array_equal(alone[1][1], xb[n0:])
     for k in range(2):
         assert np.all(np.isfinite(alone[k][1]))
+
+
+def _check_against_oracle(engine, oracle, s, q):
+    ref = oracle.single_point(s, q)
+    engine.set_systems([s])
+    engine.set_charges(q)
+    out = engine.compute(census=True)
+    e, e_ref = out["e"][0], ref["e"]
+    rel = np.abs(e[FP64_TERMS] - e_ref[FP64_TERMS]) / np.maximum(1.0, np.abs(e_ref[FP64_TERMS]))
+    assert rel.max() <= 1e-7, (s["name"], e, e_ref)
+    assert abs(e.sum() - e_ref.sum()) / len(s["type"]) <= C3_ENERGY_PER_ATOM
+    fmax, frms = force_metrics(ref["grad"], out["grad"])
+    assert fmax <= C3_FORCE_MAX and frms <= C3_FORCE_RMS, (s["name"], fmax, frms)
+    for k in range(7):
+        assert np.array_equal(out["census"][k], ref["census"][k]), (s["name"], k)
+
+
+def test_triclinic_box_matches_oracle(engine, oracle):
+    """A general triclinic cell (tilted lattice rows): images, cut-off pruning by face distances and the lattice-shift
+    table on a non-orthogonal box."""
+    import systems
+    s = systems.triclinic(systems.water_box(4))
+    _check_against_oracle(engine, oracle, s, fixed_charges(s))
+
+
+def test_sparse_system_matches_oracle(engine, oracle):
+    """Two far-apart atoms in a large periodic box (no bonds, only images beyond the bond cut-off): every term of the
+    empty-list path, and the charge solve of a 2-atom system."""
+    s = {"name": "lone2", "origin": np.zeros(3), "box": np.eye(3) * 30.0, "periodic": np.ones(3, dtype=np.int32),
+         "x": np.array([[1.0, 1.0, 1.0], [15.0, 15.0, 15.0]]), "type": np.array([0, 2], dtype=np.int32),
+         "tag": np.array([1, 2], dtype=np.int64)}
+    _check_against_oracle(engine, oracle, s, np.array([0.1, -0.1]))
+    engine.set_qeq(0.0, 10.0, 1e-12, 100)
+    got = engine.qeq_solve()
+    ref = oracle.qeq(s, tol=1e-12, imax=100)
+    assert np.abs(got["q"] - ref["q"]).max() <= 1e-10
+    engine.set_qeq()

@@ -171,3 +171,17 @@ def test_engine_reader_rejects_bad_files():
     with pytest.raises(rxcuda.RxError):
         e.set_forcefield(text[: len(text) // 2])     # truncated file (strict mode rejects)
     e.close()
+
+
+def test_oracle_matches_reference_triclinic(coracle):
+    """General triclinic box (system.hpp Box: lattice rows a, b, c with tilts): the restatement against the reference."""
+    from oracle.oracle import RefOracle
+    import systems
+    if not RefOracle.available():
+        pytest.skip("reference oracle not built here")
+    s = systems.triclinic(systems.water_box(4))
+    q = fixed_charges(s)
+    a, b = coracle.single_point(s, q), RefOracle(ffield_text(), shell=15.0).single_point(s, q)
+    assert np.array_equal(a["census"], b["census"])
+    assert np.abs(a["e"] - b["e"]).max() <= 1e-9 * max(1.0, np.abs(b["e"]).max())
+    assert np.abs(a["grad"] - b["grad"]).max() <= 1e-9
