@@ -74,7 +74,7 @@ __device__ inline void taper_horner(const double* c, double r, double& Tap, doub
 // coalesced. Entries are written through a warp ballot in visiting order (deterministic). Fused: the charge-matrix
 // entry H = 14.4 Tap(r) / cbrt(r^3 + (gamma_i gamma_j)^-1.5) for r <= swb (ENGINE_SPEC 7; fix_qeq_reaxff compute_H),
 // and the near row (entries within max(bond_cut, hbond_cut)) the bond and H-bond kernels scan.
-__global__ void __launch_bounds__(128) k_neighbors(Dev d, DevFF ff, QeqParams qp) {
+__global__ void __launch_bounds__(128, 6) k_neighbors(Dev d, DevFF ff, QeqParams qp) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
