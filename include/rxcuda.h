@@ -115,13 +115,20 @@ int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature
  * q = s - (sum s / sum t) t. Every pointer is a device pointer on the current device, owned by the caller:
  * H as CSR (row_start[n+1], col[nnz], val[nnz]; every periodic image of a pair summed into its entry), eta[n] and
  * chi[n] per atom, s[n] and t[n] the initial guesses on entry and the solutions on return, q[n] the charges,
- * iters[2] and rel[2] (s then t; may be NULL). The call is asynchronous on `stream` (a cudaStream_t, NULL = default).
+ * iters[2] and rel[2] (s then t; may be NULL). iters[k] = -1 reports a CG breakdown of that right-hand side (a step
+ * length that is not finite: a singular or indefinite matrix); s, t and q are then not a solution. Pass iters to see
+ * a breakdown: without it a breakdown cannot be told from convergence. The call is asynchronous on `stream` (a
+ * cudaStream_t, NULL = default). A launch failure returns RX_ERR_CUDA; the CUDA error state is peeked, not cleared, so
+ * an error left pending by earlier work on the thread is reported here as well.
  * The CG work vectors live in one fixed device array of RX_QEQ_STATIC_MAX_ATOMS * 8 doubles (2 MiB) that every GPU
  * loading the library holds until the process exits; larger n is rejected with RX_ERR_INVALID. All calls share that
  * array: calls whose kernels overlap on the GPU (other streams, other threads) race, so serialise them. The array keeps
  * the last call's contents; nothing in it needs to start at zero, since every work vector is written before it is
- * read. The first call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
- * current, so make that first call before any stream capture. err/errlen (may be NULL) receive a message. */
+ * read. The first call on a device does a one-time set-up with that device current: it looks up the array's device
+ * address (cudaGetSymbolAddress), which under CUDA's lazy module loading also loads this library's device code and
+ * its array on that device - the driver's own allocation and synchronisation. Make that first call at start-up and
+ * before any stream capture; n = 0 does the set-up alone (no other argument is read, nothing is launched).
+ * err/errlen (may be NULL) receive a message. */
 #define RX_QEQ_STATIC_MAX_ATOMS 32768
 int rx_qeq_solve_static(int n, const int* row_start, const int* col, const double* val, const double* eta, const double* chi,
                         double* s, double* t, double* q, double tol, int imax, int* iters, double* rel, void* stream,

@@ -30,6 +30,7 @@ enum Status : int {
   ST_CG_BREAKDOWN = 16,
   ST_NONFINITE = 32,
   ST_NEAR_OVERFLOW = 64,
+  ST_CG_NOTCONV = 128,   // a system's charge solve ended above its tolerance (iteration limit)
 };
 
 struct SysInfo {

@@ -213,7 +213,7 @@ struct Context {
     size_t off = 0;
     auto put = [&](const double* src, size_t n) { std::memcpy(h.data() + off, src, n * sizeof(double)); size_t o = off; off += n; return o; };
     std::vector<double> gp(64, 0.0);
-    std::copy(ff.gp.begin(), ff.gp.end(), gp.begin());
+    std::copy(ff.gp.begin(), ff.gp.begin() + std::min<size_t>(ff.gp.size(), 64), gp.begin());
     const size_t o_gp = put(gp.data(), 64), o_sb = put(ff.sb.data(), nsb), o_tb = put(ff.tb.data(), ntb), o_thb = put(ff.thb.data(), nthb);
     const size_t o_fb = put(ff.fb.data(), nfb), o_hb = put(ff.hb.data(), nhb), o_shld = put(shld.data(), shld.size());
     const size_t o_nbf = off;
@@ -606,7 +606,7 @@ struct Context {
       launch_gather(d);
       if (do_qeq) {   // history shift and the solve's counts, in the same round trip as the status word
         ++launches;
-        k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p);
+        k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p, qeq_strict);
         last_iters.resize(2 * static_cast<size_t>(nsys));
         last_rel.resize(2 * static_cast<size_t>(nsys));
         RXCU(cudaMemcpyAsync(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
@@ -714,7 +714,7 @@ struct Context {
       build_lists(d);
       launch_qeq(d);
       ++launches;
-      k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p);
+      k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p, qeq_strict);
       last_iters.resize(2 * static_cast<size_t>(nsys));
       last_rel.resize(2 * static_cast<size_t>(nsys));
       RXCU(cudaMemcpyAsync(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost, stream));

@@ -91,12 +91,26 @@ void need(const Line& l, size_t n) {
 ForceField parse_force_field(std::string_view text, bool lg) {
   ForceField ff;
   Reader rd(text);
-  if (!rd.line()) throw FfieldError("empty force-field file");
-  // general parameters
+  // header (src/io/ffield_parser.cpp:100-115): the first non-blank line is a comment, and is rejected when it looks
+  // like the "N ! Number of general parameters" line (a file whose comment line is missing)
+  {
+    auto first = rd.line();
+    if (!first) throw FfieldError("empty force-field file");
+    const auto& w = first->tok;
+    bool digits = !w.empty() && !w[0].empty();
+    for (char c : w[0]) digits = digits && c >= '0' && c <= '9';
+    std::string joined;
+    for (const auto& x : w) joined += x + " ";
+    if (digits && w.size() >= 2 && !w[1].empty() && w[1][0] == '!' && joined.find("general parameters") != std::string::npos)
+      throw FfieldError("line " + std::to_string(first->lineno) + ": first line of ReaxFF potential file must be a comment or empty");
+  }
+  // general parameters (src/io/ffield_parser.cpp:118-129: at least 38). A file with 38 has no p_coa3 (gp[38]); the
+  // device copy of the list is zero-padded, so the coalition term then reads 0 there.
   {
     Line v = rd.values();
     const int n = inum(v, 0);
-    if (n < 39) throw FfieldError("the force field has " + std::to_string(n) + " general parameters; at least 39 are read");
+    if (n < 1) throw FfieldError("line " + std::to_string(v.lineno) + ": invalid number of global parameters");
+    if (n < 38) throw FfieldError("the force field has only " + std::to_string(n) + " general parameters (>= 38 required)");
     ff.gp.resize(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) ff.gp[static_cast<size_t>(i)] = num(rd.values(), 0);
   }

@@ -47,7 +47,7 @@ __global__ void k_nonbonded(Dev d, DevFF ff);
 __global__ void k_cg_grid(Dev d, CgArgs a);
 __global__ void k_cg_seg(Dev d, CgArgs a);
 __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, const double* t_hist);
-__global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist);
+__global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist, int strict);
 __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y);
 __global__ void k_energy_sum(Dev d, double* out);
 

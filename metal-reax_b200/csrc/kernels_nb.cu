@@ -489,6 +489,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
     a.out_rel[0] = sqrt(sig_s) / bnorm_s;
     a.out_rel[1] = sqrt(sig_t) / bnorm_t;
     if (breakdown) atomicOr(d.status, ST_CG_BREAKDOWN);
+    if (!(a.out_rel[0] <= a.tol && a.out_rel[1] <= a.tol)) atomicOr(d.status, ST_CG_NOTCONV);
   }
 }
 
@@ -711,6 +712,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_seg(Dev d, CgArgs a) {
       a.out_rel[2 * s] = sqrt(c.sig_s) / c.bnorm_s;
       a.out_rel[2 * s + 1] = sqrt(c.sig_t) / c.bnorm_t;
       if (c.breakdown) atomicOr(d.status, ST_CG_BREAKDOWN);
+      if (!(a.out_rel[2 * s] <= tol && a.out_rel[2 * s + 1] <= tol)) atomicOr(d.status, ST_CG_NOTCONV);
     }
   }
 }
@@ -729,9 +731,13 @@ __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, c
   a.eta[i] = ff.sb[t * SB_N + SB_ETA];
 }
 
-// the solve just finished becomes the newest history entry (not after a list overflow: the evaluation is repeated)
-__global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist) {
+// the solve just finished becomes the newest history entry; not after a list overflow (the evaluation is repeated),
+// nor after a failed solve (a breakdown, or a system above its tolerance in strict mode): the call then reports an
+// error and leaves the histories as they were
+__global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist, int strict) {
   if (lists_failed(d)) return;
+  const int st = *reinterpret_cast<volatile const int*>(d.status);
+  if ((st & ST_CG_BREAKDOWN) || (strict && (st & ST_CG_NOTCONV))) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.na) return;
   double* sh = s_hist + 4 * static_cast<size_t>(i);

@@ -54,7 +54,9 @@ __device__ inline double2 csr_row_mv(int i, const int* rs, const int* col, const
 // A single-block Jacobi-PCG for one system held as a CSR matrix: solves
 // (diag(eta) + H) s = -chi and (diag(eta) + H) t = -1 with the stopping rule of the stock fix (sqrt(r.M^-1 r)/|b| <=
 // tol, at most imax - 1 iterations per system), then q = s - (sum s / sum t) t. Every work vector is written before
-// it is read, so the previous call's contents of the scratch array never reach the result.
+// it is read, so the previous call's contents of the scratch array never reach the result. A breakdown (a step length
+// that is not finite, e.g. a singular or indefinite matrix) stops the loop and is reported as iters = -1 for the
+// right-hand side(s) it hit.
 __global__ void k_cg_csr_static(int n, const int* rs, const int* col, const double* val, const double* eta, const double* chi,
                                 double* s_io, double* t_io, double* q_out, double tol, int imax, int* iters, double* rel,
                                 double* scratch) {
@@ -102,7 +104,7 @@ __global__ void k_cg_csr_static(int n, const int* rs, const int* col, const doub
   __syncthreads();
   const double bnorm_s = sqrt(loc[0]), bnorm_t = sqrt(loc[1]);
   double sig_s = loc[2], sig_t = loc[3];
-  bool act_s = true, act_t = true;
+  bool act_s = true, act_t = true, broke_s = false, broke_t = false;
   int it_s = 1, it_t = 1;
   for (int it = 1; it < imax; ++it) {
     act_s = act_s && (sqrt(sig_s) / bnorm_s > tol);
@@ -120,7 +122,11 @@ __global__ void k_cg_csr_static(int n, const int* rs, const int* col, const doub
     reduce(loc, 2);
     const double alpha_s = act_s ? sig_s / loc[0] : 0.0;
     const double alpha_t = act_t ? sig_t / loc[1] : 0.0;
-    if (!(isfinite(alpha_s) && isfinite(alpha_t))) break;
+    if (!(isfinite(alpha_s) && isfinite(alpha_t))) {
+      broke_s = !isfinite(alpha_s);
+      broke_t = !isfinite(alpha_t);
+      break;
+    }
     loc[0] = loc[1] = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const double2 dd = d[i], qq = qv[i];
@@ -154,7 +160,7 @@ __global__ void k_cg_csr_static(int n, const int* rs, const int* col, const doub
   const double u = loc[0] / loc[1];
   for (int i = threadIdx.x; i < n; i += blockDim.x) q_out[i] = s_io[i] - u * t_io[i];
   if (threadIdx.x == 0) {
-    if (iters) { iters[0] = it_s; iters[1] = it_t; }
+    if (iters) { iters[0] = broke_s ? -1 : it_s; iters[1] = broke_t ? -1 : it_t; }
     if (rel) { rel[0] = sqrt(sig_s) / bnorm_s; rel[1] = sqrt(sig_t) / bnorm_t; }
   }
 }
@@ -166,18 +172,18 @@ extern "C" int rx_qeq_solve_static(int n, const int* row_start, const int* col, 
                                    const double* chi, double* s, double* t, double* q, double tol, int imax, int* iters,
                                    double* rel, void* stream, char* err, int errlen) {
   using namespace rx;
-  if (n <= 0 || n > kStaticMaxAtoms) {
+  if (n < 0 || n > kStaticMaxAtoms) {
     char m[160];
-    std::snprintf(m, sizeof m, "rx_qeq_solve_static: %d atoms; this entry point takes 1 to %d atoms (its fixed work array)", n,
+    std::snprintf(m, sizeof m, "rx_qeq_solve_static: %d atoms; this entry point takes 0 (set-up only) to %d atoms (its fixed work array)", n,
                   kStaticMaxAtoms);
     put_err(err, errlen, m);
     return RX_ERR_INVALID;
   }
-  if (!row_start || !col || !val || !eta || !chi || !s || !t || !q) {
+  if (n > 0 && (!row_start || !col || !val || !eta || !chi || !s || !t || !q)) {
     put_err(err, errlen, "rx_qeq_solve_static: null device array");
     return RX_ERR_INVALID;
   }
-  if (!(tol > 0.0) || imax < 1) {
+  if (n > 0 && (!(tol > 0.0) || imax < 1)) {
     put_err(err, errlen, "rx_qeq_solve_static: need tol > 0 and imax >= 1");
     return RX_ERR_INVALID;
   }
@@ -190,12 +196,16 @@ extern "C" int rx_qeq_solve_static(int n, const int* row_start, const int* col, 
   {
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_scratch[dev]) {
-      // the device address of the work array on this (current) device; the host-side name is not one
+      // the device address of the work array on this (current) device; the host-side name is not one. Looking it up
+      // loads this library's device code on the device (with the array) if lazy module loading has not done so yet;
+      // the kernel's attributes are queried too, so that its first launch loads nothing more.
       void* ptr = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&ptr, rx_qeq_static_scratch);
+      cudaError_t e = cudaGetSymbolAddress(&ptr, rx_qeq_static_scratch);
+      cudaFuncAttributes fa;
+      if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_cg_csr_static);
       if (e != cudaSuccess) {
         char m[200];
-        std::snprintf(m, sizeof m, "rx_qeq_solve_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        std::snprintf(m, sizeof m, "rx_qeq_solve_static: set-up on device %d failed: %s", dev, cudaGetErrorString(e));
         put_err(err, errlen, m);
         return RX_ERR_CUDA;
       }
@@ -203,9 +213,15 @@ extern "C" int rx_qeq_solve_static(int n, const int* row_start, const int* col, 
     }
     scratch = g_scratch[dev];
   }
+  if (n == 0) {   // set-up only
+    put_err(err, errlen, "");
+    return RX_OK;
+  }
   k_cg_csr_static<<<1, 512, 0, static_cast<cudaStream_t>(stream)>>>(n, row_start, col, val, eta, chi, s, t, q, tol, imax, iters,
                                                                      rel, scratch);
-  const cudaError_t e = cudaGetLastError();
+  // peek, not get: the error state is left as it is for the caller (an error still pending from earlier work on this
+  // thread is therefore reported here too)
+  const cudaError_t e = cudaPeekAtLastError();
   if (e != cudaSuccess) {
     char m[200];
     std::snprintf(m, sizeof m, "rx_qeq_solve_static: launch failed: %s", cudaGetErrorString(e));

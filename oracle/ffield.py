@@ -65,7 +65,10 @@ def _f(tok):
 
 def parse(text):
     rd = _Reader(text)
-    rd.values()  # header comment line
+    first = rd.values()  # header comment line (src/io/ffield_parser.cpp:100-115)
+    if (first and first[0].isdigit() and len(first) >= 2 and first[1].startswith("!")
+            and "general parameters" in " ".join(first) + " "):
+        raise FfieldError("first line of ReaxFF potential file must be a comment or empty")
     v = rd.values()
     ngp = int(v[0])
     if ngp < 38:
@@ -308,6 +311,8 @@ def oracle_arrays(t):
     for key, h in t["hbp"].items():
         hbp_on[key] = 1
         hbp[key] = [h[k] for k in HB_FIELDS]
-    return {"gp": np.array(t["gp"], dtype=np.float64), "sbp": np.ascontiguousarray(sbp), "tbp": np.ascontiguousarray(tbp),
+    gp = np.zeros(max(39, len(t["gp"])))   # a 38-parameter file has no p_coa3 (gp[38]): it reads 0, as on the device
+    gp[:len(t["gp"])] = t["gp"]
+    return {"gp": gp, "sbp": np.ascontiguousarray(sbp), "tbp": np.ascontiguousarray(tbp),
             "thb_n": thb_n, "thb": np.ascontiguousarray(thb), "fbp_on": fbp_on, "fbp": np.ascontiguousarray(fbp),
             "hbp_on": hbp_on, "hbp": np.ascontiguousarray(hbp)}

@@ -43,11 +43,16 @@ class _Box(ctypes.Structure):
     _fields_ = [("origin", _D * 3), ("vec", _D * 9), ("periodic", _I * 3)]
 
 
+def reference_dir_default():
+    """The reference checkout: $RX_REFERENCE_DIR, else a directory named `reference` beside this repository."""
+    return os.environ.get("RX_REFERENCE_DIR", str(HERE.parent.parent / "reference"))
+
+
 def build(reference_dir=None):
     """Compile the C restatement (always) and, when the reference tree exists, the reference oracle."""
     import subprocess
     subprocess.run(["make", "-s", "-C", str(HERE), "c"], check=True)
-    ref = reference_dir or os.environ.get("RX_REFERENCE_DIR", "/root/reference")
+    ref = reference_dir or reference_dir_default()
     if Path(ref, "src", "cpu", "bonded.cpp").exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", "REF=" + str(ref)], check=True)
 

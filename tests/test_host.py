@@ -63,10 +63,13 @@ def test_null_context_and_static_solve_argument_checks():
     out = np.zeros(3, dtype=np.int32)
     assert lib.rx_get_capacities(None, out.ctypes.data) == 1
     err = ctypes.create_string_buffer(256)
-    for n in (0, -5, 32769):
+    for n in (-5, 32769):
         assert lib.rx_qeq_solve_static(n, None, None, None, None, None, None, None, None, 1e-6, 10, None, None, None,
                                        err, 256) == 1
     assert b"32768" in err.value
+    # n = 0 is the set-up call: without a GPU it reports the CUDA error, with one it succeeds
+    assert lib.rx_qeq_solve_static(0, None, None, None, None, None, None, None, None, 0.0, 0, None, None, None,
+                                   err, 256) in (0, 4)
     dummy = ctypes.c_void_p(16)
     assert lib.rx_qeq_solve_static(10, None, dummy, dummy, dummy, dummy, dummy, dummy, dummy, 1e-6, 10, None, None,
                                    None, err, 256) == 1

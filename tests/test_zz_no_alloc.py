@@ -7,8 +7,9 @@ CG work vectors come from a fixed array the library reserves once per GPU.
 
 The test builds the charge matrix of a small periodic system on the host (every image within the taper radius summed
 into its entry), solves it twice in a row through the C ABI (the second call sees the work array exactly as the
-first call left it), and compares both results with the charges of rx_qeq_solve for the same system, within the
-charge tolerance of the parity tests (1e-10 e at tol 1e-12). This file is collected last on purpose.
+first call left it), and compares both results with the charges of rx_qeq_solve for the same system and with the
+oracle's, within the charge tolerance of the parity tests (1e-10 e at tol 1e-12); the device's free memory is
+checked before and after each call. This file is collected last on purpose.
 """
 import ctypes
 
@@ -86,21 +87,59 @@ def test_static_solve_matches_engine_solve():
     rel_d = torch.zeros(2, dtype=torch.float64, device=dev)
     lib = rxcuda.load()
     err = ctypes.create_string_buffer(256)
+    # the one-time set-up on this device (n = 0), as a caller would make it at start-up
+    assert lib.rx_qeq_solve_static(0, None, None, None, None, None, None, None, None, 0.0, 0, None, None, None, err,
+                                   256) == 0, err.value.decode()
+    torch.cuda.synchronize(dev)
     results = []
+    free_before = []
     for _ in range(2):     # two calls in a row: the second one starts from whatever the first left in the work array
         s_d = torch.zeros(n, dtype=torch.float64, device=dev)
         t_d = torch.zeros(n, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        free_before.append(torch.cuda.mem_get_info(dev)[0])
         rc = lib.rx_qeq_solve_static(n, rs_d.data_ptr(), col_d.data_ptr(), val_d.data_ptr(), eta_d.data_ptr(),
                                      chi_d.data_ptr(), s_d.data_ptr(), t_d.data_ptr(), q_d.data_ptr(), TOL, IMAX,
                                      it_d.data_ptr(), rel_d.data_ptr(), torch.cuda.current_stream(dev).cuda_stream, err, 256)
         assert rc == 0, err.value.decode()
         torch.cuda.synchronize(dev)
+        # the call allocated nothing: the device's free memory is what it was before the call
+        assert torch.cuda.mem_get_info(dev)[0] == free_before[-1]
         results.append((q_d.cpu().numpy().copy(), it_d.cpu().numpy().copy(), rel_d.cpu().numpy().copy()))
+    from oracle.oracle import COracle
+    orc = COracle(ffield_text(), shell=15.0).qeq(s, tol=TOL, imax=IMAX)
     for q, it, rel in results:
         assert np.abs(q - ref["q"]).max() <= 1e-10
+        assert np.abs(q - orc["q"]).max() <= 1e-10
         assert abs(q.sum()) <= 1e-9
-        assert rel.max() <= TOL and it.max() < IMAX
+        assert rel.max() <= TOL and 0 < it.min() and it.max() < IMAX
     assert np.array_equal(results[0][0], results[1][0])
+
+
+def test_static_solve_reports_breakdown():
+    """A singular matrix (eta = 1, H = -1 between two atoms) makes the first step length infinite: the call reports
+    iters = -1 for that right-hand side instead of a count that looks like convergence."""
+    import torch
+    import rxcuda
+    dev = torch.device("cuda", 0)
+    lib = rxcuda.load()
+    rs = torch.tensor([0, 1, 2], dtype=torch.int32, device=dev)
+    col = torch.tensor([1, 0], dtype=torch.int32, device=dev)
+    val = torch.tensor([-1.0, -1.0], dtype=torch.float64, device=dev)
+    eta = torch.ones(2, dtype=torch.float64, device=dev)
+    chi = torch.ones(2, dtype=torch.float64, device=dev)
+    s_d = torch.zeros(2, dtype=torch.float64, device=dev)
+    t_d = torch.zeros(2, dtype=torch.float64, device=dev)
+    q_d = torch.zeros(2, dtype=torch.float64, device=dev)
+    it_d = torch.zeros(2, dtype=torch.int32, device=dev)
+    rel_d = torch.zeros(2, dtype=torch.float64, device=dev)
+    err = ctypes.create_string_buffer(256)
+    rc = lib.rx_qeq_solve_static(2, rs.data_ptr(), col.data_ptr(), val.data_ptr(), eta.data_ptr(), chi.data_ptr(),
+                                 s_d.data_ptr(), t_d.data_ptr(), q_d.data_ptr(), 1e-10, 50, it_d.data_ptr(),
+                                 rel_d.data_ptr(), torch.cuda.current_stream(dev).cuda_stream, err, 256)
+    assert rc == 0, err.value.decode()
+    torch.cuda.synchronize(dev)
+    assert it_d.cpu().numpy().tolist() == [-1, -1]
 
 
 def test_static_solve_rejects_too_many_atoms():
