@@ -99,6 +99,14 @@ int rx_qeq_last(const rx_context* ctx, int32_t* iters, double* rel);
  * counted non-bonded pairs, neighbor entries, H-bond triples). Any output pointer may be NULL. */
 int rx_compute(rx_context* ctx, int flags, double* energies, double* grad, int32_t* census, int64_t* counts);
 
+/* Virial of the most recent force evaluation (rx_compute or the last rx_md_run step) per system: virial[6*nsys] in
+ * LAMMPS's order xx, yy, zz, xy, xz, yz, the sum of x_a f_b over every atom and periodic image (kcal/mol) - what
+ * virial_fdotr_compute() makes of the owned + ghost forces the reference's pair style hands LAMMPS
+ * (pair_reaxff_metal.cpp:500-504,523). rx_compute returns forces folded onto owned atoms, so a LAMMPS adapter sets
+ * the pair's virial from this array instead of calling virial_fdotr_compute(). Computed on the device from relative
+ * positions inside each interaction, in fixed order. */
+int rx_get_virial(rx_context* ctx, double* virial);
+
 /* Nose-Hoover chain NVT (the LAMMPS `fix nvt temp Tstart Tstop Tdamp` the reference's examples run), velocity Verlet
  * with dt [fs]. mass[ntypes] g/mol per force-field type. Charges are re-equilibrated before every force evaluation. */
 int rx_md_setup(rx_context* ctx, const double* mass, double dt, double t_start, double t_stop, double t_damp, int chain);

@@ -19,6 +19,7 @@ namespace rx {
 
 constexpr int kTerms = 13;   // bond, over, under, lone_pair, valence, penalty, coalition, hbond, torsion, conjugation, vdw, coulomb, polarization
 constexpr int kCensus = 7;   // bonds, angle_sets, torsions, hbonds, nonbonded, sbo_region, lp_trunc
+constexpr int kVir = 6;      // virial components in LAMMPS's order: xx, yy, zz, xy, xz, yz (sum of x_a f_b)
 enum Term { E_BOND, E_OV, E_UN, E_LP, E_ANG, E_PEN, E_COA, E_HB, E_TOR, E_CON, E_VDW, E_ELE, E_POL };
 
 // status bits written by kernels (read by the host after a launch sequence)
@@ -128,6 +129,7 @@ struct Dev {
   double4* fnb;          // non-bonded gradient
   double4* grad;         // result
   double* eatom;         // kTerms per atom
+  double* vir;           // kVir per atom: virial of the interactions this atom centres (LAMMPS order xx yy zz xy xz yz)
   int* census;           // kCensus per atom (atom-major: census[c*na + a])
   int* status;
   long long* counters;   // [0] neighbor entries, [1] counted pairs, [2] bonds (directed), [3] H-bond triples
@@ -169,6 +171,15 @@ __device__ inline void pair_dvec(const Dev& d, const SysInfo& s, int i, int j, i
 // A list of this evaluation overflowed (the host grows it and repeats the evaluation): later kernels skip their work.
 __device__ inline bool lists_failed(const Dev& d) {
   return (*reinterpret_cast<volatile const int*>(d.status) & (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW | ST_BOND_OVERFLOW | ST_SHIFT_RANGE)) != 0;
+}
+
+// Virial of an interaction cluster, sum over its atoms of x_a f_b = -x_a g_b, taken with positions P relative to the
+// cluster's own atom (every term is translation invariant, so its gradients sum to zero and the origin drops out).
+// Accumulates -P (x) g into v[6] in LAMMPS's component order (virial_fdotr_compute: xx, yy, zz, xy, xz, yz).
+template <class T, class U>
+__device__ inline void vir_add(double* v, const T* P, const U* g, double scale = 1.0) {
+  const double p0 = P[0], p1 = P[1], p2 = P[2], g0 = g[0] * scale, g1 = g[1] * scale, g2 = g[2] * scale;
+  v[0] -= p0 * g0; v[1] -= p1 * g1; v[2] -= p2 * g2; v[3] -= p0 * g1; v[4] -= p0 * g2; v[5] -= p1 * g2;
 }
 
 __device__ inline double safe_exp(double v) { return exp(v > 700.0 ? 700.0 : v); }

@@ -115,7 +115,7 @@ struct Context {
   DBuf<AtomQ> aq;
   DBuf<int> census, status;
   DBuf<long long> counters;
-  DBuf<double> energies;
+  DBuf<double> energies, virial, vir;
   // QEq
   DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
   DBuf<double> cg_eta, cg_part, s_hist, t_hist, cg_rel;
@@ -321,6 +321,7 @@ struct Context {
     RXCU(cudaMemset(s_hist.p, 0, sizeof(double) * 4 * na));
     RXCU(cudaMemset(t_hist.p, 0, sizeof(double) * 4 * na));
     have_pos = false;
+    have_virial = false;
     md_ready = false;
     ncap = 0;
     bcap = 0;
@@ -430,6 +431,8 @@ struct Context {
     aq.ensure(n); census.ensure(n * kCensus);
     nbr_cnt.ensure(n); bcnt.ensure(n); near_cnt.ensure(n);
     energies.ensure(static_cast<size_t>(nsys) * kTerms);
+    virial.ensure(static_cast<size_t>(nsys) * kVir);
+    vir.ensure(n * kVir);
     cg_x.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
     cg_sys.ensure(nsys); cg_rb0.ensure(n); cg_rb1.ensure(n); cg_nlive.ensure(2);
@@ -462,7 +465,7 @@ struct Context {
     d.bcap = bcap; d.bcode = bcode.p; d.bsym = bsym.p; d.bcnt = bcnt.p; d.bdv = bdv.p; d.bBO = bBO.p; d.bdBOp = bdBOp.p;
     d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p;
     d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
-    d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.census = census.p; d.status = status.p;
+    d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.census = census.p; d.status = status.p;
     d.counters = counters.p;
     return d;
   }
@@ -644,9 +647,11 @@ struct Context {
                                                 " iterations (relative residual " + std::to_string(last_rel[k]) + ")");
   }
 
+  bool have_virial = false;
   void energy_sums() {
+    have_virial = true;
     ++launches;
-    k_energy_sum<<<dim3(nsys, kTerms), 256, 0, stream>>>(dev(), energies.p);
+    k_energy_sum<<<dim3(nsys, kTerms + kVir), 256, 0, stream>>>(dev(), energies.p, virial.p);
   }
 
   // ------------------------------------------------------------------ state I/O
@@ -702,6 +707,12 @@ struct Context {
       counts[2] = sn;
       counts[3] = hb;
     }
+  }
+
+  void get_virial(double* out) {
+    require_sys();
+    if (!have_virial) throw Error(RX_ERR_STATE, "no force evaluation yet");
+    RXCU(cudaMemcpy(out, virial.p, sizeof(double) * kVir * nsys, cudaMemcpyDeviceToHost));
   }
 
   void qeq_solve(int* iters, double* rel) {
@@ -1009,6 +1020,13 @@ int rx_set_velocities(rx_context* ctx, const double* v) { return guarded(ctx, [&
 int rx_get_velocities(rx_context* ctx, double* v) { return guarded(ctx, [&](rx::Context& c) { c.get_velocities(v); }); }
 int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature) {
   return guarded(ctx, [&](rx::Context& c) { c.md_run(nsteps, energies, temperature, 0); });
+}
+
+int rx_get_virial(rx_context* ctx, double* virial) {
+  return guarded(ctx, [&](rx::Context& c) {
+    if (!virial) throw rx::Error(RX_ERR_INVALID, "null virial array");
+    c.get_virial(virial);
+  });
 }
 
 int64_t rx_kernel_launches(const rx_context* ctx) { return (ctx && ctx->c) ? ctx->c->launches : 0; }

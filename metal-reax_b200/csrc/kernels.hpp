@@ -49,7 +49,7 @@ __global__ void k_cg_seg(Dev d, CgArgs a);
 __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, const double* t_hist);
 __global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist, int strict);
 __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y);
-__global__ void k_energy_sum(Dev d, double* out);
+__global__ void k_energy_sum(Dev d, double* out, double* out_vir);
 
 __global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl);
 __global__ void k_bond_sym(Dev d);

@@ -293,6 +293,7 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
   }
   double fj[3] = {0, 0, 0}, cdd = 0.0;
   double e_bond = 0, e_lp = 0, e_ov = 0, e_un = 0, e_ang = 0, e_pen = 0, e_coa = 0;
+  double vir[kVir] = {0, 0, 0, 0, 0, 0};
 
   // ---- bond energy (owned end chosen by tag order)
   {
@@ -532,6 +533,8 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
           add3(d.bfn[bi], CEval8, dci);
           fj[0] += CEval8 * dcj[0]; fj[1] += CEval8 * dcj[1]; fj[2] += CEval8 * dcj[2];
           add3(d.bfn[bk], CEval8, dck);
+          vir_add(vir, vi, dci, CEval8);
+          vir_add(vir, vk, dck, CEval8);
         }
       }
     }
@@ -550,6 +553,7 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
     d.census[1 * d.na + j] = nsets;
   }
   d.fown[j] = make_double4(fj[0], fj[1], fj[2], cdd);
+  for (int c = 0; c < kVir; ++c) d.vir[static_cast<size_t>(j) * kVir + c] = vir[c];   // first writer of the step
   double* ea = d.eatom + static_cast<size_t>(j) * kTerms;
   ea[E_BOND] = e_bond; ea[E_OV] = e_ov; ea[E_UN] = e_un; ea[E_LP] = e_lp;
   ea[E_ANG] = e_ang; ea[E_PEN] = e_pen; ea[E_COA] = e_coa;
@@ -625,6 +629,7 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
   const double hc2 = ctl.hbond_cut * ctl.hbond_cut;
   const size_t base = static_cast<size_t>(j) * d.bcap;
   double e = 0.0, fj0 = 0.0, fj1 = 0.0, fj2 = 0.0;
+  double vir[kVir] = {0, 0, 0, 0, 0, 0};
   int ntrip = 0;
   for (int pi = 0; pi < nb; ++pi) {
     const size_t bi = base + pi;
@@ -658,6 +663,13 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
       fj0 += o.CEhb2 * o.dtj[0] + c3 * vk[0];
       fj1 += o.CEhb2 * o.dtj[1] + c3 * vk[1];
       fj2 += o.CEhb2 * o.dtj[2] + c3 * vk[2];
+      // virial of the triple about the hydrogen: donor at the bond vector, acceptor at vk
+      const float gk[3] = {o.CEhb2 * o.dtk[0] - c3 * vk[0], o.CEhb2 * o.dtk[1] - c3 * vk[1], o.CEhb2 * o.dtk[2] - c3 * vk[2]};
+      const float gi[3] = {o.CEhb2 * o.dti[0], o.CEhb2 * o.dti[1], o.CEhb2 * o.dti[2]};
+      const double4 dvi = d.bdv[bi];
+      const double pi3[3] = {dvi.x, dvi.y, dvi.z};
+      vir_add(vir, pi3, gi);
+      vir_add(vir, vk, gk);
     }
     c1 = warp_sum(c1); fi0 = warp_sum(fi0); fi1 = warp_sum(fi1); fi2 = warp_sum(fi2);
     if (lane == 0) {
@@ -669,11 +681,13 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
     __syncwarp();
   }
   e = warp_sum(e); fj0 = warp_sum(fj0); fj1 = warp_sum(fj1); fj2 = warp_sum(fj2);
+  for (int c = 0; c < kVir; ++c) vir[c] = warp_sum(vir[c]);
   for (int o = 16; o > 0; o >>= 1) ntrip += __shfl_xor_sync(0xffffffffu, ntrip, o);
   if (lane == 0) {
     double4 f = d.fown[j];
     f.x += fj0; f.y += fj1; f.z += fj2;
     d.fown[j] = f;
+    for (int c = 0; c < kVir; ++c) d.vir[static_cast<size_t>(j) * kVir + c] += vir[c];
     d.eatom[static_cast<size_t>(j) * kTerms + E_HB] = e;
     d.census[3 * d.na + j] = ntrip;
   }
@@ -748,6 +762,7 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
     for (int q = 0; q < nbk; ++q) d.Tl[(base + c) * d.bcap + q] = make_double4(0, 0, 0, 0);
   }
   double fj[3] = {0, 0, 0}, cdd = 0.0, e_tor = 0.0, e_con = 0.0;
+  double vir[kVir] = {0, 0, 0, 0, 0, 0};
   int ntor = 0;
   const double Delta_j = d.aq[j].Delta_boc;
   for (int pk = 0; pk < nbj; ++pk) {
@@ -912,20 +927,31 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
         const double c78 = CEtors7 + CEconj4, c85 = CEtors8 + CEconj5, c96 = CEtors9 + CEconj6;
         double4 fi = d.bfn[bij];
         double4 fk = d.bfn[bjk];
+        double gi[3], gk[3], gl[3];
         for (int c = 0; c < 3; ++c) {
-          (&fi.x)[c] += c78 * pijk_dk[c] + c96 * dco_i[c];
+          gi[c] = c78 * pijk_dk[c] + c96 * dco_i[c];
+          gk[c] = c78 * pijk_di[c] + c85 * pjkl_dj[c] + c96 * dco_k[c];
+          gl[c] = c85 * pjkl_dk[c] + c96 * dco_l[c];
+          (&fi.x)[c] += gi[c];
           fj[c] += c78 * pijk_dj[c] + c85 * pjkl_di[c] + c96 * dco_j[c];
-          (&fk.x)[c] += c78 * pijk_di[c] + c85 * pjkl_dj[c] + c96 * dco_k[c];
-          (&tl.x)[c] += c85 * pjkl_dk[c] + c96 * dco_l[c];
+          (&fk.x)[c] += gk[c];
+          (&tl.x)[c] += gl[c];
         }
         d.bfn[bij] = fi;
         d.bfn[bjk] = fk;
+        {   // virial about j: i at dij, k at djk, l at djk + dkl
+          const double pl[3] = {djk[0] + dkl[0], djk[1] + dkl[1], djk[2] + dkl[2]};
+          vir_add(vir, dij, gi);
+          vir_add(vir, djk, gk);
+          vir_add(vir, pl, gl);
+        }
       }
     }
   }
   double4 f = d.fown[j];
   f.x += fj[0]; f.y += fj[1]; f.z += fj[2]; f.w += cdd;
   d.fown[j] = f;
+  for (int c = 0; c < kVir; ++c) d.vir[static_cast<size_t>(j) * kVir + c] += vir[c];
   d.eatom[static_cast<size_t>(j) * kTerms + E_TOR] = e_tor;
   d.eatom[static_cast<size_t>(j) * kTerms + E_CON] = e_con;
   d.census[2 * d.na + j] = ntor;
@@ -968,6 +994,7 @@ __global__ void k_dbond(Dev d) {
   const int nb = min(d.bcnt[a], d.bcap);
   const size_t base = static_cast<size_t>(a) * d.bcap;
   double f[3] = {0, 0, 0}, W = 0.0;
+  double vir[kVir] = {0, 0, 0, 0, 0, 0}, vw[kVir] = {0, 0, 0, 0, 0, 0};
   const double cda = d.cdtot[a];
   for (int k = 0; k < nb; ++k) {
     const size_t b = base + k;
@@ -980,15 +1007,24 @@ __global__ void k_dbond(Dev d) {
     const double Xs = C0.y * c_bo + C0.y * c_dd + C1.y * c_pi + C2.y * c_pi2;
     const double Ypi = C0.w * c_pi, Ypi2 = C1.w * c_pi2;
     const double4 g = d.bdBOp[b], l1 = d.bdlnpi[b], l2 = d.bdlnpi2[b];
-    f[0] += X1 * g.x + Ypi * l1.x + Ypi2 * l2.x;
-    f[1] += X1 * g.y + Ypi * l1.y + Ypi2 * l2.y;
-    f[2] += X1 * g.z + Ypi * l1.z + Ypi2 * l2.z;
+    const double u[3] = {X1 * g.x + Ypi * l1.x + Ypi2 * l2.x, X1 * g.y + Ypi * l1.y + Ypi2 * l2.y, X1 * g.z + Ypi * l1.z + Ypi2 * l2.z};
+    f[0] += u[0];
+    f[1] += u[1];
+    f[2] += u[2];
     W += Xs;
+    // virial: u acts on a and -u on p (the reverse slot computes the same pair), so each slot carries half of it;
+    // the dDeltap_self part W dBOp(a->p) pairs with -W dBOp(a->p) that p gathers in k_force_final: whole here
+    const double4 dv = d.bdv[b];
+    const double P[3] = {-dv.x, -dv.y, -dv.z};
+    const double gg[3] = {g.x, g.y, g.z};
+    vir_add(vir, P, u, 0.5);
+    vir_add(vw, P, gg);
   }
   const double4 ds = d.dDp_self[a];
   f[0] += W * ds.x; f[1] += W * ds.y; f[2] += W * ds.z;
   d.W[a] = W;
   d.fdb[a] = make_double4(f[0], f[1], f[2], 0.0);
+  for (int c = 0; c < kVir; ++c) d.vir[static_cast<size_t>(a) * kVir + c] += vir[c] + W * vw[c];
 }
 
 __global__ void k_force_final(Dev d) {

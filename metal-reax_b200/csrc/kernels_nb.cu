@@ -222,6 +222,7 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
   const long long tag_i = d.tag[i];
   const int center = (d.S * d.S * d.S - 1) / 2;
   double gx = 0, gy = 0, gz = 0, ev = 0, ee = 0;
+  double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;   // pair virial, half per directed entry
   int counted = 0;
   for (int e = lane; e < cnt; e += 32) {
     const unsigned code = d.nbr[static_cast<size_t>(i) * d.ncap + e];
@@ -278,6 +279,11 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     gx -= static_cast<double>(CE * dx);
     gy -= static_cast<double>(CE * dy);
     gz -= static_cast<double>(CE * dz);
+    {   // the gradient -CE dv on i and +CE dv on the partner: virial -CE dv (x) dv, half of it from each direction
+      const double c = -0.5 * static_cast<double>(CE);
+      v0 += c * dvd[0] * dvd[0]; v1 += c * dvd[1] * dvd[1]; v2 += c * dvd[2] * dvd[2];
+      v3 += c * dvd[0] * dvd[1]; v4 += c * dvd[0] * dvd[2]; v5 += c * dvd[1] * dvd[2];
+    }
     // owner-computes counting of the energy
     bool count = false;
     if (sidx == center) count = j > i;
@@ -300,9 +306,12 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     }
   }
   gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); ev = warp_sum(ev); ee = warp_sum(ee);
+  v0 = warp_sum(v0); v1 = warp_sum(v1); v2 = warp_sum(v2); v3 = warp_sum(v3); v4 = warp_sum(v4); v5 = warp_sum(v5);
   for (int o = 16; o > 0; o >>= 1) counted += __shfl_xor_sync(0xffffffffu, counted, o);
   if (lane == 0) {
     d.fnb[i] = make_double4(gx, gy, gz, 0.0);
+    double* vi = d.vir + static_cast<size_t>(i) * kVir;
+    vi[0] += v0; vi[1] += v1; vi[2] += v2; vi[3] += v3; vi[4] += v4; vi[5] += v5;
     d.eatom[static_cast<size_t>(i) * kTerms + E_VDW] = ev;
     d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] = ee;
     const double chi = ff.sb[ti * SB_N + SB_CHI], eta = ff.sb[ti * SB_N + SB_ETA], qd = d.q[i];
@@ -757,20 +766,26 @@ __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y) {
 }
 
 // ------------------------------------------------------------------------------------------------ energy sums
-// Per system, per term: fixed-order sum over the system's atoms (one block per system and term).
-__global__ void k_energy_sum(Dev d, double* out) {
+// Per system, per term: fixed-order sum over the system's atoms (one block per system and term). Terms kTerms ..
+// kTerms + kVir - 1 are the virial components, written to out_vir.
+__global__ void k_energy_sum(Dev d, double* out, double* out_vir) {
   const int sidx = blockIdx.x, t = blockIdx.y;
   const SysInfo s = d.sys[sidx];
   __shared__ double sh[256];
   double v = 0.0;
-  for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) v += d.eatom[static_cast<size_t>(s.begin + r) * kTerms + t];
+  const double* src = t < kTerms ? d.eatom + t : d.vir + (t - kTerms);
+  const int stride = t < kTerms ? kTerms : kVir;
+  for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) v += src[static_cast<size_t>(s.begin + r) * stride];
   sh[threadIdx.x] = v;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[sidx * kTerms + t] = sh[0];
+  if (threadIdx.x == 0) {
+    if (t < kTerms) out[sidx * kTerms + t] = sh[0];
+    else out_vir[sidx * kVir + (t - kTerms)] = sh[0];
+  }
 }
 
 }  // namespace rx

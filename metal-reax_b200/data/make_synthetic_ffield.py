@@ -16,7 +16,7 @@ path is active:
   * lone pair, over/under coordination, angles with positive and negative p_val1, penalty, coalition;
   * explicit and 0-X-Y-0 torsions, O-H...O hydrogen bonds, and the light-element valency override for O.
 
-Run:  python make_synthetic_ffield.py [output path]
+Run:  python make_synthetic_ffield.py [output path [variant]]   (variants: see VARIANTS)
 """
 import sys
 from pathlib import Path
@@ -138,20 +138,46 @@ def fmt(v):
     return f"{v:10.4f}"
 
 
-def render():
-    out = ["Synthetic C/H/O ReaxFF parameter set (not the published CHO file; see make_synthetic_ffield.py)"]
-    out.append(f"{len(GENERAL):3d}       ! Number of general parameters")
-    for i, v in enumerate(GENERAL):
+# lgvdw data per element (fifth atom line): lgcij, lgre; the off-diagonal lines then carry an lgcij column
+LG = {"C": (400.0, 1.95), "H": (30.0, 1.40), "O": (150.0, 1.75)}
+OFFDIAG_LG = {(1, 2): 110.0, (1, 3): -1.0, (2, 3): 60.0}
+
+# variants of the file that switch the non-bonded branches (the van der Waals method follows from the atom lines,
+# src/io/ffield_parser.cpp:207-230): "vdw3" inner wall + shielding (the default), "vdw1" shielding only (no inner
+# wall: rcore2 = acore2 = 0), "vdw2" inner wall only (gamma_w <= 0.5), "lg" the default with lgvdw data (read with
+# `lgvdw yes`; gp[35] = 0.5 so that lgre = sqrt(lgre_i lgre_j))
+VARIANTS = ("vdw3", "vdw1", "vdw2", "lg")
+
+
+def render(variant="vdw3"):
+    if variant not in VARIANTS:
+        raise ValueError("unknown variant %r" % variant)
+    general = list(GENERAL)
+    atoms = [(n, list(l1), list(l2), list(l3), list(l4)) for n, l1, l2, l3, l4 in ATOMS]
+    if variant == "vdw1":
+        for a in atoms:
+            a[4][5] = a[4][7] = 0.0
+    elif variant == "vdw2":
+        for a in atoms:
+            a[2][1] = 0.4
+    elif variant == "lg":
+        general[35] = 0.5
+    title = "Synthetic C/H/O ReaxFF parameter set (not the published CHO file; see make_synthetic_ffield.py)"
+    out = [title if variant == "vdw3" else title + " variant " + variant]
+    out.append(f"{len(general):3d}       ! Number of general parameters")
+    for i, v in enumerate(general):
         out.append(f"{fmt(v)} !gp{i}")
     out.append(f"{len(ATOMS):3d}    ! Nr of atoms; cov.r; valency;a.m;Rvdw;Evdw;gammaEEM;cov.r2;#")
     out.append("            alfa;gammavdW;valency;Eunder;Eover;chiEEM;etaEEM;n.u.")
     out.append("            cov r3;Elp;Heat inc.;n.u.;n.u.;n.u.;n.u.")
     out.append("            ov/un;val1;n.u.;val3,vval4")
-    for name, l1, l2, l3, l4 in ATOMS:
+    for name, l1, l2, l3, l4 in atoms:
         out.append(f" {name:<2}" + "".join(fmt(v) for v in l1))
         out.append("   " + "".join(fmt(v) for v in l2))
         out.append("   " + "".join(fmt(v) for v in l3))
         out.append("   " + "".join(fmt(v) for v in l4))
+        if variant == "lg":
+            out.append("   " + "".join(fmt(v) for v in LG[name]))
     out.append(f"{len(BONDS):3d}      ! Nr of bonds; Edis1;LPpen;n.u.;pbe1;pbo5;13corr;pbo6")
     out.append("                         pbe2;pbo3;pbo4;n.u.;pbo1;pbo2;ovcorr")
     for i, j, l1, l2 in BONDS:
@@ -159,7 +185,8 @@ def render():
         out.append("      " + "".join(fmt(v) for v in l2))
     out.append(f"{len(OFFDIAG):3d}    ! Nr of off-diagonal terms; at1;at2;Dij;RvdW;alfa;ro(sigma);ro(pi);ro(pipi)")
     for i, j, vals in OFFDIAG:
-        out.append(f"{i:3d}{j:3d}" + "".join(fmt(v) for v in vals))
+        extra = [OFFDIAG_LG[(i, j)]] if variant == "lg" else []
+        out.append(f"{i:3d}{j:3d}" + "".join(fmt(v) for v in list(vals) + extra))
     out.append(f"{len(ANGLES):3d}    ! Nr of angles;at1;at2;at3;Thetao,o;ka;kb;pv1;pv2")
     for i, j, k, vals in ANGLES:
         out.append(f"{i:3d}{j:3d}{k:3d}" + "".join(fmt(v) for v in vals))
@@ -174,7 +201,8 @@ def render():
 
 def main():
     path = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).with_name("ffield.synthetic.cho")
-    path.write_text(render())
+    variant = sys.argv[2] if len(sys.argv) > 2 else "vdw3"
+    path.write_text(render(variant))
     print(path)
 
 

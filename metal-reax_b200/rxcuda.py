@@ -31,7 +31,7 @@ EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
-           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last"]
+           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -70,7 +70,7 @@ def load():
         "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
         "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
-        "rx_qeq_last": (_I, [_V, _V, _V]),
+        "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -186,6 +186,12 @@ class Engine:
         if counts:
             out["counts"] = cnt
         return out
+
+    def virial(self):
+        """LAMMPS-order virial (xx, yy, zz, xy, xz, yz) of the last force evaluation, per system."""
+        v = np.zeros(6 * self.nsys)
+        self._check(self.lib.rx_get_virial(self.h, _p(v)))
+        return v.reshape(self.nsys, 6)
 
     def qeq_solve(self):
         it = np.zeros(2 * self.nsys, dtype=np.int32)

@@ -63,7 +63,9 @@ def _f(tok):
     return v
 
 
-def parse(text):
+def parse(text, lgvdw=False):
+    """The reader's tables; lgvdw=True reads `pair_style reaxff lgvdw yes` files (a fifth line per element with lgcij
+    and lgre, an lgcij column on the off-diagonal lines: src/io/ffield_parser.cpp:196-205,314-330)."""
     rd = _Reader(text)
     first = rd.values()  # header comment line (src/io/ffield_parser.cpp:100-115)
     if (first and first[0].isdigit() and len(first) >= 2 and first[1].startswith("!")
@@ -104,7 +106,17 @@ def parse(text):
             raise FfieldError("atom line 4 needs 8 columns")
         s["p_ovun2"], s["p_val3"] = _f(t[0]), _f(t[1])
         s["valency_val"], s["p_val5"], s["rcore2"], s["ecore2"], s["acore2"] = (_f(x) for x in t[3:8])
-        s["lgcij"] = s["lgre"] = 0.0
+        if lgvdw:
+            t = rd.values()
+            try:
+                float(t[0])
+            except ValueError:
+                raise FfieldError("ReaxFF potential file is not compatible with 'lgvdw yes'")
+            if len(t) < 2:
+                raise FfieldError("lgvdw line needs 2 columns")
+            s["lgcij"], s["lgre"] = _f(t[0]), _f(t[1])
+        else:
+            s["lgcij"] = s["lgre"] = 0.0
         inner = s["rcore2"] > 0.01 and s["acore2"] > 0.01
         shield = s["gamma_w"] > 0.5
         want = 3 if (inner and shield) else 2 if inner else 1 if shield else 0
@@ -162,6 +174,8 @@ def parse(text):
     no = int(rd.values()[0])
     for _ in range(no):
         t = rd.values()
+        if len(t) < 8 + (1 if lgvdw else 0):
+            raise FfieldError("off-diagonal line needs %d columns" % (8 + (1 if lgvdw else 0)))
         j, k = int(t[0]) - 1, int(t[1]) - 1
         if j < nt and k < nt:
             for key, tok, scale in (("D", t[2], 1.0), ("r_vdW", t[3], 2.0), ("alpha", t[4], 1.0), ("r_s", t[5], 1.0),
@@ -170,6 +184,11 @@ def parse(text):
                 if val > 0.0:
                     tb[j][k][key] = scale * val
                     tb[k][j][key] = scale * val
+            if lgvdw:
+                val = _f(t[8])
+                if val >= 0.0:
+                    tb[j][k]["lgcij"] = val
+                    tb[k][j]["lgcij"] = val
     thb = {}
     slots = {}
     n3 = int(rd.values()[0])

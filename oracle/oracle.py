@@ -32,7 +32,8 @@ def _ptr(a):
 
 class _FF(ctypes.Structure):
     _fields_ = [("nt", _I), ("ngp", _I), ("gp", _V), ("vdw_type", _I), ("bo_cut", _D), ("nonb_low", _D), ("nonb_cut", _D),
-                ("sbp", _V), ("tbp", _V), ("thb_n", _V), ("thb", _V), ("fbp_on", _V), ("fbp", _V), ("hbp_on", _V), ("hbp", _V)]
+                ("sbp", _V), ("tbp", _V), ("thb_n", _V), ("thb", _V), ("fbp_on", _V), ("fbp", _V), ("hbp_on", _V), ("hbp", _V),
+                ("lgvdw", _I)]
 
 
 class _Ctl(ctypes.Structure):
@@ -71,19 +72,20 @@ def _box_struct(system):
 class COracle:
     """The C restatement. `ffield_text` is parsed by the Python restatement of the reader (oracle/ffield.py)."""
 
-    def __init__(self, ffield_text, bond_cut=5.0, hbond_cut=7.5, thb_cut=0.001, thb_cutsq=0.00001, enobonds=True, shell=12.0):
+    def __init__(self, ffield_text, bond_cut=5.0, hbond_cut=7.5, thb_cut=0.001, thb_cutsq=0.00001, enobonds=True, shell=12.0,
+                 lgvdw=False):
         path = HERE / "_c" / "librxoracle.so"
         if not path.exists():
             build()
         self.lib = ctypes.CDLL(str(path))
-        self.tables = _ff.parse(ffield_text)
+        self.tables = _ff.parse(ffield_text, lgvdw=lgvdw)
         self.arr = _ff.oracle_arrays(self.tables)
         a = self.arr
         self.ff = _FF(self.tables["nt"], len(self.tables["gp"]), _ptr(a["gp"]), self.tables["vdw_type"], self.tables["bo_cut"],
                       self.tables["nonb_low"], self.tables["nonb_cut"], _ptr(a["sbp"]), _ptr(a["tbp"]), _ptr(a["thb_n"]),
-                      _ptr(a["thb"]), _ptr(a["fbp_on"]), _ptr(a["fbp"]), _ptr(a["hbp_on"]), _ptr(a["hbp"]))
+                      _ptr(a["thb"]), _ptr(a["fbp_on"]), _ptr(a["fbp"]), _ptr(a["hbp_on"]), _ptr(a["hbp"]), 1 if lgvdw else 0)
         self.ctl = _Ctl(bond_cut, hbond_cut, thb_cut, thb_cutsq, 1 if enobonds else 0, shell)
-        self.lib.rxo_single_point.argtypes = [_V, _V, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V, ctypes.c_char_p, _I]
+        self.lib.rxo_single_point.argtypes = [_V, _V, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V, _V, ctypes.c_char_p, _I]
         self.lib.rxo_qeq.argtypes = [_V, _V, _V, _I, _V, _V, _V, _D, _D, _D, _I, _V, _V, _V, _V, _V, _V, _V, ctypes.c_char_p, _I]
         self.lib.rxo_qeq_matvec.argtypes = [_V, _V, _V, _I, _V, _V, _V, _D, _D, _V, _V, ctypes.c_char_p, _I]
 
@@ -100,13 +102,14 @@ class COracle:
         g = np.zeros(3 * n)
         cen = np.zeros(7 * n, dtype=np.int32)
         cnt = np.zeros(4, dtype=np.int64)
+        vir = np.zeros(6)
         err = ctypes.create_string_buffer(512)
         box = _box_struct(system)
         rc = self.lib.rxo_single_point(ctypes.byref(self.ff), ctypes.byref(self.ctl), ctypes.byref(box), n, _ptr(x), _ptr(ty),
-                                       _ptr(tg), _ptr(qq), _ptr(e), _ptr(g), _ptr(cen), _ptr(cnt), err, 512)
+                                       _ptr(tg), _ptr(qq), _ptr(e), _ptr(g), _ptr(cen), _ptr(cnt), _ptr(vir), err, 512)
         if rc:
             raise RuntimeError("oracle: " + err.value.decode())
-        return {"e": e, "grad": g.reshape(n, 3), "census": cen.reshape(7, n), "counts": cnt}
+        return {"e": e, "grad": g.reshape(n, 3), "census": cen.reshape(7, n), "counts": cnt, "virial": vir}
 
     def qeq(self, system, swa=0.0, swb=10.0, tol=1e-6, imax=200, s0=None, t0=None):
         n = len(system["type"])
@@ -151,12 +154,13 @@ class RefOracle:
     def available(cls):
         return cls.PATH.exists()
 
-    def __init__(self, ffield_text, bond_cut=5.0, hbond_cut=7.5, enobonds=True, shell=12.0):
+    def __init__(self, ffield_text, bond_cut=5.0, hbond_cut=7.5, enobonds=True, shell=12.0, lgvdw=False):
         self.lib = ctypes.CDLL(str(self.PATH))
         self.text = ffield_text.encode()
         self.bond_cut, self.hbond_cut, self.enobonds, self.shell = bond_cut, hbond_cut, enobonds, shell
-        self.lib.ref_single_point.argtypes = [ctypes.c_char_p, _V, _V, _V, _I, _V, _V, _V, _V, _D, _D, _D, _I, _V, _V, _V, _V,
-                                              ctypes.c_char_p, _I]
+        self.lgvdw = lgvdw
+        self.lib.ref_single_point.argtypes = [ctypes.c_char_p, _V, _V, _V, _I, _V, _V, _V, _V, _D, _D, _D, _I, _I, _V, _V, _V,
+                                              _V, _V, ctypes.c_char_p, _I]
         self.lib.ref_table_dump.argtypes = [ctypes.c_char_p, _I, ctypes.c_char_p, ctypes.c_long]
         self.lib.ref_table_dump.restype = ctypes.c_long
 
@@ -180,10 +184,12 @@ class RefOracle:
         g = np.zeros(3 * n)
         cen = np.zeros(7 * n, dtype=np.int32)
         cnt = np.zeros(4, dtype=np.int64)
+        vir = np.zeros(6)
         err = ctypes.create_string_buffer(512)
         rc = self.lib.ref_single_point(self.text, _ptr(org), _ptr(box), _ptr(per), n, _ptr(x), _ptr(ty), _ptr(tg), _ptr(qq),
-                                       self.bond_cut, self.hbond_cut, self.shell, 1 if self.enobonds else 0, _ptr(e), _ptr(g),
-                                       _ptr(cen), _ptr(cnt), err, 512)
+                                       self.bond_cut, self.hbond_cut, self.shell, 1 if self.enobonds else 0,
+                                       1 if self.lgvdw else 0, _ptr(e), _ptr(g),
+                                       _ptr(cen), _ptr(cnt), _ptr(vir), err, 512)
         if rc:
             raise RuntimeError("reference: " + err.value.decode())
-        return {"e": e, "grad": g.reshape(n, 3), "census": cen.reshape(7, n), "counts": cnt}
+        return {"e": e, "grad": g.reshape(n, 3), "census": cen.reshape(7, n), "counts": cnt, "virial": vir}

@@ -50,18 +50,24 @@ long ref_table_dump(const char* ffield_text, int portable, char* out, long outle
 // One single point of the cpu64 engine.
 //   box9: lattice vectors a, b, c (row-major); origin3; periodic3 (0/1)
 //   x: 3n owned coordinates, type: n force-field type indices (0-based), tag: n atom ids
+//   lgvdw: 1 reads and evaluates the force field as `pair_style reaxff lgvdw yes`
 //   q: n charges or NULL (NULL: the non-bonded terms are skipped, as energy_tool does without charges)
 //   e13: energies in EnergyTerm order (bond, over, under, lone_pair, valence, penalty, coalition, hbond,
 //        torsion, conjugation, vdw, coulomb, polarization), kcal/mol
 //   grad: 3n, dE/dx folded onto the owners (ghost gradient added to its owner)
 //   census: 7n int32 (bonds, angle_sets, torsions, hbonds, nonbonded, sbo_region, lp_trunc) or NULL
 //   counts: [undirected bonds incl. ghost rows, counted non-bonded pairs, nall, far-list entries]
+//   virial6: NULL or LAMMPS's fdotr virial of the owned + ghost forces the pair style hands LAMMPS
+//            (pair_reaxff_metal.cpp:500-504 then virial_fdotr_compute, :523): sum over nall of x_a f_b in the
+//            order xx, yy, zz, xy, xz, yz, f = -grad
 int ref_single_point(const char* ffield_text, const double* origin3, const double* box9, const int* periodic3, int n,
                      const double* x, const int* type, const long long* tag, const double* q, double bond_cut,
-                     double hbond_cut, double shell, int enobonds, double* e13, double* grad, int* census,
-                     long long* counts, char* err, int errlen) {
+                     double hbond_cut, double shell, int enobonds, int lgvdw, double* e13, double* grad, int* census,
+                     long long* counts, double* virial6, char* err, int errlen) {
   try {
-    const ForceField ff = parse_force_field(ffield_text, "ffield");
+    FfieldOptions fo;
+    fo.lgvdw = lgvdw != 0;
+    const ForceField ff = parse_force_field(ffield_text, "ffield", fo);
     ControlParams ctl;
     ctl.bond_cut = bond_cut;
     ctl.hbond_cut = hbond_cut;
@@ -90,6 +96,7 @@ int ref_single_point(const char* ffield_text, const double* origin3, const doubl
     if (q) {
       NonbondedOptions no;
       no.census = census != nullptr;
+      no.lgvdw = lgvdw != 0;
       std::vector<double> qv(q, q + n);
       nb = compute_nonbonded_core(ff, cut, a, f, qv, no);
     }
@@ -99,6 +106,18 @@ int ref_single_point(const char* ffield_text, const double* origin3, const doubl
       for (std::size_t c = 0; c < 3; ++c)
         g[3 * static_cast<std::size_t>(a.owner[i]) + c] += r.grad[3 * i + c] + (nb.grad.empty() ? 0.0 : nb.grad[3 * i + c]);
     std::memcpy(grad, g.data(), g.size() * sizeof(double));
+    if (virial6) {
+      for (int c = 0; c < 6; ++c) virial6[c] = 0.0;
+      for (std::size_t i = 0; i < a.nall(); ++i) {
+        double f[3], xi[3];
+        for (std::size_t c = 0; c < 3; ++c) {
+          f[c] = -(r.grad[3 * i + c] + (nb.grad.empty() ? 0.0 : nb.grad[3 * i + c]));
+          xi[c] = a.x[3 * i + c];
+        }
+        virial6[0] += f[0] * xi[0]; virial6[1] += f[1] * xi[1]; virial6[2] += f[2] * xi[2];
+        virial6[3] += f[1] * xi[0]; virial6[4] += f[2] * xi[0]; virial6[5] += f[2] * xi[1];
+      }
+    }
     if (census) {
       const std::vector<std::int32_t>* cols[7] = {&r.census.bonds, &r.census.angle_sets, &r.census.torsions, &r.census.hbonds,
                                                  &nb.census_nonbonded, &r.census.sbo_region, &r.census.lp_trunc};

@@ -1146,6 +1146,13 @@ static void nonbonded_core(const rxo_ff* ff, const atomset* a, const farlist* fa
         e_vdW += Tap * e_core;
         const double de_core = -(acore / rcore) * e_core;
         CEvd += dTap * e_core + Tap * de_core / r;
+        if (ff->lgvdw) {   /* include/reaxmetal/terms.hpp:308-314: nested in the inner-wall branch (Q-06) */
+          const double r_ij5 = pow(r, 5.0), r_ij6 = pow(r, 6.0), re6 = pow(TB(ti, tj, TB_LGRE), 6.0);
+          const double e_lg = -(TB(ti, tj, TB_LGCIJ) / (r_ij6 + re6));
+          e_vdW += Tap * e_lg;
+          const double de_lg = -6.0 * e_lg * r_ij5 / (r_ij6 + re6);
+          CEvd += dTap * e_lg + Tap * de_lg / r;
+        }
       }
       const double dr3gamij_1 = (r * r * r + TB(ti, tj, TB_GAMMA));
       const double dr3gamij_3 = pow(dr3gamij_1, 0.33333333333333);
@@ -1191,7 +1198,7 @@ static int setup(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, int n
 
 int rxo_single_point(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, int n, const double* x, const int* type,
                      const long long* tag, const double* q, double* e13, double* grad, int* census, long long* counts,
-                     char* err, int errlen) {
+                     double* virial6, char* err, int errlen) {
   atomset a;
   farlist far;
   int rc = setup(ff, ctl, box, n, x, type, tag, &a, &far, err, errlen);
@@ -1207,6 +1214,15 @@ int rxo_single_point(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, i
     memset(grad, 0, sizeof(double) * 3 * (size_t)n);
     for (int i = 0; i < N; ++i)
       for (int c = 0; c < 3; ++c) grad[3 * a.owner[i] + c] += f[3 * i + c];
+    if (virial6) {   /* LAMMPS virial_fdotr_compute over owned + ghost atoms, force = -gradient */
+      for (int c = 0; c < 6; ++c) virial6[c] = 0.0;
+      for (int i = 0; i < N; ++i) {
+        const double* xi = a.x + 3 * (size_t)i;
+        const double* gi = f + 3 * (size_t)i;
+        virial6[0] -= gi[0] * xi[0]; virial6[1] -= gi[1] * xi[1]; virial6[2] -= gi[2] * xi[2];
+        virial6[3] -= gi[1] * xi[0]; virial6[4] -= gi[2] * xi[0]; virial6[5] -= gi[2] * xi[1];
+      }
+    }
     if (counts) { counts[0] = nbonds; counts[1] = npairs; counts[2] = N; counts[3] = far.entries; }
   }
   free(f);

@@ -52,6 +52,7 @@ typedef struct {
   const double* fbp;      /* nt^4 * FB_NFIELDS */
   const int* hbp_on;      /* nt^3: H-bond entry exists (donor, H, acceptor) */
   const double* hbp;      /* nt^3 * HB_NFIELDS */
+  int lgvdw;              /* 1: `pair_style reaxff lgvdw yes` (the lg dispersion inside the inner-wall branch) */
 } rxo_ff;
 
 typedef struct {
@@ -74,11 +75,12 @@ typedef struct {
 /* One energy + gradient evaluation (bonded + non-bonded with the given charges; q == NULL skips the non-bonded
  * terms as the reference's driver does). grad: 3n, dE/dx folded onto the owned atoms. census: 7n (bonds,
  * angle_sets, torsions, hbonds, nonbonded, sbo_region, lp_trunc) or NULL. counts: [undirected bonds incl.
- * ghost rows, counted non-bonded pairs, nall, far-list entries] or NULL. Returns 0, or a nonzero error code
- * with a message in err. */
+ * ghost rows, counted non-bonded pairs, nall, far-list entries] or NULL. virial6: NULL or the LAMMPS fdotr virial
+ * (sum over owned + ghost atoms of x_a f_b, order xx yy zz xy xz yz, f = -gradient). Returns 0, or a nonzero error
+ * code with a message in err. */
 int rxo_single_point(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, int n, const double* x, const int* type,
                      const long long* tag, const double* q, double* e13, double* grad, int* census, long long* counts,
-                     char* err, int errlen);
+                     double* virial6, char* err, int errlen);
 
 /* Charge equilibration: solves H s = -chi and H t = -1 with the stock Jacobi-preconditioned CG (tolerance
  * sqrt(r.M^-1 r)/|b| <= tol, at most imax - 1 iterations) from the initial guesses s0/t0 (n each), then

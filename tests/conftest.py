@@ -2,7 +2,7 @@ import sys
 from pathlib import Path
 
 REPO = Path(__file__).resolve().parents[1]
-for p in (str(REPO), str(REPO / "metal-reax_b200")):
+for p in (str(REPO), str(REPO / "metal-reax_b200"), str(REPO / "metal-reax_b200" / "data")):
     if p not in sys.path:
         sys.path.insert(0, p)
 

@@ -1,0 +1,133 @@
+"""GPU parity on the benchmark workloads themselves: the 648-atom water box (216 H2O) and the 24,000-atom water box
+(8000 H2O) of the throughput measurement, at step 0 and at the frame the GPU's own NVT trajectory reaches after 100
+steps (dt 0.25 fs, 300 K, charges equilibrated every step at tol 1e-6), each frame re-evaluated on the CPU.
+
+The CPU side is the reference's own cpu64 engine compiled from its sources (RefOracle) where it was built, else the C
+restatement pinned to it (COracle); the charge solve is the oracle's restatement of the stock QEq CG.
+
+Bars (the reference's acceptance of an FP32 GPU engine against cpu64, tolerances/tolerances.json "C3"):
+  energy   |dE_total| / N <= 1e-3 kcal/mol/atom, and every term's |dE| / N within the same bar
+  force    max |dF| <= 0.05, RMS <= 5e-3 kcal/mol/A
+  virial   every component |dW| / N <= 1e-3 kcal/mol/atom (the energy bar: the virial is an energy)
+  census   every discrete decision identical atom by atom
+  charges  <= 1e-4 e with the same CG iteration counts at tol 1e-6 (step 0), <= 1e-10 e at tol 1e-12 (each frame)
+With RX_REPORT_DIR set, the measured per-term errors are written there as JSON.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import C3_ENERGY_PER_ATOM, C3_FORCE_MAX, C3_FORCE_RMS, ffield_text, force_metrics
+
+pytestmark = pytest.mark.gpu
+
+MASS = [12.0, 1.008, 15.999]
+TERMS = ["bond", "over", "under", "lone_pair", "valence", "penalty", "coalition", "hbond", "torsion", "conjugation", "vdw",
+         "coulomb", "polarization"]
+
+
+def _cpu_single_point(s, q):
+    from oracle.oracle import COracle, RefOracle
+    if RefOracle.available():
+        return RefOracle(ffield_text(), shell=15.0).single_point(s, q), "reference cpu64"
+    return COracle(ffield_text(), shell=15.0).single_point(s, q), "C restatement"
+
+
+def _compare(tag, s, out, vir, q, report):
+    ref, kind = _cpu_single_point(s, q)
+    n = len(s["type"])
+    de = np.abs(out["e"][0] - ref["e"])
+    fmax, frms = force_metrics(ref["grad"], out["grad"])
+    dv = np.abs(vir - ref["virial"])
+    rep = {"frame": tag, "atoms": n, "cpu": kind,
+           "term_abs_error_kcal": dict(zip(TERMS, de.tolist())),
+           "term_rel_error": dict(zip(TERMS, (de / np.maximum(1.0, np.abs(ref["e"]))).tolist())),
+           "total_error_per_atom": float(abs(out["e"][0].sum() - ref["e"].sum()) / n),
+           "force_max": fmax, "force_rms": frms,
+           "virial_abs_error": dv.tolist(), "virial_ref": ref["virial"].tolist()}
+    report.append(rep)
+    assert rep["total_error_per_atom"] <= C3_ENERGY_PER_ATOM, rep
+    assert (de / n).max() <= C3_ENERGY_PER_ATOM, rep
+    assert fmax <= C3_FORCE_MAX and frms <= C3_FORCE_RMS, rep
+    assert (dv / n).max() <= C3_ENERGY_PER_ATOM, rep
+    for k in range(7):
+        assert np.array_equal(out["census"][k], ref["census"][k]), (tag, k)
+
+
+def _write(name, report):
+    d = os.environ.get("RX_REPORT_DIR")
+    if d:
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, "parity_%s.json" % name), "w") as f:
+            json.dump(report, f, indent=1)
+
+
+@pytest.mark.parametrize("n_side", [6, 20], ids=["water648", "water24k"])
+def test_water_step0_and_trajectory_frame(n_side):
+    import rxcuda
+    import systems
+    from oracle.oracle import COracle
+    s = systems.water_box(n_side)
+    orc = COracle(ffield_text(), shell=15.0)
+    eng = rxcuda.Engine(0)
+    eng.set_forcefield(ffield_text())
+    eng.set_control()
+    eng.set_qeq(0.0, 10.0, 1e-6, 200)
+    eng.set_systems([s])
+    report = []
+    # ---- step 0: one energy + force + charge evaluation (charges from zero guesses, as the oracle's solve)
+    out = eng.compute(qeq=True, census=True, cold=True)
+    q = eng.get_charges()
+    it = eng.qeq_last()["iters"][0]
+    ref_q = orc.qeq(s, tol=1e-6, imax=200)
+    assert np.abs(q - ref_q["q"]).max() <= 1e-4
+    assert tuple(it) == tuple(ref_q["iters"])
+    _compare("step0", s, out, eng.virial()[0], q, report)
+    # ---- 100 NVT steps on the GPU, then the frame they reach, re-evaluated on the CPU
+    eng.md_setup(MASS, dt=0.25, t_start=300.0, t_damp=25.0, chain=3)
+    eng.set_velocities(systems.maxwell_velocities(s, 300.0, seed=11))
+    md = eng.md_run(100)
+    assert np.all(np.isfinite(md["e"])) and 100.0 < md["T"][0] < 900.0
+    frame = dict(s)
+    frame["x"] = eng.get_positions()
+    qf = eng.get_charges()
+    out = eng.compute(census=True)           # the frame with the trajectory's own charges
+    _compare("step100", frame, out, eng.virial()[0], qf, report)
+    # ---- a tight charge solve at that frame
+    eng.set_qeq(0.0, 10.0, 1e-12, 400)
+    got = eng.qeq_solve()
+    ref = orc.qeq(frame, tol=1e-12, imax=400)
+    report.append({"frame": "step100", "charge_max_error_tol1e-12": float(np.abs(got["q"] - ref["q"]).max())})
+    assert np.abs(got["q"] - ref["q"]).max() <= 1e-10
+    eng.close()
+    _write("water%d" % (3 * n_side ** 3), report)
+
+
+def test_energy_conservation_short_nve_like_run():
+    """With the thermostat coupled only weakly (a 1e6 fs damping time) the chain barely acts, so the 648-atom water
+    run conserves total energy: the drift over 200 steps stays far below the kinetic energy (a check of the integrator
+    and of force/energy consistency that needs no trajectory comparison)."""
+    import rxcuda
+    import systems
+    s = systems.water_box(6)
+    eng = rxcuda.Engine(0)
+    eng.set_forcefield(ffield_text())
+    eng.set_control()
+    eng.set_qeq(0.0, 10.0, 1e-10, 400)
+    eng.set_systems([s])
+    eng.md_setup(MASS, dt=0.1, t_start=300.0, t_damp=1e6, chain=1)
+    v = systems.maxwell_velocities(s, 300.0, seed=3)
+    eng.set_velocities(v)
+    m = np.array(MASS)[s["type"]]
+    etot = []
+    for _ in range(5):
+        r = eng.md_run(40)
+        vv = eng.get_velocities()
+        ke = 0.5 * (m[:, None] * vv ** 2).sum() / 4.184e-4     # g/mol A^2/fs^2 -> kcal/mol
+        etot.append(r["e"][0].sum() + ke)
+    eng.close()
+    n = len(s["type"])
+    drift = (max(etot) - min(etot)) / n
+    assert drift <= 5e-3, (etot, drift)

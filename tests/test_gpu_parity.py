@@ -277,3 +277,73 @@ def test_sparse_system_matches_oracle(engine, oracle):
     ref = oracle.qeq(s, tol=1e-12, imax=100)
     assert np.abs(got["q"] - ref["q"]).max() <= 1e-10
     engine.set_qeq()
+
+
+@pytest.mark.parametrize("idx", range(5))
+def test_virial_matches_oracle(engine, oracle, idx):
+    """The per-system virial (LAMMPS fdotr order xx yy zz xy xz yz) against the oracle's sum of x f over owned and
+    ghost atoms. Bars: each component within the C3 energy bar per atom (1e-3 kcal/mol/atom), and within 1e-6 of the
+    largest component (FP32 non-bonded and H-bond terms, FP64 elsewhere)."""
+    s = small_systems()[idx]
+    q = fixed_charges(s)
+    ref = oracle.single_point(s, q)
+    engine.set_systems([s])
+    engine.set_charges(q)
+    engine.compute()
+    w = engine.virial()[0]
+    n = len(s["type"])
+    dv = np.abs(w - ref["virial"])
+    assert dv.max() / n <= C3_ENERGY_PER_ATOM, (s["name"], w, ref["virial"])
+    assert dv.max() <= 1e-6 * np.abs(ref["virial"]).max(), (s["name"], w, ref["virial"])
+
+
+def test_virial_of_a_batch_is_per_system(engine):
+    """Each system's virial is the same alone and inside a batch."""
+    ss = small_systems()[1:4]
+    alone = []
+    for s in ss:
+        engine.set_systems([s])
+        engine.set_charges(fixed_charges(s))
+        engine.compute()
+        alone.append(engine.virial()[0])
+    engine.set_systems(ss)
+    engine.set_charges(np.concatenate([fixed_charges(s) for s in ss]))
+    engine.compute()
+    both = engine.virial()
+    for k in range(len(ss)):
+        assert np.array_equal(both[k], alone[k])
+
+
+@pytest.mark.parametrize("variant", ["vdw1", "vdw2", "lg"])
+def test_vdw_variants_match_oracle(variant):
+    """The non-bonded branches the default force field does not take: van der Waals with shielding only (type 1), inner
+    wall only (type 2), and the lg dispersion of `lgvdw yes` (include/reaxmetal/terms.hpp:280-323). Same bars as the
+    single-point test, on the water box and a mixed CHO system."""
+    import make_synthetic_ffield
+    import rxcuda
+    import systems
+    from oracle.oracle import COracle
+    text = make_synthetic_ffield.render(variant)
+    lg = variant == "lg"
+    orc = COracle(text, shell=15.0, lgvdw=lg)
+    eng = rxcuda.Engine(0)
+    eng.set_forcefield(text, lgvdw=lg)
+    eng.set_control()
+    for s in (systems.water_box(4), systems.random_cho(7)):
+        q = fixed_charges(s)
+        ref = orc.single_point(s, q)
+        eng.set_systems([s])
+        eng.set_charges(q)
+        out = eng.compute(census=True)
+        n = len(s["type"])
+        e, e_ref = out["e"][0], ref["e"]
+        rel = np.abs(e[FP64_TERMS] - e_ref[FP64_TERMS]) / np.maximum(1.0, np.abs(e_ref[FP64_TERMS]))
+        assert rel.max() <= 1e-7, (variant, s["name"])
+        assert abs(e[10] - e_ref[10]) <= 1e-5 * max(1.0, abs(e_ref[10])), (variant, s["name"], e[10], e_ref[10])
+        assert abs(e.sum() - e_ref.sum()) / n <= C3_ENERGY_PER_ATOM, (variant, s["name"])
+        fmax, frms = force_metrics(ref["grad"], out["grad"])
+        assert fmax <= C3_FORCE_MAX and frms <= C3_FORCE_RMS, (variant, s["name"], fmax, frms)
+        for k in range(7):
+            assert np.array_equal(out["census"][k], ref["census"][k]), (variant, s["name"], k)
+        assert np.abs(eng.virial()[0] - ref["virial"]).max() / n <= C3_ENERGY_PER_ATOM
+    eng.close()

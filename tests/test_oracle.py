@@ -35,14 +35,65 @@ def test_python_reader_matches_reference_dump():
     assert ffield.canonical_dump(ffield.parse(ffield_text())) == (GOLDEN / "ffield_synthetic.dump.txt").read_text()
 
 
-@pytest.mark.parametrize("name", ["water192", "cho3_108", "cho7_78", "cho11_141", "carbon200"])
-def test_oracle_matches_golden(coracle, name):
+@pytest.mark.parametrize("name", ["water192", "cho3_108", "cho7_78", "cho11_141", "carbon200",
+                                  "water192_vdw1", "water192_vdw2", "water192_lg"])
+def test_oracle_matches_golden(name):
+    """The C restatement against the reference's own outputs (energies, gradient, census, counts and the fdotr
+    virial), including the force-field variants that switch the non-bonded branches (vdW types 1 and 2, lgvdw)."""
+    from oracle.oracle import COracle
+    import make_synthetic_ffield
     s, z = _golden_system(GOLDEN / (name + ".npz"))
-    r = coracle.single_point(s, z["q"])
+    variant = name.rsplit("_", 1)[-1]
+    variant = variant if variant in make_synthetic_ffield.VARIANTS else "vdw3"
+    orc = COracle(make_synthetic_ffield.render(variant), shell=15.0, lgvdw=(variant == "lg"))
+    r = orc.single_point(s, z["q"])
     assert np.array_equal(r["census"], z["census"])
     assert np.array_equal(r["counts"], z["counts"])
     assert np.abs(r["e"] - z["e"]).max() <= 1e-9 * max(1.0, np.abs(z["e"]).max())
     assert np.abs(r["grad"] - z["grad"]).max() <= 1e-9
+    assert np.abs(r["virial"] - z["virial"]).max() <= 1e-9 * max(1.0, np.abs(z["virial"]).max())
+
+
+@pytest.mark.parametrize("idx", [0, 1, 4])
+def test_oracle_virial_is_the_strain_derivative(coracle, idx):
+    """An independent check of the virial's definition (every periodic image counted at its own position): under the
+    affine strain x_b -> x_b + eps x_a of the atoms and the lattice, dE/deps = -W_ab. Central differences of the
+    oracle's energy (charges held fixed) against its fdotr virial, within 1e-6 of the largest component."""
+    s = small_systems()[idx]
+    q = fixed_charges(s)
+    w = coracle.single_point(s, q)["virial"]
+
+    def energy(a, b, eps):
+        F = np.eye(3)
+        F[b, a] += eps
+        st = dict(s)
+        st["x"] = s["x"] @ F.T
+        st["box"] = np.asarray(s["box"]) @ F.T
+        st["origin"] = np.asarray(s["origin"]) @ F.T
+        return coracle.single_point(st, q)["e"].sum()
+
+    h = 1e-6
+    fd = np.array([-(energy(a, b, h) - energy(a, b, -h)) / (2 * h)
+                   for a, b in [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]])
+    assert np.abs(fd - w).max() <= 1e-6 * np.abs(w).max(), (fd, w)
+
+
+def test_oracle_variants_match_reference_live():
+    from oracle.oracle import COracle, RefOracle
+    import make_synthetic_ffield
+    import systems
+    if not RefOracle.available():
+        pytest.skip("reference oracle not built here")
+    s = systems.random_cho(7)
+    q = fixed_charges(s)
+    for v in make_synthetic_ffield.VARIANTS:
+        text = make_synthetic_ffield.render(v)
+        a = COracle(text, shell=15.0, lgvdw=(v == "lg")).single_point(s, q)
+        b = RefOracle(text, shell=15.0, lgvdw=(v == "lg")).single_point(s, q)
+        assert np.array_equal(a["census"], b["census"]), v
+        assert np.abs(a["e"] - b["e"]).max() <= 1e-9 * max(1.0, np.abs(b["e"]).max()), v
+        assert np.abs(a["grad"] - b["grad"]).max() <= 1e-9, v
+        assert np.abs(a["virial"] - b["virial"]).max() <= 1e-9 * max(1.0, np.abs(b["virial"]).max()), v
 
 
 def test_golden_fixtures_are_current():
