@@ -63,7 +63,9 @@ int rx_set_control(rx_context* ctx, double bond_cut, double hbond_cut, double th
 
 /* The systems of this context. natoms[nsys]; origin[3*nsys]; box[9*nsys] lattice vectors a, b, c as rows;
  * periodic[3*nsys] (must be 1: the engine is periodic in all directions); type[NA] force-field type index;
- * tag[NA] atom ids, unique within a system (the owner-computes tie-breaks of neighbor.cpp:295-310 use them). */
+ * tag[NA] atom ids, unique within a system (the owner-computes tie-breaks of neighbor.cpp:295-310 use them).
+ * The charge-equilibration histories (the warm start of the next solve) carry over for every atom whose system index
+ * and tag existed before the call, wherever it now sits in the arrays; new atoms start from zero. */
 int rx_set_systems(rx_context* ctx, int nsys, const int* natoms, const double* origin, const double* box, const int* periodic,
                    const int* type, const int64_t* tag);
 int rx_num_atoms(const rx_context* ctx);
@@ -74,6 +76,11 @@ int rx_num_atoms(const rx_context* ctx);
  * serving context from capacities measured earlier. Values below 1 are rejected with RX_ERR_INVALID. */
 int rx_set_capacities(rx_context* ctx, int nbr, int bonds, int near_entries);
 int rx_get_capacities(const rx_context* ctx, int* out3);
+/* Neighbor skin (the `neighbor <skin> bin` command; LAMMPS real units default 2.0, this engine 1.0 A): the rows hold
+ * every image within nonb_cut + skin and a system's rows are rebuilt only when one of its atoms has moved more than
+ * skin/2 since the last rebuild (neighbor.cpp:362-374 rebuilds every step; the cut-off decisions of every step are the
+ * same either way, taken on the current positions). 0 rebuilds every evaluation. */
+int rx_set_neighbor(rx_context* ctx, double skin);
 int rx_set_positions(rx_context* ctx, const double* x);   /* x[3*NA] */
 int rx_get_positions(rx_context* ctx, double* x);         /* positions as held (wrapped into the primary cell) */
 int rx_set_charges(rx_context* ctx, const double* q);     /* q[NA] */
@@ -86,6 +93,14 @@ int rx_set_qeq(rx_context* ctx, double swa, double swb, double tol, int imax, in
  * Jacobi-preconditioned CG from the history-extrapolated guesses (Q-23), sets q = s - (sum s / sum t) t
  * (calculate_Q) and advances the histories. iters[2*nsys] and rel[2*nsys] (s then t per system) may be NULL. */
 int rx_qeq_solve(rx_context* ctx, int* iters, double* rel);
+/* mtl::Context::qeq_solve (metal_backend.hpp:84-86) for the caller's right-hand sides and guesses, as the resident
+ * fix hands them over (fix_qeq_reaxff_metal.cpp:69-75): builds the charge matrix of the current positions, then runs
+ * the CG of both systems. b[2*NA] (the s system for every atom, then the t system), x0[2*NA] (same layout; NULL = 0),
+ * x_out[2*NA]; per system, s then t: iters[2*nsys] (iterations performed + 1, as the stock loop counts),
+ * rel[2*nsys] (final relative residual sqrt(r.M^-1 r)/|b|), status[2*nsys] (1 converged, 2 breakdown, 3 iteration
+ * limit). The preconditioner is diag(eta)^-1 (the fix's Hdia_inv). Charges and histories are not touched. Any of
+ * iters, rel, status may be NULL. */
+int rx_qeq_cg(rx_context* ctx, const double* b, const double* x0, double* x_out, int* iters, double* rel, int* status);
 /* mtl::Context::qeq_matvec (metal_backend.hpp:82): y = (diag(eta) + H) v over the owned atoms, v[NA], y[NA]. */
 int rx_qeq_matvec(rx_context* ctx, const double* v, double* y);
 /* CG iteration counts and final relative residuals (s, t per system, as rx_qeq_solve reports them) of the most recent

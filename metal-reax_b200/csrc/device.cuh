@@ -32,7 +32,10 @@ enum Status : int {
   ST_NONFINITE = 32,
   ST_NEAR_OVERFLOW = 64,
   ST_CG_NOTCONV = 128,   // a system's charge solve ended above its tolerance (iteration limit)
+  ST_VERLET_OVERFLOW = 256,
 };
+// status words: [0] bits, [1] max neighbor-row count, [2] max bond count, [3] max near-row count, [4] max Verlet-row count
+constexpr int kStatusWords = 8;
 
 struct SysInfo {
   double origin[3];
@@ -60,6 +63,7 @@ struct DevFF {
   const int* hb_on;
   const double* hb;
   const double* shld;    // nt x nt: (gamma_i gamma_j)^-1.5, the charge-matrix shielding
+  const double* rbo2;    // nt x nt: squared bond-order reach (no bond beyond it; HUGE_VAL where it cannot be bounded)
   const float* nbf;      // nt x nt x 12: single-precision pair parameters of the non-bonded kernel
   double tap[8];   // taper coefficients on [nonb_low, nonb_cut] (include/reaxmetal/terms_host.hpp:16-29)
 };
@@ -87,11 +91,21 @@ struct Dev {
   double4* xs;           // positions in cell order (w = type), so candidate loads are contiguous
   int* cell_start;       // ncell_total + 1
   int ncell_total;
-  // neighbor rows (full: both directions, every image within nonb_cut)
+  // Verlet rows: every image within nonb_cut + skin at the last rebuild of the atom's system (rebuilt when an atom of
+  // the system has moved more than skin/2 since: k_nbr_check sets the system's flag)
+  int vcap;
+  unsigned* vrow;
+  int* vcnt;
+  double4* xref;         // positions at the last rebuild
+  int* sys_flag;         // per system: rebuild in this evaluation
+  double rv2;            // (nonb_cut + skin)^2
+  double half_skin2;     // (skin / 2)^2
+  // neighbor rows (full: both directions, every image within nonb_cut), filtered from the Verlet rows every step
   int ncap;
   unsigned* nbr;
   int* nbr_cnt;
-  double* hval;          // charge-matrix entry of every neighbor entry (0 beyond swb)
+  float* hhi;            // charge-matrix entry of every neighbor entry (0 beyond swb) as hi + lo single-precision
+  float* hlo;            // parts: hi = (float)H, lo = (float)(H - hi), H = hi + lo to ~1e-15 relative
   int abits;
   unsigned amask;
   int smax, S;
@@ -114,22 +128,33 @@ struct Dev {
   double4* bC0;          // C1dbo, C2dbo, C3dbo, C1dbopi
   double4* bC1;          // C2dbopi, C3dbopi, C4dbopi, C1dbopi2
   double4* bC2;          // C2dbopi2, C3dbopi2, C4dbopi2, -
-  double4* bacc;         // Cdbo, Cdbopi, Cdbopi2, CdDelta contribution to the partner
-  double4* bfn;          // gradient contribution to the partner (xyz)
+  double4* bacc;         // Cdbo, Cdbopi, Cdbopi2, CdDelta contribution to the partner (k_bonded_atom)
+  double4* bfn;          // gradient contribution to the partner (xyz) (k_bonded_atom)
+  // the H-bond and torsion kernels run concurrently with k_bonded_atom, so each keeps its own per-slot and per-atom
+  // contributions; the gathers add them in fixed order
+  double* bcdbo_h;       // H-bond: Cdbo of the donor bond
+  double4* bfn_h;        // H-bond: gradient on the donor (xyz)
+  double4* bacc_t;       // torsion: Cdbo, Cdbopi, -, CdDelta to the partner
+  double4* bfn_t;        // torsion: gradient on the partner (xyz)
   double4* Tl;           // torsion: per (central slot, position in the far atom's slots): gradient xyz, Cdbo (w)
   // atoms
   double* Deltap;
   double* Deltap_boc;
   double4* dDp_self;
   AtomQ* aq;
-  double4* fown;         // gradient on the atom itself (xyz), own CdDelta (w)
+  double4* fown;         // gradient on the atom itself (xyz), own CdDelta (w) (k_bonded_atom)
+  double4* fown_h;       // H-bond: gradient on the hydrogen or acceptor itself
+  double4* fown_t;       // torsion: gradient on the central atom (xyz), own CdDelta (w)
   double* cdtot;
   double* W;
   double4* fdb;
   double4* fnb;          // non-bonded gradient
   double4* grad;         // result
   double* eatom;         // kTerms per atom
-  double* vir;           // kVir per atom: virial of the interactions this atom centres (LAMMPS order xx yy zz xy xz yz)
+  double* vir;           // kVir per atom: virial of the bonded interactions this atom centres (LAMMPS order xx yy zz xy xz yz)
+  double* vir_h;         // kVir per atom: H-bond triples centred on this hydrogen
+  double* vir_t;         // kVir per atom: torsions centred on this atom
+  double* vir_nb;        // kVir per atom: half the virial of the atom's non-bonded pairs
   int* census;           // kCensus per atom (atom-major: census[c*na + a])
   int* status;
   long long* counters;   // [0] neighbor entries, [1] counted pairs, [2] bonds (directed), [3] H-bond triples
@@ -170,7 +195,8 @@ __device__ inline void pair_dvec(const Dev& d, const SysInfo& s, int i, int j, i
 
 // A list of this evaluation overflowed (the host grows it and repeats the evaluation): later kernels skip their work.
 __device__ inline bool lists_failed(const Dev& d) {
-  return (*reinterpret_cast<volatile const int*>(d.status) & (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW | ST_BOND_OVERFLOW | ST_SHIFT_RANGE)) != 0;
+  return (*reinterpret_cast<volatile const int*>(d.status) &
+          (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW | ST_BOND_OVERFLOW | ST_SHIFT_RANGE | ST_VERLET_OVERFLOW)) != 0;
 }
 
 // Virial of an interaction cluster, sum over its atoms of x_a f_b = -x_a g_b, taken with positions P relative to the

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <unordered_map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -75,6 +76,18 @@ struct Context {
   int device = 0;
   int nsm = 0;
   cudaStream_t stream = nullptr;
+  // concurrent branches of an evaluation: non-bonded pairs (side), H-bonds (side_h) and torsions (side_t) next to
+  // the bonded chain on `stream`
+  cudaStream_t side = nullptr, side_h = nullptr, side_t = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join_h = nullptr, ev_join_t = nullptr;
+  // one captured MD step (replayed for every step of rx_md_run); dropped whenever a buffer or a parameter it holds
+  // changes
+  cudaGraphExec_t md_graph = nullptr;
+  bool graphs_ok = true;                // false after a capture failed: steps are then launched one by one
+  void drop_graph() {
+    if (md_graph) cudaGraphExecDestroy(md_graph);
+    md_graph = nullptr;
+  }
   std::string err;
 
   bool have_ff = false;
@@ -91,8 +104,9 @@ struct Context {
   int nsys = 0, na = 0;
   std::vector<SysInfo> hsys;
   std::vector<int> hsys_of;
+  std::vector<long long> htag;
   DBuf<SysInfo> sys;
-  DBuf<int> sys_of, type, cell_key, cell_key_sorted, cell_atoms, atom_iota, cell_start;
+  DBuf<int> sys_of, type, cell_key, cell_key_sorted, cell_atoms, atom_iota, cell_start, sys_flag;
   DBuf<double4> xs;
   DBuf<long long> tag;
   DBuf<double4> x;
@@ -103,23 +117,25 @@ struct Context {
   bool have_pos = false;
 
   // lists
-  int ncap = 0, bcap = 0, ncap_near = 0;
-  DBuf<unsigned> nbr, bcode, near;
-  DBuf<int> nbr_cnt, bsym, bcnt, near_cnt;
-  DBuf<double4> shifts;
-  DBuf<double> hval;
-  DBuf<double4> bdv, bBO, bdBOp, bdlnpi, bdlnpi2, bC0, bC1, bC2, bacc, bfn, Tl;
+  int ncap = 0, bcap = 0, ncap_near = 0, vcap = 0;
+  double skin = 1.0;   // Verlet skin [A]: rows hold every image within nonb_cut + skin, rebuilt per system on demand
+  DBuf<unsigned> nbr, bcode, near, vrow;
+  DBuf<int> nbr_cnt, bsym, bcnt, near_cnt, vcnt;
+  DBuf<double4> shifts, xref;
+  DBuf<float> hhi, hlo;
+  DBuf<double4> bdv, bBO, bdBOp, bdlnpi, bdlnpi2, bC0, bC1, bC2, bacc, bfn, Tl, bfn_h, bacc_t, bfn_t;
+  DBuf<double> bcdbo_h;
   // atoms
   DBuf<double> Deltap, Deltap_boc, cdtot, W, eatom;
-  DBuf<double4> dDp_self, fown, fdb, fnb, grad;
+  DBuf<double4> dDp_self, fown, fdb, fnb, grad, fown_h, fown_t;
   DBuf<AtomQ> aq;
   DBuf<int> census, status;
   DBuf<long long> counters;
-  DBuf<double> energies, virial, vir;
+  DBuf<double> energies, virial, vir, vir_nb, vir_h, vir_t;
   // QEq
   DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
   DBuf<double> cg_eta, cg_part, s_hist, t_hist, cg_rel;
-  DBuf<int> cg_iters, cg_nlive;
+  DBuf<int> cg_iters, cg_nlive, cg_nref, cg_brk;
   DBuf<SysCg> cg_sys;
   DBuf<double2> cg_rb0, cg_rb1;
   std::vector<int> last_iters;
@@ -127,7 +143,7 @@ struct Context {
   // MD
   bool md_ready = false;
   DBuf<double4> v;
-  DBuf<double> mass, ke, temp, scale, xi, vxi, kpart;
+  DBuf<double> mass, ke, temp, scale, xi, vxi, kpart, ramp;
   DBuf<int> kfirst, ksys;
   MdDev md{};
   long long md_step = 0;
@@ -165,14 +181,21 @@ struct Context {
     RXCU(cudaSetDevice(dev));
     RXCU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     RXCU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    status.ensure(4);
+    for (cudaStream_t* st : {&side, &side_h, &side_t}) RXCU(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
+    for (cudaEvent_t* ev : {&ev_fork, &ev_join, &ev_fork2, &ev_join_h, &ev_join_t}) RXCU(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    status.ensure(kStatusWords);
     counters.ensure(8);
     set_qeq(0.0, 10.0, 1e-6, 200, 0);
   }
   ~Context() {
     if (host_only) return;
     if (pinned) cudaFreeHost(pinned);
+    drop_graph();
     for (auto& p : phases) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    for (cudaEvent_t ev : {ev_fork, ev_join, ev_fork2, ev_join_h, ev_join_t})
+      if (ev) cudaEventDestroy(ev);
+    for (cudaStream_t st : {side, side_h, side_t})
+      if (st) cudaStreamDestroy(st);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -208,7 +231,32 @@ struct Context {
         o[9] = static_cast<float>(std::pow(ff.p(a, b, TB_LGRE), 6.0));
       }
     const size_t nbf_d = nbf.size() / 2;
-    const size_t total = 64 + nsb + ntb + nthb + nfb + nhb + nthn + nfo + nho + shld.size() + nbf_d;
+    // Bond-order reach per type pair: beyond r_bo every uncorrected component BO'_s, BO'_pi, BO'_pipi is below bo_cut/3
+    // (each decreases with r when its exponent pair is p_bo(odd) < 0 < p_bo(even)), so BO' < bo_cut there and the pair
+    // is no bond (the gate of src/cpu/bonded.cpp:130). k_bonds skips their exponentials; the bond list is unchanged.
+    // Pairs whose parameters do not decrease keep the whole bond_cut (r_bo = infinity).
+    std::vector<double> rbo2(static_cast<size_t>(ff.nt) * ff.nt, HUGE_VAL);
+    for (int a = 0; a < ff.nt; ++a)
+      for (int b = 0; b < ff.nt; ++b) {
+        const double c = ff.bo_cut / 3.0;
+        double reach = 0.0;
+        bool ok = c > 0.0;
+        auto comp = [&](bool present, double r0, double p_odd, double p_even, double scale) {
+          if (!present || !ok) return;
+          if (!(r0 > 0.0) || !(p_odd < 0.0) || !(p_even > 0.0)) { ok = false; return; }
+          const double arg = std::log(c / scale) / p_odd;   // (r / r0)^p_even at the crossing
+          if (!(arg > 0.0)) { ok = false; return; }
+          reach = std::max(reach, r0 * std::pow(arg, 1.0 / p_even));
+        };
+        comp(ff.s(a, SB_R_S) > 0.0 && ff.s(b, SB_R_S) > 0.0, ff.p(a, b, TB_R_S), ff.p(a, b, TB_P_BO1), ff.p(a, b, TB_P_BO2), 1.0 + ff.bo_cut);
+        comp(ff.s(a, SB_R_PI) > 0.0 && ff.s(b, SB_R_PI) > 0.0, ff.p(a, b, TB_R_P), ff.p(a, b, TB_P_BO3), ff.p(a, b, TB_P_BO4), 1.0);
+        comp(ff.s(a, SB_R_PI_PI) > 0.0 && ff.s(b, SB_R_PI_PI) > 0.0, ff.p(a, b, TB_R_PP), ff.p(a, b, TB_P_BO5), ff.p(a, b, TB_P_BO6), 1.0);
+        if (ok && std::isfinite(reach)) {
+          const double r = reach * (1.0 + 1e-6) + 1e-6;
+          rbo2[static_cast<size_t>(a) * ff.nt + b] = r * r;
+        }
+      }
+    const size_t total = 64 + nsb + ntb + nthb + nfb + nhb + nthn + nfo + nho + shld.size() + rbo2.size() + nbf_d;
     std::vector<double> h(total, 0.0);
     size_t off = 0;
     auto put = [&](const double* src, size_t n) { std::memcpy(h.data() + off, src, n * sizeof(double)); size_t o = off; off += n; return o; };
@@ -216,6 +264,7 @@ struct Context {
     std::copy(ff.gp.begin(), ff.gp.begin() + std::min<size_t>(ff.gp.size(), 64), gp.begin());
     const size_t o_gp = put(gp.data(), 64), o_sb = put(ff.sb.data(), nsb), o_tb = put(ff.tb.data(), ntb), o_thb = put(ff.thb.data(), nthb);
     const size_t o_fb = put(ff.fb.data(), nfb), o_hb = put(ff.hb.data(), nhb), o_shld = put(shld.data(), shld.size());
+    const size_t o_rbo2 = put(rbo2.data(), rbo2.size());
     const size_t o_nbf = off;
     std::memcpy(h.data() + off, nbf.data(), nbf.size() * sizeof(float));
     off += nbf_d;
@@ -245,6 +294,7 @@ struct Context {
     dff.fb = ff_buf.p + o_fb;
     dff.hb = ff_buf.p + o_hb;
     dff.shld = ff_buf.p + o_shld;
+    dff.rbo2 = ff_buf.p + o_rbo2;
     dff.nbf = reinterpret_cast<const float*>(ff_buf.p + o_nbf);
     dff.thb_n = reinterpret_cast<const int*>(ff_buf.p + o_thn);
     dff.fb_on = reinterpret_cast<const int*>(ff_buf.p + o_fo);
@@ -258,6 +308,14 @@ struct Context {
     if (!(bond_cut > 0) || !(hbond_cut >= 0) || !std::isfinite(bond_cut) || !std::isfinite(hbond_cut))
       throw Error(RX_ERR_INVALID, "cut-offs must be finite, bond_cut > 0, hbond_cut >= 0");
     ctl = DevCtl{bond_cut, hbond_cut, thb_cut, thb_cutsq, enobonds};
+    drop_graph();
+  }
+
+  void set_neighbor(double sk) {
+    if (!(sk >= 0.0) || !std::isfinite(sk) || sk > 10.0) throw Error(RX_ERR_INVALID, "neighbor skin must be in [0, 10] A");
+    skin = sk;
+    vcap = 0;
+    if (have_ff && nsys > 0) layout_systems();
   }
 
   void set_qeq(double swa, double swb, double tol, int imax, int strict) {
@@ -268,6 +326,7 @@ struct Context {
     qeq_tol = tol;
     qeq_imax = imax;
     qeq_strict = strict;
+    drop_graph();
   }
 
   void require_ff() const { if (!have_ff) throw Error(RX_ERR_STATE, "no force field set"); }
@@ -292,6 +351,18 @@ struct Context {
     if (total > (1LL << 30)) throw Error(RX_ERR_INVALID, "too many atoms");
     for (long long a = 0; a < total; ++a)
       if (types[a] < 0 || types[a] >= ff.nt) throw Error(RX_ERR_INVALID, "atom " + std::to_string(a) + " has a type outside the force field");
+    // the charge-equilibration histories of the previous systems, to carry over by (system index, tag): a caller that
+    // re-neighbours or reorders its atoms (fix qeq/reaxff's s_hist/t_hist travel with the atoms) keeps its warm start
+    std::vector<double> old_sh, old_th;
+    std::vector<long long> old_tag = htag;
+    std::vector<int> old_sys = hsys_of;
+    const int old_nsys = nsys;
+    if (na > 0 && s_hist.p && static_cast<size_t>(na) == old_tag.size()) {
+      old_sh.resize(4 * static_cast<size_t>(na));
+      old_th.resize(4 * static_cast<size_t>(na));
+      RXCU(cudaMemcpy(old_sh.data(), s_hist.p, sizeof(double) * old_sh.size(), cudaMemcpyDeviceToHost));
+      RXCU(cudaMemcpy(old_th.data(), t_hist.p, sizeof(double) * old_th.size(), cudaMemcpyDeviceToHost));
+    }
     nsys = n_sys;
     na = static_cast<int>(total);
     hsys.assign(static_cast<size_t>(nsys), SysInfo{});
@@ -318,22 +389,43 @@ struct Context {
     RXCU(cudaMemset(q.p, 0, sizeof(double) * na));
     s_hist.ensure(4 * static_cast<size_t>(na));
     t_hist.ensure(4 * static_cast<size_t>(na));
-    RXCU(cudaMemset(s_hist.p, 0, sizeof(double) * 4 * na));
-    RXCU(cudaMemset(t_hist.p, 0, sizeof(double) * 4 * na));
+    htag.assign(tags, tags + na);
+    {
+      std::vector<double> sh(4 * static_cast<size_t>(na), 0.0), th(4 * static_cast<size_t>(na), 0.0);
+      if (!old_sh.empty()) {
+        std::vector<std::unordered_map<long long, int>> by_sys(static_cast<size_t>(old_nsys));
+        for (size_t k = 0; k < old_tag.size(); ++k) by_sys[static_cast<size_t>(old_sys[k])].emplace(old_tag[k], static_cast<int>(k));
+        for (int a = 0; a < na; ++a) {
+          const int sy = hsys_of[static_cast<size_t>(a)];
+          if (sy >= old_nsys) continue;
+          const auto it = by_sys[static_cast<size_t>(sy)].find(htag[static_cast<size_t>(a)]);
+          if (it == by_sys[static_cast<size_t>(sy)].end()) continue;
+          for (int c = 0; c < 4; ++c) {
+            sh[4 * static_cast<size_t>(a) + c] = old_sh[4 * static_cast<size_t>(it->second) + c];
+            th[4 * static_cast<size_t>(a) + c] = old_th[4 * static_cast<size_t>(it->second) + c];
+          }
+        }
+      }
+      RXCU(cudaMemcpy(s_hist.p, sh.data(), sizeof(double) * sh.size(), cudaMemcpyHostToDevice));
+      RXCU(cudaMemcpy(t_hist.p, th.data(), sizeof(double) * th.size(), cudaMemcpyHostToDevice));
+    }
     have_pos = false;
     have_virial = false;
     md_ready = false;
     ncap = 0;
     bcap = 0;
+    vcap = 0;
     layout_systems();
   }
 
   // cell grids, search ranges, shift encoding, neighbor capacity estimate
   void layout_systems() {
-    const double rc = ff.nonb_cut;
-    if (!(rc > 0)) throw Error(RX_ERR_INVALID, "force field has no positive non-bonded cut-off");
-    if (ctl.bond_cut > rc || ctl.hbond_cut > rc) throw Error(RX_ERR_INVALID, "bond_cut and hbond_cut must not exceed the non-bonded cut-off");
-    if (qp.swb > rc) throw Error(RX_ERR_INVALID, "fix qeq: the taper radius exceeds the force field's nonb_cut (qeq_device.cpp:14)");
+    drop_graph();
+    const double rc0 = ff.nonb_cut;
+    if (!(rc0 > 0)) throw Error(RX_ERR_INVALID, "force field has no positive non-bonded cut-off");
+    const double rc = rc0 + skin;   // the Verlet radius sets the cell search range and the shift encoding
+    if (ctl.bond_cut > rc0 || ctl.hbond_cut > rc0) throw Error(RX_ERR_INVALID, "bond_cut and hbond_cut must not exceed the non-bonded cut-off");
+    if (qp.swb > rc0) throw Error(RX_ERR_INVALID, "fix qeq: the taper radius exceeds the force field's nonb_cut (qeq_device.cpp:14)");
     int cell_begin = 0, sm = 1;
     double max_density = 0;
     for (auto& si : hsys) {
@@ -413,15 +505,19 @@ struct Context {
     size_t tmp = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, key_bits, stream);
     cub_tmp.ensure(tmp);
-    const double expect = 4.0 / 3.0 * M_PI * rc * rc * rc * max_density;
+    const double expect = 4.0 / 3.0 * M_PI * rc0 * rc0 * rc0 * max_density;
     const int want_ncap = static_cast<int>(std::ceil((expect * 1.3 + 32) / 32.0)) * 32;
     if (ncap < want_ncap) ncap = want_ncap;
+    const double expect_v = 4.0 / 3.0 * M_PI * rc * rc * rc * max_density;
+    const int want_vcap = static_cast<int>(std::ceil((expect_v * 1.3 + 32) / 32.0)) * 32;
+    if (vcap < want_vcap) vcap = want_vcap;
     const double rn = std::max(ctl.bond_cut, ctl.hbond_cut);
     const int want_near = static_cast<int>(std::ceil((4.0 / 3.0 * M_PI * rn * rn * rn * max_density * 1.3 + 32) / 32.0)) * 32;
     if (ncap_near < want_near) ncap_near = want_near;
     if (bcap < 16) bcap = 16;
     alloc_atoms();
     alloc_lists();
+    force_rebuild();
   }
 
   void alloc_atoms() {
@@ -429,10 +525,13 @@ struct Context {
     Deltap.ensure(n); Deltap_boc.ensure(n); cdtot.ensure(n); W.ensure(n); eatom.ensure(n * kTerms);
     dDp_self.ensure(n); fown.ensure(n); fdb.ensure(n); fnb.ensure(n); grad.ensure(n);
     aq.ensure(n); census.ensure(n * kCensus);
-    nbr_cnt.ensure(n); bcnt.ensure(n); near_cnt.ensure(n);
+    nbr_cnt.ensure(n); bcnt.ensure(n); near_cnt.ensure(n); vcnt.ensure(n); xref.ensure(n);
+    sys_flag.ensure(static_cast<size_t>(nsys)); cg_nref.ensure(1); cg_brk.ensure(static_cast<size_t>(nsys));
     energies.ensure(static_cast<size_t>(nsys) * kTerms);
     virial.ensure(static_cast<size_t>(nsys) * kVir);
     vir.ensure(n * kVir);
+    vir_nb.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
+    fown_h.ensure(n); fown_t.ensure(n);
     cg_x.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
     cg_sys.ensure(nsys); cg_rb0.ensure(n); cg_rb1.ensure(n); cg_nlive.ensure(2);
@@ -440,14 +539,18 @@ struct Context {
   }
 
   void alloc_lists() {
+    drop_graph();
     const size_t n = static_cast<size_t>(na);
+    vrow.ensure(n * vcap);
     nbr.ensure(n * ncap);
-    hval.ensure(n * ncap);
+    hhi.ensure(n * ncap);
+    hlo.ensure(n * ncap);
     near.ensure(n * ncap_near);
     const size_t nb = n * bcap;
     bcode.ensure(nb); bsym.ensure(nb);
     bdv.ensure(nb); bBO.ensure(nb); bdBOp.ensure(nb); bdlnpi.ensure(nb); bdlnpi2.ensure(nb);
     bC0.ensure(nb); bC1.ensure(nb); bC2.ensure(nb); bacc.ensure(nb); bfn.ensure(nb);
+    bcdbo_h.ensure(nb); bfn_h.ensure(nb); bacc_t.ensure(nb); bfn_t.ensure(nb);
     Tl.ensure(nb * bcap);
   }
 
@@ -455,7 +558,10 @@ struct Context {
     Dev d{};
     d.na = na; d.nsys = nsys; d.sys = sys.p; d.sys_of = sys_of.p; d.x = x.p; d.type = type.p; d.tag = tag.p; d.q = q.p;
     d.cell_key = cell_key.p; d.cell_atoms = cell_atoms.p; d.xs = xs.p; d.cell_start = cell_start.p; d.ncell_total = ncell_total;
-    d.ncap = ncap; d.nbr = nbr.p; d.nbr_cnt = nbr_cnt.p; d.hval = hval.p;
+    d.ncap = ncap; d.nbr = nbr.p; d.nbr_cnt = nbr_cnt.p; d.hhi = hhi.p; d.hlo = hlo.p;
+    d.vcap = vcap; d.vrow = vrow.p; d.vcnt = vcnt.p; d.xref = xref.p; d.sys_flag = sys_flag.p;
+    d.rv2 = (ff.nonb_cut + skin) * (ff.nonb_cut + skin);
+    d.half_skin2 = 0.25 * skin * skin;
     d.abits = abits; d.amask = (abits >= 32) ? 0xffffffffu : ((1u << abits) - 1u); d.smax = smax; d.S = S;
     d.shifts = shifts.p; d.ncap_near = ncap_near; d.near = near.p; d.near_cnt = near_cnt.p;
     {  // a superset of every consumer's sqrt(r2) <= cut test
@@ -465,7 +571,8 @@ struct Context {
     d.bcap = bcap; d.bcode = bcode.p; d.bsym = bsym.p; d.bcnt = bcnt.p; d.bdv = bdv.p; d.bBO = bBO.p; d.bdBOp = bdBOp.p;
     d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p;
     d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
-    d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.census = census.p; d.status = status.p;
+    d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.vir_nb = vir_nb.p; d.vir_h = vir_h.p; d.vir_t = vir_t.p;
+    d.fown_h = fown_h.p; d.fown_t = fown_t.p; d.bcdbo_h = bcdbo_h.p; d.bfn_h = bfn_h.p; d.bacc_t = bacc_t.p; d.bfn_t = bfn_t.p; d.census = census.p; d.status = status.p;
     d.counters = counters.p;
     return d;
   }
@@ -497,16 +604,23 @@ struct Context {
   // ------------------------------------------------------------------ the force evaluation
   static unsigned blocks(long long n, int per) { return static_cast<unsigned>((n + per - 1) / per); }
 
+  // every system's Verlet rows are rebuilt at the next evaluation (new positions, capacities or cut-offs)
+  void force_rebuild() {
+    if (nsys > 0) RXCU(cudaMemsetAsync(sys_flag.p, 1, sizeof(int) * nsys, stream));
+  }
+
+  // Verlet maintenance + this evaluation's rows (neighbor rows, charge matrix, near rows). The wrap/bin, sort and
+  // cell-start kernels run every evaluation but do work only for systems whose flag is set; k_neighbors likewise.
   void build_lists(const Dev& d) {
     tic(0, "neighbors");
-    ++launches;
+    launches += 5;
+    k_nbr_check<<<blocks(na, 256), 256, 0, stream>>>(d);
     k_wrap_bin<<<blocks(na, 256), 256, 0, stream>>>(d);
     size_t tmp = cub_tmp.n;
     RXCU(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, key_bits, stream));
-    ++launches;
     k_cell_start<<<blocks(na + 1, 256), 256, 0, stream>>>(d, cell_key_sorted.p);
-    ++launches;
-    k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, qp);
+    k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d);
+    k_pairs<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, qp);
     toc(0);
   }
 
@@ -514,31 +628,26 @@ struct Context {
     CgArgs a{};
     a.imax = qeq_imax; a.tol = qeq_tol;
     a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.eta = cg_eta.p; a.part = cg_part.p;
-    a.out_iters = cg_iters.p; a.out_rel = cg_rel.p;
+    a.out_iters = cg_iters.p; a.out_rel = cg_rel.p; a.out_nref = cg_nref.p; a.out_brk = cg_brk.p; a.write_q = 1;
     return a;
   }
 
-  void launch_qeq(const Dev& d) {
-    tic(1, "qeq");
-    CgArgs a = cg_args();
-    ++launches;
-    k_qeq_prepare<<<blocks(na, 256), 256, 0, stream>>>(d, dff, a, s_hist.p, t_hist.p);
+  int grid_per_sm = 0, seg_per_sm = 0;
+  void launch_cg(const Dev& d, CgArgs a) {
     if (nsys == 1 && na > 4096) {   // one large system: all SMs on its rows, block partials summed in block order
       const int threads = 256;
-      int per_sm = 0;
-      RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_grid, threads, 0));
-      int grid = std::max(1, std::min(per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
+      if (!grid_per_sm) RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k_cg_grid, threads, 0));
+      int grid = std::max(1, std::min(grid_per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
       grid = std::min(grid, nsm * 32);
       a.begin = 0;
       a.n = na;
       void* args[] = {const_cast<Dev*>(&d), &a};
       ++launches;
-    RXCU(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_grid), dim3(grid), dim3(threads), args, 0, stream));
+      RXCU(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_grid), dim3(grid), dim3(threads), args, 0, stream));
     } else {   // a batch (or one small system): every row of every system on all SMs, per-system fixed-order sums
       const int threads = 256;
-      int per_sm = 0;
-      RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_seg, threads, 0));
-      int grid = std::max(1, std::min(per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
+      if (!seg_per_sm) RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&seg_per_sm, k_cg_seg, threads, 0));
+      int grid = std::max(1, std::min(seg_per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
       grid = std::min(grid, nsm * 32);
       a.sc = cg_sys.p; a.rb0 = cg_rb0.p; a.rb1 = cg_rb1.p; a.nlive = cg_nlive.p;
       RXCU(cudaMemsetAsync(cg_sys.p, 0, sizeof(SysCg) * nsys, stream));
@@ -547,50 +656,111 @@ struct Context {
       ++launches;
       RXCU(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_seg), dim3(grid), dim3(threads), args, 0, stream));
     }
+  }
+
+  // charges: guesses from the histories, the CG, q, and the history shift (skipped by the kernel after a failure)
+  void launch_qeq(const Dev& d) {
+    tic(1, "qeq");
+    CgArgs a = cg_args();
+    ++launches;
+    k_qeq_prepare<<<blocks(na, 256), 256, 0, stream>>>(d, dff, a, s_hist.p, t_hist.p);
+    launch_cg(d, a);
+    ++launches;
+    k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p, qeq_strict);
     toc(1);
   }
 
-  void launch_bonded(const Dev& d) {
+  // After the rows (and the charges): the non-bonded pairs on `side` run next to the bonded chain; after the bond
+  // orders, the H-bonds (`side_h`) and the torsions (`side_t`) run next to k_bonded_atom. Each branch writes its own
+  // arrays (fnb, vir_nb; *_h; *_t, Tl), and all join before the gathers, which add them in fixed order. With timing on,
+  // every branch runs on `stream`, one after the other, so each phase is timed alone.
+  void launch_forces(const Dev& d) {
+    const bool conc = !timing;
+    cudaStream_t nbs = conc ? side : stream, hs = conc ? side_h : stream, ts = conc ? side_t : stream;
+    if (conc) {
+      RXCU(cudaEventRecord(ev_fork, stream));
+      RXCU(cudaStreamWaitEvent(side, ev_fork, 0));
+    }
+    tic(5, "nonbonded");
+    ++launches;
+    k_nonbonded<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, nbs>>>(d, dff);
+    toc(5);
+    if (conc) RXCU(cudaEventRecord(ev_join, side));
     tic(2, "bond_orders");
-    ++launches;
+    launches += 4;
     k_bonds<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, ctl);
-    ++launches;
     k_bond_sym<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d);
-    ++launches;
     k_bo_correct<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d, dff);
-    ++launches;
     k_atom_quantities<<<blocks(na, 128), 128, 0, stream>>>(d, dff);
     toc(2);
+    if (conc) {
+      RXCU(cudaEventRecord(ev_fork2, stream));
+      RXCU(cudaStreamWaitEvent(side_h, ev_fork2, 0));
+      RXCU(cudaStreamWaitEvent(side_t, ev_fork2, 0));
+    }
     tic(3, "bonded_terms");
-    ++launches;
+    launches += 3;
     k_bonded_atom<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
-    ++launches;
-    k_hbond<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, ctl);
-    ++launches;
-    k_hbond_acceptor<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, ctl);
+    k_hbond<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, hs>>>(d, dff, ctl);
+    k_hbond_acceptor<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, hs>>>(d, dff, ctl);
     toc(3);
     tic(4, "torsion");
     ++launches;
-    k_torsion<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
+    k_torsion<<<blocks(na, 64), 64, 0, ts>>>(d, dff, ctl);
     toc(4);
-  }
-
-  void launch_nonbonded(const Dev& d) {
-    tic(5, "nonbonded");
-    ++launches;
-    k_nonbonded<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff);
-    toc(5);
-  }
-
-  void launch_gather(const Dev& d) {
+    if (conc) {
+      RXCU(cudaEventRecord(ev_join_h, side_h));
+      RXCU(cudaEventRecord(ev_join_t, side_t));
+      RXCU(cudaStreamWaitEvent(stream, ev_join_h, 0));
+      RXCU(cudaStreamWaitEvent(stream, ev_join_t, 0));
+    }
     tic(6, "gather");
-    ++launches;
+    launches += 3;
     k_fold<<<blocks(na, 128), 128, 0, stream>>>(d);
-    ++launches;
     k_dbond<<<blocks(na, 128), 128, 0, stream>>>(d);
-    ++launches;
+    if (conc) RXCU(cudaStreamWaitEvent(stream, ev_join, 0));
     k_force_final<<<blocks(na, 128), 128, 0, stream>>>(d);
     toc(6);
+  }
+
+  // One evaluation of every system, enqueued without any host synchronisation: kernels after a failure (a list
+  // overflow) return at once; the host reads the status word when it next synchronises.
+  void enqueue_eval(bool do_qeq) {
+    const Dev d = dev();
+    build_lists(d);
+    if (do_qeq) launch_qeq(d);
+    launch_forces(d);
+  }
+
+  // grow the capacities from a status word with overflow bits; false if nothing overflowed
+  bool grow_from_status(const int* st, int attempt) {
+    if (!(st[0] & (ST_NBR_OVERFLOW | ST_BOND_OVERFLOW | ST_NEAR_OVERFLOW | ST_VERLET_OVERFLOW))) return false;
+    if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "list capacity still exceeded after 4 grow attempts");
+    if (st[0] & ST_NBR_OVERFLOW) ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
+    if (st[0] & ST_NEAR_OVERFLOW) ncap_near = ((st[3] * 5 / 4) + 31) / 32 * 32;
+    if (st[0] & ST_VERLET_OVERFLOW) vcap = ((st[4] * 5 / 4) + 31) / 32 * 32;
+    if (st[0] & ST_BOND_OVERFLOW) bcap = std::max(bcap, ((st[2] * 5 / 4) + 3) / 4 * 4);
+    alloc_lists();
+    return true;
+  }
+
+  void check_status(const int* st, bool do_qeq) {
+    if (st[0] & ST_SHIFT_RANGE) throw Error(RX_ERR_INVALID, "a periodic image outside the shift encoding was requested");
+    if (st[0] & ST_NONFINITE) throw Error(RX_ERR_INVALID, "non-finite coordinate");
+    if (st[0] & ST_SYM_MISSING) throw Error(RX_ERR_INVALID, "inconsistent bond list (a bond without its reverse)");
+    if (do_qeq) {
+      if (st[0] & ST_CG_BREAKDOWN) throw Error(RX_ERR_NOT_CONVERGED, "charge equilibration: CG breakdown");
+      if (qeq_strict && (st[0] & ST_CG_NOTCONV))
+        throw Error(RX_ERR_NOT_CONVERGED, "charge equilibration did not converge within " + std::to_string(qeq_imax) + " iterations");
+      finish_qeq();
+    }
+  }
+
+  void fetch_qeq_counts() {
+    last_iters.resize(2 * static_cast<size_t>(nsys));
+    last_rel.resize(2 * static_cast<size_t>(nsys));
+    RXCU(cudaMemcpyAsync(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
+    RXCU(cudaMemcpyAsync(last_rel.data(), cg_rel.p, sizeof(double) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
   }
 
   // One force evaluation of every system, with grow-and-retry of the list capacities (neighbor.cpp:362-374,
@@ -600,40 +770,18 @@ struct Context {
     require_sys();
     if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
     for (int attempt = 0;; ++attempt) {
-      RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * 4, stream));
-      const Dev d = dev();
-      build_lists(d);
-      if (do_qeq) launch_qeq(d);
-      launch_bonded(d);
-      launch_nonbonded(d);
-      launch_gather(d);
-      if (do_qeq) {   // history shift and the solve's counts, in the same round trip as the status word
-        ++launches;
-        k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p, qeq_strict);
-        last_iters.resize(2 * static_cast<size_t>(nsys));
-        last_rel.resize(2 * static_cast<size_t>(nsys));
-        RXCU(cudaMemcpyAsync(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
-        RXCU(cudaMemcpyAsync(last_rel.data(), cg_rel.p, sizeof(double) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
-      }
-      int st[4];
+      RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * kStatusWords, stream));
+      enqueue_eval(do_qeq);
+      if (do_qeq) fetch_qeq_counts();
+      int st[kStatusWords];
       RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaStreamSynchronize(stream));
       RXCU(cudaGetLastError());
-      if (st[0] & (ST_NBR_OVERFLOW | ST_BOND_OVERFLOW | ST_NEAR_OVERFLOW)) {
-        if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "list capacity still exceeded after 4 grow attempts");
-        if (st[0] & ST_NBR_OVERFLOW) ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
-        if (st[0] & ST_NEAR_OVERFLOW) ncap_near = ((st[3] * 5 / 4) + 31) / 32 * 32;
-        if (st[0] & ST_BOND_OVERFLOW) bcap = std::max(bcap, ((st[2] * 5 / 4) + 3) / 4 * 4);
-        alloc_lists();
+      if (grow_from_status(st, attempt)) {
+        force_rebuild();
         continue;
       }
-      if (st[0] & ST_SHIFT_RANGE) throw Error(RX_ERR_INVALID, "a periodic image outside the shift encoding was requested");
-      if (st[0] & ST_NONFINITE) throw Error(RX_ERR_INVALID, "non-finite coordinate");
-      if (st[0] & ST_SYM_MISSING) throw Error(RX_ERR_INVALID, "inconsistent bond list (a bond without its reverse)");
-      if (do_qeq) {
-        if (st[0] & ST_CG_BREAKDOWN) throw Error(RX_ERR_NOT_CONVERGED, "charge equilibration: CG breakdown");
-        finish_qeq();
-      }
+      check_status(st, do_qeq);
       break;
     }
     collect_times();
@@ -660,6 +808,7 @@ struct Context {
     double4* h = stage(static_cast<size_t>(na));
     for (int a = 0; a < na; ++a) h[a] = make_double4(xin[3 * a], xin[3 * a + 1], xin[3 * a + 2], 0.0);
     RXCU(cudaMemcpyAsync(x.p, h, sizeof(double4) * na, cudaMemcpyHostToDevice, stream));
+    force_rebuild();
     RXCU(cudaStreamSynchronize(stream));
     have_pos = true;
   }
@@ -720,59 +869,92 @@ struct Context {
     require_sys();
     if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
     for (int attempt = 0;; ++attempt) {
-      RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * 4, stream));
+      RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * kStatusWords, stream));
       const Dev d = dev();
       build_lists(d);
       launch_qeq(d);
-      ++launches;
-      k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p, qeq_strict);
-      last_iters.resize(2 * static_cast<size_t>(nsys));
-      last_rel.resize(2 * static_cast<size_t>(nsys));
-      RXCU(cudaMemcpyAsync(last_iters.data(), cg_iters.p, sizeof(int) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
-      RXCU(cudaMemcpyAsync(last_rel.data(), cg_rel.p, sizeof(double) * 2 * nsys, cudaMemcpyDeviceToHost, stream));
-      int st[4];
+      fetch_qeq_counts();
+      int st[kStatusWords];
       RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaStreamSynchronize(stream));
       RXCU(cudaGetLastError());
-      if (st[0] & (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW)) {
-        if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "neighbor capacity still exceeded after 4 grow attempts");
-        if (st[0] & ST_NBR_OVERFLOW) ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
-        if (st[0] & ST_NEAR_OVERFLOW) ncap_near = ((st[3] * 5 / 4) + 31) / 32 * 32;
-        alloc_lists();
+      if (grow_from_status(st, attempt)) {
+        force_rebuild();
         continue;
       }
-      if (st[0] & ST_SHIFT_RANGE) throw Error(RX_ERR_INVALID, "a periodic image outside the shift encoding was requested");
-      if (st[0] & ST_NONFINITE) throw Error(RX_ERR_INVALID, "non-finite coordinate");
-      if (st[0] & ST_CG_BREAKDOWN) throw Error(RX_ERR_NOT_CONVERGED, "charge equilibration: CG breakdown");
-      finish_qeq();
+      check_status(st, true);
       break;
     }
     if (iters) std::copy(last_iters.begin(), last_iters.end(), iters);
     if (rel) std::copy(last_rel.begin(), last_rel.end(), rel);
   }
 
+  // mtl::Context::qeq_solve: the charge matrix of the current positions (compute_H), then the CG of both systems for
+  // the caller's right-hand sides from the caller's guesses; charges and histories are left alone.
+  void qeq_cg(const double* b, const double* x0, double* x_out, int* iters, double* rel, int* stat) {
+    require_ff();
+    require_sys();
+    if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
+    if (!b || !x_out) throw Error(RX_ERR_INVALID, "rx_qeq_cg: null b or x_out");
+    rows_only();
+    const size_t n2 = 2 * static_cast<size_t>(na);
+    DBuf<double> bd, xd;
+    bd.ensure(n2);
+    RXCU(cudaMemcpyAsync(bd.p, b, sizeof(double) * n2, cudaMemcpyHostToDevice, stream));
+    if (x0) {
+      xd.ensure(n2);
+      RXCU(cudaMemcpyAsync(xd.p, x0, sizeof(double) * n2, cudaMemcpyHostToDevice, stream));
+    }
+    RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * kStatusWords, stream));
+    const Dev d = dev();
+    CgArgs a = cg_args();
+    a.write_q = 0;
+    ++launches;
+    k_qeq_prepare_given<<<blocks(na, 256), 256, 0, stream>>>(d, dff, a, bd.p, x0 ? xd.p : nullptr);
+    launch_cg(d, a);
+    fetch_qeq_counts();
+    std::vector<double2> xh(static_cast<size_t>(na));
+    std::vector<int> brk(static_cast<size_t>(nsys));
+    RXCU(cudaMemcpyAsync(xh.data(), cg_x.p, sizeof(double2) * na, cudaMemcpyDeviceToHost, stream));
+    RXCU(cudaMemcpyAsync(brk.data(), cg_brk.p, sizeof(int) * nsys, cudaMemcpyDeviceToHost, stream));
+    RXCU(cudaStreamSynchronize(stream));
+    RXCU(cudaGetLastError());
+    for (int i = 0; i < na; ++i) { x_out[i] = xh[static_cast<size_t>(i)].x; x_out[na + i] = xh[static_cast<size_t>(i)].y; }
+    for (int sy = 0; sy < nsys; ++sy)
+      for (int k = 0; k < 2; ++k) {
+        const size_t j = 2 * static_cast<size_t>(sy) + k;
+        if (iters) iters[j] = last_iters[j];
+        if (rel) rel[j] = last_rel[j];
+        if (stat) stat[j] = brk[static_cast<size_t>(sy)] ? 2 : (last_rel[j] <= qeq_tol ? 1 : 3);
+      }
+  }
+
+  // rows and charge matrix of the current positions, with grow-and-retry (no charge solve, no forces)
+  void rows_only() {
+    for (int attempt = 0;; ++attempt) {
+      RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * kStatusWords, stream));
+      build_lists(dev());
+      int st[kStatusWords];
+      RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
+      RXCU(cudaStreamSynchronize(stream));
+      RXCU(cudaGetLastError());
+      if (grow_from_status(st, attempt)) {
+        force_rebuild();
+        continue;
+      }
+      check_status(st, false);
+      break;
+    }
+  }
+
   void qeq_matvec(const double* vin, double* yout) {
     require_ff();
     require_sys();
     if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
-    for (int attempt = 0;; ++attempt) {
-      RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * 4, stream));
-      build_lists(dev());
-      int st[4];
-      RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
-      RXCU(cudaStreamSynchronize(stream));
-      if (st[0] & (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW)) {
-        if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "neighbor capacity still exceeded after 4 grow attempts");
-        if (st[0] & ST_NBR_OVERFLOW) ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
-        if (st[0] & ST_NEAR_OVERFLOW) ncap_near = ((st[3] * 5 / 4) + 31) / 32 * 32;
-        alloc_lists();
-        continue;
-      }
-      break;
-    }
+    rows_only();
     std::vector<double2> h(static_cast<size_t>(na));
     for (int a = 0; a < na; ++a) h[static_cast<size_t>(a)] = make_double2(vin[a], 0.0);
-    RXCU(cudaMemcpy(cg_d.p, h.data(), sizeof(double2) * na, cudaMemcpyHostToDevice));
+    RXCU(cudaMemcpyAsync(cg_d.p, h.data(), sizeof(double2) * na, cudaMemcpyHostToDevice, stream));
     ++launches;
     k_qeq_matvec<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(dev(), dff, cg_d.p, cg_q.p);
     RXCU(cudaMemcpyAsync(h.data(), cg_q.p, sizeof(double2) * na, cudaMemcpyDeviceToHost, stream));
@@ -804,9 +986,12 @@ struct Context {
     kpart.ensure(std::max(nchunks, 1)); kfirst.ensure(first.size()); ksys.ensure(std::max(nchunks, 1));
     RXCU(cudaMemcpy(kfirst.p, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
     if (nchunks > 0) RXCU(cudaMemcpy(ksys.p, csys.data(), sizeof(int) * csys.size(), cudaMemcpyHostToDevice));
-    md = MdDev{v.p, mass.p, ke.p, temp.p, scale.p, xi.p, vxi.p, dt, t0, t1, tdamp, chain, kpart.p, kfirst.p, ksys.p, nchunks};
+    ramp.ensure(2);
+    RXCU(cudaMemset(ramp.p, 0, sizeof(double) * 2));
+    md = MdDev{v.p, mass.p, ke.p, temp.p, scale.p, xi.p, vxi.p, dt, t0, t1, tdamp, chain, kpart.p, kfirst.p, ksys.p, nchunks, ramp.p};
     md_ready = true;
     md_step = 0;
+    drop_graph();
   }
 
   void set_velocities(const double* vin) {
@@ -822,29 +1007,126 @@ struct Context {
     for (int a = 0; a < na; ++a) { vout[3 * a] = h[a].x; vout[3 * a + 1] = h[a].y; vout[3 * a + 2] = h[a].z; }
   }
 
-  void thermostat_half(double frac) {
-    ++launches;
+  void thermostat_half(int advance) {
+    launches += 3;
     k_md_kinetic_part<<<md.nchunks, 256, 0, stream>>>(md, sys.p, type.p);
-    ++launches;
-    k_md_chain<<<blocks(nsys, 64), 64, 0, stream>>>(md, sys.p, nsys, frac);
-    ++launches;
-    k_md_scale<<<blocks(na, 256), 256, 0, stream>>>(md, sys_of.p, na);
+    k_md_chain<<<blocks(nsys, 64), 64, 0, stream>>>(md, sys.p, nsys);
+    k_md_scale<<<blocks(na, 256), 256, 0, stream>>>(md, sys_of.p, na, advance);
   }
 
+  // one velocity-Verlet step with the chain applied for dt/2 on each side (see md_kernels.cu), enqueued only
+  void enqueue_step() {
+    thermostat_half(0);
+    ++launches;
+    k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 1);
+    enqueue_eval(true);
+    ++launches;
+    k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 0);
+    thermostat_half(1);
+  }
+
+  // Capture one step into a CUDA graph (every kernel argument of a step is fixed; what changes from step to step lives
+  // in device memory). Returns false, with graphs switched off for this context, if the capture is refused.
+  long long step_launches = 0;   // this engine's kernels in one captured step
+  bool capture_step() {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      (void)cudaGetLastError();
+      graphs_ok = false;
+      return false;
+    }
+    const long long l0 = launches;
+    bool ok = true;
+    try {
+      enqueue_step();
+    } catch (const Error&) {
+      ok = false;
+    }
+    step_launches = launches - l0;
+    launches = l0;   // the capture itself launched nothing
+    const cudaError_t e = cudaStreamEndCapture(stream, &g);
+    ok = ok && e == cudaSuccess && g && cudaGraphInstantiate(&md_graph, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {
+      md_graph = nullptr;
+      (void)cudaGetLastError();
+      graphs_ok = false;
+    }
+    return ok;
+  }
+
+  // state that a chunk of steps changes, saved before the chunk so that an overflow (lists grown, chunk repeated)
+  // restarts from it
+  DBuf<double4> snap_x, snap_v, snap_g;
+  DBuf<double> snap_q, snap_sh, snap_th, snap_xi, snap_vxi, snap_ramp;
+  void snapshot(bool save) {
+    const size_t n = static_cast<size_t>(na), nc = static_cast<size_t>(nsys) * kMaxChain;
+    if (save) {
+      snap_x.ensure(n); snap_v.ensure(n); snap_g.ensure(n); snap_q.ensure(n); snap_sh.ensure(4 * n); snap_th.ensure(4 * n);
+      snap_xi.ensure(nc); snap_vxi.ensure(nc); snap_ramp.ensure(2);
+    }
+    auto cp = [&](void* dst_snap, void* live, size_t bytes) {
+      if (save) RXCU(cudaMemcpyAsync(dst_snap, live, bytes, cudaMemcpyDeviceToDevice, stream));
+      else RXCU(cudaMemcpyAsync(live, dst_snap, bytes, cudaMemcpyDeviceToDevice, stream));
+    };
+    cp(snap_x.p, x.p, sizeof(double4) * n);
+    cp(snap_v.p, v.p, sizeof(double4) * n);
+    cp(snap_g.p, grad.p, sizeof(double4) * n);
+    cp(snap_q.p, q.p, sizeof(double) * n);
+    cp(snap_sh.p, s_hist.p, sizeof(double) * 4 * n);
+    cp(snap_th.p, t_hist.p, sizeof(double) * 4 * n);
+    cp(snap_xi.p, xi.p, sizeof(double) * nc);
+    cp(snap_vxi.p, vxi.p, sizeof(double) * nc);
+    cp(snap_ramp.p, ramp.p, sizeof(double) * 2);
+  }
+
+  static constexpr int kChunk = 50;   // steps between host synchronisations of rx_md_run
+
+  // Steps are enqueued in chunks without any host synchronisation (from a captured graph when possible); the host reads
+  // the status word once per chunk. A list overflow inside a chunk restores the state saved before it, grows the
+  // lists and repeats the chunk; any other failure is reported.
   void md_run(int nsteps, double* e_out, double* t_out, long long total_steps_hint) {
     if (!md_ready) throw Error(RX_ERR_STATE, "call rx_md_setup first");
-    if (md_step == 0) evaluate(true);   // forces of the initial configuration
+    if (nsteps < 0) throw Error(RX_ERR_INVALID, "negative step count");
     const long long span = total_steps_hint > 0 ? total_steps_hint : nsteps;
-    for (int s = 0; s < nsteps; ++s) {
-      const double frac = span > 0 ? static_cast<double>(s) / static_cast<double>(span) : 0.0;
-      thermostat_half(frac);
-      ++launches;
-      k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 1);
-      evaluate(true);
-      ++launches;
-      k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 0);
-      thermostat_half(frac);
-      ++md_step;
+    const double rh[2] = {0.0, static_cast<double>(span)};
+    RXCU(cudaMemcpyAsync(ramp.p, rh, sizeof rh, cudaMemcpyHostToDevice, stream));
+    if (md_step == 0) evaluate(true);   // forces of the initial configuration
+    int done = 0;
+    while (done < nsteps) {
+      const int chunk = std::min(nsteps - done, kChunk);
+      for (int attempt = 0;; ++attempt) {
+        snapshot(true);
+        RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * kStatusWords, stream));
+        const bool use_graph = graphs_ok && !timing;
+        if (use_graph && !md_graph) capture_step();
+        for (int k = 0; k < chunk; ++k) {
+          if (use_graph && md_graph) {
+            RXCU(cudaGraphLaunch(md_graph, stream));
+            launches += step_launches;
+          } else {
+            enqueue_step();
+            if (timing) {
+              RXCU(cudaStreamSynchronize(stream));
+              collect_times();
+            }
+          }
+        }
+        fetch_qeq_counts();
+        int st[kStatusWords];
+        RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
+        RXCU(cudaStreamSynchronize(stream));
+        RXCU(cudaGetLastError());
+        if (grow_from_status(st, attempt)) {
+          snapshot(false);
+          force_rebuild();
+          continue;
+        }
+        check_status(st, true);
+        break;
+      }
+      done += chunk;
+      md_step += chunk;
     }
     energy_sums();
     if (e_out) RXCU(cudaMemcpyAsync(e_out, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
@@ -968,6 +1250,7 @@ int rx_set_capacities(rx_context* ctx, int nbr_entries, int bonds, int near_entr
     c.bcap = bonds;
     c.ncap_near = (near_entries + 31) / 32 * 32;
     c.alloc_lists();
+    c.force_rebuild();
   });
 }
 
@@ -1007,6 +1290,9 @@ int rx_set_qeq(rx_context* ctx, double swa, double swb, double tol, int imax, in
   });
 }
 int rx_qeq_solve(rx_context* ctx, int* iters, double* rel) { return guarded(ctx, [&](rx::Context& c) { c.qeq_solve(iters, rel); }); }
+int rx_qeq_cg(rx_context* ctx, const double* b, const double* x0, double* x_out, int* iters, double* rel, int* status) {
+  return guarded(ctx, [&](rx::Context& c) { c.qeq_cg(b, x0, x_out, iters, rel, status); });
+}
 int rx_qeq_matvec(rx_context* ctx, const double* v, double* y) { return guarded(ctx, [&](rx::Context& c) { c.qeq_matvec(v, y); }); }
 
 int rx_compute(rx_context* ctx, int flags, double* energies, double* grad, int32_t* census, int64_t* counts) {
@@ -1020,6 +1306,10 @@ int rx_set_velocities(rx_context* ctx, const double* v) { return guarded(ctx, [&
 int rx_get_velocities(rx_context* ctx, double* v) { return guarded(ctx, [&](rx::Context& c) { c.get_velocities(v); }); }
 int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature) {
   return guarded(ctx, [&](rx::Context& c) { c.md_run(nsteps, energies, temperature, 0); });
+}
+
+int rx_set_neighbor(rx_context* ctx, double skin) {
+  return guarded(ctx, [&](rx::Context& c) { c.set_neighbor(skin); });
 }
 
 int rx_get_virial(rx_context* ctx, double* virial) {
@@ -1036,6 +1326,7 @@ void* rx_stream(rx_context* ctx) { return (ctx && ctx->c) ? reinterpret_cast<voi
 int rx_set_timing(rx_context* ctx, int on) {
   return guarded(ctx, [&](rx::Context& c) {
     c.timing = on != 0;
+    c.drop_graph();
     for (auto& p : c.phases) p.ms = 0.0;
   });
 }

@@ -33,6 +33,9 @@ struct CgArgs {
   double* part;    // 2 * 4 * gridDim.x partial sums (double-buffered)
   int* out_iters;
   double* out_rel;
+  int* out_nref;   // FP64 residual passes of the last single-system solve (may be null)
+  int* out_brk;    // per system: 1 after a breakdown (a step length that is not finite)
+  int write_q;     // 1: calculate_Q into the charges (the fix's solve); 0: solutions only
   // segmented CG only
   SysCg* sc;       // nsys
   double2* rb0;    // per-row dot-product terms (fixed-order per-system sums)
@@ -42,11 +45,14 @@ struct CgArgs {
 
 __global__ void k_wrap_bin(Dev d);
 __global__ void k_cell_start(Dev d, const int* sorted_keys);
-__global__ void k_neighbors(Dev d, DevFF ff, QeqParams qp);
+__global__ void k_nbr_check(Dev d);
+__global__ void k_neighbors(Dev d);
+__global__ void k_pairs(Dev d, DevFF ff, QeqParams qp);
 __global__ void k_nonbonded(Dev d, DevFF ff);
 __global__ void k_cg_grid(Dev d, CgArgs a);
 __global__ void k_cg_seg(Dev d, CgArgs a);
 __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, const double* t_hist);
+__global__ void k_qeq_prepare_given(Dev d, DevFF ff, CgArgs a, const double* b, const double* x0);
 __global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist, int strict);
 __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y);
 __global__ void k_energy_sum(Dev d, double* out, double* out_vir);

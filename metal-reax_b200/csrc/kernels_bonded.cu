@@ -92,9 +92,10 @@ __global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl) {
       const int j = static_cast<int>(code & d.amask);
       const int sidx = static_cast<int>(code >> d.abits);
       pair_dvec(d, s, i, j, sidx, dv);
-      dd = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
-      if (dd <= ctl.bond_cut) {
-        const int tj = d.type[j];
+      const double r2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+      dd = sqrt(r2);
+      const int tj = d.type[j];
+      if (dd <= ctl.bond_cut && r2 <= ff.rbo2[ti * ff.nt + tj]) {
         const double* sj = SBp(ff, tj);
         tb = TBp(ff, ti, tj);
         if (si[SB_R_S] > 0.0 && sj[SB_R_S] > 0.0) { C12 = tb[TB_P_BO1] * pow(dd / tb[TB_R_S], tb[TB_P_BO2]); BO_s = (1.0 + bo_cut) * exp(C12); }
@@ -616,6 +617,16 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
   if (warp >= d.na) return;
   const int j = warp;
   const int tj = d.type[j];
+  {   // this kernel's accumulators of atom j start at zero (the acceptor kernel adds to fown_h after it)
+    const int nbj = min(d.bcnt[j], d.bcap);
+    for (int k = lane; k < nbj; k += 32) {
+      d.bcdbo_h[static_cast<size_t>(j) * d.bcap + k] = 0.0;
+      d.bfn_h[static_cast<size_t>(j) * d.bcap + k] = make_double4(0, 0, 0, 0);
+    }
+    if (lane < kVir) d.vir_h[static_cast<size_t>(j) * kVir + lane] = 0.0;
+    if (lane == 0) d.fown_h[j] = make_double4(0, 0, 0, 0);
+    __syncwarp();
+  }
   if (!(ctl.hbond_cut > 0) || static_cast<int>(SBp(ff, tj)[SB_P_HBOND]) != 1) {
     if (lane == 0) {
       d.eatom[static_cast<size_t>(j) * kTerms + E_HB] = 0.0;
@@ -673,10 +684,8 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
     }
     c1 = warp_sum(c1); fi0 = warp_sum(fi0); fi1 = warp_sum(fi1); fi2 = warp_sum(fi2);
     if (lane == 0) {
-      d.bacc[bi].x += c1;
-      double4 fn = d.bfn[bi];
-      fn.x += fi0; fn.y += fi1; fn.z += fi2;
-      d.bfn[bi] = fn;
+      d.bcdbo_h[bi] = c1;
+      d.bfn_h[bi] = make_double4(fi0, fi1, fi2, 0.0);
     }
     __syncwarp();
   }
@@ -684,10 +693,8 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
   for (int c = 0; c < kVir; ++c) vir[c] = warp_sum(vir[c]);
   for (int o = 16; o > 0; o >>= 1) ntrip += __shfl_xor_sync(0xffffffffu, ntrip, o);
   if (lane == 0) {
-    double4 f = d.fown[j];
-    f.x += fj0; f.y += fj1; f.z += fj2;
-    d.fown[j] = f;
-    for (int c = 0; c < kVir; ++c) d.vir[static_cast<size_t>(j) * kVir + c] += vir[c];
+    d.fown_h[j] = make_double4(fj0, fj1, fj2, 0.0);
+    for (int c = 0; c < kVir; ++c) d.vir_h[static_cast<size_t>(j) * kVir + c] = vir[c];
     d.eatom[static_cast<size_t>(j) * kTerms + E_HB] = e;
     d.census[3 * d.na + j] = ntrip;
   }
@@ -735,9 +742,9 @@ __global__ void __launch_bounds__(128) k_hbond_acceptor(Dev d, DevFF ff, DevCtl 
   }
   f0 = warp_sum(f0); f1 = warp_sum(f1); f2 = warp_sum(f2);
   if (lane == 0) {
-    double4 f = d.fown[k];
+    double4 f = d.fown_h[k];
     f.x += f0; f.y += f1; f.z += f2;
-    d.fown[k] = f;
+    d.fown_h[k] = f;
   }
 }
 
@@ -760,6 +767,8 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
     const int ka = static_cast<int>(d.bcode[base + c] & d.amask);
     const int nbk = min(d.bcnt[ka], d.bcap);
     for (int q = 0; q < nbk; ++q) d.Tl[(base + c) * d.bcap + q] = make_double4(0, 0, 0, 0);
+    d.bacc_t[base + c] = make_double4(0, 0, 0, 0);
+    d.bfn_t[base + c] = make_double4(0, 0, 0, 0);
   }
   double fj[3] = {0, 0, 0}, cdd = 0.0, e_tor = 0.0, e_con = 0.0;
   double vir[kVir] = {0, 0, 0, 0, 0, 0};
@@ -916,17 +925,17 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
         const double CEconj5 = -p_cot1 * fn12 * ((cos_omega * cos_omega) - 1.0) * sin_ijk * tan_jkl_i;
         const double CEconj6 = 2.0 * p_cot1 * fn12 * cos_omega * sin_ijk * sin_jkl;
         // coefficients
-        d.bacc[bjk].y += CEtors2;
+        d.bacc_t[bjk].y += CEtors2;
         cdd += CEtors3;
-        d.bacc[bjk].w += CEtors3;
-        d.bacc[bij].x += (CEtors4 + CEconj1);
-        d.bacc[bjk].x += (CEtors5 + CEconj2);
+        d.bacc_t[bjk].w += CEtors3;
+        d.bacc_t[bij].x += (CEtors4 + CEconj1);
+        d.bacc_t[bjk].x += (CEtors5 + CEconj2);
         double4& tl = d.Tl[bjk * d.bcap + pl];
         tl.w += (CEtors6 + CEconj3);
         // gradient
         const double c78 = CEtors7 + CEconj4, c85 = CEtors8 + CEconj5, c96 = CEtors9 + CEconj6;
-        double4 fi = d.bfn[bij];
-        double4 fk = d.bfn[bjk];
+        double4 fi = d.bfn_t[bij];
+        double4 fk = d.bfn_t[bjk];
         double gi[3], gk[3], gl[3];
         for (int c = 0; c < 3; ++c) {
           gi[c] = c78 * pijk_dk[c] + c96 * dco_i[c];
@@ -937,8 +946,8 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
           (&fk.x)[c] += gk[c];
           (&tl.x)[c] += gl[c];
         }
-        d.bfn[bij] = fi;
-        d.bfn[bjk] = fk;
+        d.bfn_t[bij] = fi;
+        d.bfn_t[bjk] = fk;
         {   // virial about j: i at dij, k at djk, l at djk + dkl
           const double pl[3] = {djk[0] + dkl[0], djk[1] + dkl[1], djk[2] + dkl[2]};
           vir_add(vir, dij, gi);
@@ -948,10 +957,8 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
       }
     }
   }
-  double4 f = d.fown[j];
-  f.x += fj[0]; f.y += fj[1]; f.z += fj[2]; f.w += cdd;
-  d.fown[j] = f;
-  for (int c = 0; c < kVir; ++c) d.vir[static_cast<size_t>(j) * kVir + c] += vir[c];
+  d.fown_t[j] = make_double4(fj[0], fj[1], fj[2], cdd);
+  for (int c = 0; c < kVir; ++c) d.vir_t[static_cast<size_t>(j) * kVir + c] = vir[c];
   d.eatom[static_cast<size_t>(j) * kTerms + E_TOR] = e_tor;
   d.eatom[static_cast<size_t>(j) * kTerms + E_CON] = e_con;
   d.census[2 * d.na + j] = ntor;
@@ -973,14 +980,18 @@ __global__ void k_fold(Dev d) {
       const double4 t = d.Tl[static_cast<size_t>(c) * d.bcap + p];
       acc.x += t.x; acc.y += t.y; acc.z += t.z; acc.w += t.w;
     }
-    double* accp = reinterpret_cast<double*>(&d.bacc[base + p]);
-    accp[0] += acc.w;
-    double4 fn = d.bfn[base + p];
+    double4 at = d.bacc_t[base + p];
+    at.x += acc.w;
+    d.bacc_t[base + p] = at;
+    double4 fn = d.bfn_t[base + p];
     fn.x += acc.x; fn.y += acc.y; fn.z += acc.z;
-    d.bfn[base + p] = fn;
+    d.bfn_t[base + p] = fn;
   }
-  double cd = d.fown[a].w;
-  for (int b = 0; b < nb; ++b) cd += reinterpret_cast<const double*>(&d.bacc[d.bsym[base + b]])[3];
+  double cd = d.fown[a].w + d.fown_t[a].w;
+  for (int b = 0; b < nb; ++b) {
+    const int c = d.bsym[base + b];
+    cd += d.bacc[c].w + d.bacc_t[c].w;
+  }
   d.cdtot[a] = cd;
 }
 
@@ -999,7 +1010,10 @@ __global__ void k_dbond(Dev d) {
   for (int k = 0; k < nb; ++k) {
     const size_t b = base + k;
     const int p = static_cast<int>(d.bcode[b] & d.amask);
-    const double4 A = d.bacc[b], B = d.bacc[d.bsym[b]];
+    const int bs = d.bsym[b];
+    const double4 A0 = d.bacc[b], B0 = d.bacc[bs], At = d.bacc_t[b], Bt = d.bacc_t[bs];
+    const double4 A = make_double4(A0.x + d.bcdbo_h[b] + At.x, A0.y + At.y, A0.z + At.z, 0.0);
+    const double4 B = make_double4(B0.x + d.bcdbo_h[bs] + Bt.x, B0.y + Bt.y, B0.z + Bt.z, 0.0);
     const double c_bo = A.x + B.x, c_pi = A.y + B.y, c_pi2 = A.z + B.z, c_dd = cda + d.cdtot[p];
     const double4 C0 = d.bC0[b], C1 = d.bC1[b], C2 = d.bC2[b];
     // C0 = (C1dbo, C2dbo, C3dbo, C1dbopi), C1 = (C2dbopi, C3dbopi, C4dbopi, C1dbopi2), C2 = (C2dbopi2, C3dbopi2, C4dbopi2)
@@ -1033,12 +1047,14 @@ __global__ void k_force_final(Dev d) {
   if (a >= d.na) return;
   const int nb = min(d.bcnt[a], d.bcap);
   const size_t base = static_cast<size_t>(a) * d.bcap;
-  const double4 f1 = d.fown[a], f2 = d.fdb[a], f3 = d.fnb[a];
-  double g[3] = {f1.x + f2.x + f3.x, f1.y + f2.y + f3.y, f1.z + f2.z + f3.z};
+  const double4 f1 = d.fown[a], fh = d.fown_h[a], ft = d.fown_t[a], f2 = d.fdb[a], f3 = d.fnb[a];
+  double g[3] = {f1.x + fh.x + ft.x + f2.x + f3.x, f1.y + fh.y + ft.y + f2.y + f3.y, f1.z + fh.z + ft.z + f2.z + f3.z};
   for (int k = 0; k < nb; ++k) {
     const size_t b = base + k;
     const int p = static_cast<int>(d.bcode[b] & d.amask);
-    const double4 fn = d.bfn[d.bsym[b]];
+    const int bs = d.bsym[b];
+    const double4 fa = d.bfn[bs], fhb = d.bfn_h[bs], ftr = d.bfn_t[bs];
+    const double4 fn = make_double4(fa.x + fhb.x + ftr.x, fa.y + fhb.y + ftr.y, fa.z + fhb.z + ftr.z, 0.0);
     const double Wp = d.W[p];
     const double4 dB = d.bdBOp[b];
     g[0] += fn.x + Wp * dB.x;

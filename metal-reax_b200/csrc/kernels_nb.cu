@@ -8,13 +8,35 @@ namespace cg = cooperative_groups;
 
 namespace rx {
 
+// ------------------------------------------------------------------------------------------------ Verlet check
+// A system's Verlet rows stay valid while no atom of it has moved more than skin/2 since they were built (no pair can
+// then have come from beyond nonb_cut + skin to within nonb_cut). Sets the system's rebuild flag otherwise.
+__global__ void k_nbr_check(Dev d) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= d.na) return;
+  const int s = d.sys_of[a];
+  const double4 x = d.x[a];
+  if (!(isfinite(x.x) && isfinite(x.y) && isfinite(x.z))) {
+    atomicOr(d.status, ST_NONFINITE);
+    return;
+  }
+  if (*reinterpret_cast<volatile const int*>(d.sys_flag + s)) return;
+  const double4 r = d.xref[a];
+  const double dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
+  if (dx * dx + dy * dy + dz * dz > d.half_skin2) atomicOr(d.sys_flag + s, 1);
+}
+
 // ------------------------------------------------------------------------------------------------ wrap + bin
-// Owned atoms are wrapped into the primary cell first (expand_images with wrap_owned, src/neighbor/neighbor.cpp:45-61),
-// then binned into a uniform grid over the fractional coordinates of their system.
+// Atoms of systems being rebuilt are wrapped into the primary cell first (expand_images with wrap_owned,
+// src/neighbor/neighbor.cpp:45-61), then binned into a uniform grid over the fractional coordinates of their system.
+// Between rebuilds positions are never re-wrapped: the lattice shifts in the rows are relative to the positions of
+// the last rebuild.
 __global__ void k_wrap_bin(Dev d) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= d.na) return;
-  const SysInfo s = d.sys[d.sys_of[a]];
+  const int sy = d.sys_of[a];
+  if (!d.sys_flag[sy]) return;   // the atom keeps its key: its system's cells are not used this evaluation
+  const SysInfo s = d.sys[sy];
   double4 x = d.x[a];
   double r[3] = {x.x, x.y, x.z};
   double f[3];
@@ -32,6 +54,7 @@ __global__ void k_wrap_bin(Dev d) {
     x.x = r[0]; x.y = r[1]; x.z = r[2];
     d.x[a] = x;
   }
+  d.xref[a] = x;
   if (!(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]))) atomicOr(d.status, ST_NONFINITE);
   int c[3];
   for (int k = 0; k < 3; ++k) {
@@ -68,33 +91,32 @@ __device__ inline void taper_horner(const double* c, double r, double& Tap, doub
   dTap = g;
 }
 
-// One warp per atom: every image of every atom within nonb_cut (the owned-row cut-off of build_far_list,
-// src/neighbor/neighbor.cpp:180-212). The cells within `range` of the atom's cell are visited as runs of consecutive
-// cells along x (one contiguous range of the cell-ordered atoms per run and periodic image), so the candidate loads are
-// coalesced. Entries are written through a warp ballot in visiting order (deterministic). Fused: the charge-matrix
-// entry H = 14.4 Tap(r) / cbrt(r^3 + (gamma_i gamma_j)^-1.5) for r <= swb (ENGINE_SPEC 7; fix_qeq_reaxff compute_H),
-// and the near row (entries within max(bond_cut, hbond_cut)) the bond and H-bond kernels scan.
-__global__ void __launch_bounds__(128, 6) k_neighbors(Dev d, DevFF ff, QeqParams qp) {
+// Verlet rows, one warp per atom of a system being rebuilt: every image within nonb_cut + skin (a superset of the
+// owned-row cut-off of build_far_list, src/neighbor/neighbor.cpp:180-212). The cells within `range` of the atom's cell
+// are visited as runs of consecutive cells along x (one contiguous range of the cell-ordered atoms per run and periodic
+// image), so the candidate loads are coalesced. Entries are written through a warp ballot in visiting order
+// (deterministic).
+__global__ void __launch_bounds__(128, 6) k_neighbors(Dev d) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
   const int i = warp;
-  const SysInfo s = d.sys[d.sys_of[i]];
+  const int sy = d.sys_of[i];
+  if (!d.sys_flag[sy]) return;
+  const SysInfo s = d.sys[sy];
   const int key = d.cell_key[i] - s.cell_begin;
   const int cx = key % s.nc[0], cy = (key / s.nc[0]) % s.nc[1], cz = key / (s.nc[0] * s.nc[1]);
-  const double rc2 = ff.nonb_cut * ff.nonb_cut;
   const double4 xi = d.x[i];
-  const int ti = d.type[i];
-  const double* shld_i = ff.shld + static_cast<size_t>(ti) * ff.nt;
-  int count = 0, count_near = 0;
+  int count = 0;
   const unsigned lt = (1u << lane) - 1u;
   const int center = (d.S * d.S * d.S - 1) / 2;
-  const size_t rowbase = static_cast<size_t>(i) * d.ncap;
+  const size_t rowbase = static_cast<size_t>(i) * d.vcap;
   // fractional coordinates of i: lower bounds of the distance to a cell slab prune whole runs and clip the x range
   double fi[3];
   for (int k = 0; k < 3; ++k)
     fi[k] = s.R[3 * k] * (xi.x - s.origin[0]) + s.R[3 * k + 1] * (xi.y - s.origin[1]) + s.R[3 * k + 2] * (xi.z - s.origin[2]);
-  const double rc = ff.nonb_cut * (1.0 + 1e-9) + 1e-9;
+  const double rcut = sqrt(d.rv2);
+  const double rc = rcut * (1.0 + 1e-9) + 1e-9;
   auto slab_gap = [&](int k, int c) {   // distance from i to the slab of cell index c (unwrapped) along direction k
     const double lo = static_cast<double>(c) / s.nc[k], hi = static_cast<double>(c + 1) / s.nc[k];
     const double g = fmax(0.0, fmax(lo - fi[k], fi[k] - hi));
@@ -135,50 +157,100 @@ __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d, DevFF ff, QeqParams
           const int p = base + lane;
           bool ok = false;
           int j = 0;
-          double r2 = 0.0;
-          double4 xj = make_double4(0, 0, 0, 0);
           if (p < c1) {
             j = d.cell_atoms[p];
-            xj = d.xs[p];
+            const double4 xj = d.xs[p];
             if (!(j == i && sidx == center)) {
               double dv[3];
               pair_dvec_x(d, s, i, j, sidx, xi, xj, dv);
-              r2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
-              ok = r2 <= rc2;
+              ok = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2] <= d.rv2;
             }
           }
           const unsigned m = __ballot_sync(0xffffffffu, ok);
-          const bool nr = ok && r2 <= d.rnear2;
-          const unsigned mn = __ballot_sync(0xffffffffu, nr);
-          if (nr) {
-            const int posn = count_near + __popc(mn & lt);
-            if (posn < d.ncap_near)
-              d.near[static_cast<size_t>(i) * d.ncap_near + posn] = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
-          }
-          count_near += __popc(mn);
           if (ok) {
             const int pos = count + __popc(m & lt);
-            if (pos < d.ncap) {
-              d.nbr[rowbase + pos] = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
-              const double r = sqrt(r2);
-              double h = 0.0;
-              if (r <= qp.swb) {
-                double Tap, dTap;
-                taper_horner(qp.tap, r, Tap, dTap);
-                const double a3 = r * r * r + shld_i[static_cast<int>(xj.w)];
-                // z = a3^(-1/3): single-precision seed, then two Newton steps z <- z + (z/3)(1 - a3 z^3), which
-                // square the relative error each (1e-7 -> 1e-14 -> rounding level); no division
-                double z = static_cast<double>(rcbrtf(static_cast<float>(a3)));
-                for (int k = 0; k < 2; ++k) z = fma(z * (1.0 / 3.0), fma(-a3 * z, z * z, 1.0), z);
-                h = Tap * 14.4 * z;
-              }
-              d.hval[rowbase + pos] = h;
-            }
+            if (pos < d.vcap) d.vrow[rowbase + pos] = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
           }
           count += __popc(m);
         }
       }
     }
+  }
+  if (lane == 0) {
+    d.vcnt[i] = count;
+    if (count > d.vcap) {
+      atomicOr(d.status, ST_VERLET_OVERFLOW);
+      atomicMax(d.status + 4, count);
+    }
+  }
+}
+
+// The rows of this evaluation, one warp per atom: the entries of the Verlet row within nonb_cut, in Verlet-row order,
+// with the exact FP64 distance test of build_far_list (every cut-off decision is the reference's). Fused: the
+// charge-matrix entry H = 14.4 Tap(r) / cbrt(r^3 + (gamma_i gamma_j)^-1.5) for r <= swb (ENGINE_SPEC 7; fix_qeq_reaxff
+// compute_H) stored as hi + lo single-precision parts, and the near row (entries within max(bond_cut, hbond_cut)) the
+// bond and H-bond kernels scan. Also clears the per-system rebuild flags for the next evaluation.
+__global__ void __launch_bounds__(128) k_pairs(Dev d, DevFF ff, QeqParams qp) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid < d.nsys) d.sys_flag[gid] = 0;
+  const int warp = gid >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= d.na) return;
+  if (lists_failed(d)) return;
+  const int i = warp;
+  const SysInfo s = d.sys[d.sys_of[i]];
+  const double rc2 = ff.nonb_cut * ff.nonb_cut;
+  const double4 xi = d.x[i];
+  const int ti = d.type[i];
+  const double* shld_i = ff.shld + static_cast<size_t>(ti) * ff.nt;
+  int count = 0, count_near = 0;
+  const unsigned lt = (1u << lane) - 1u;
+  const size_t vbase = static_cast<size_t>(i) * d.vcap, rowbase = static_cast<size_t>(i) * d.ncap;
+  const int nv = min(d.vcnt[i], d.vcap);
+  for (int base = 0; base < nv; base += 32) {
+    const int e = base + lane;
+    bool ok = false;
+    unsigned code = 0;
+    int j = 0;
+    double r2 = 0.0;
+    if (e < nv) {
+      code = d.vrow[vbase + e];
+      j = static_cast<int>(code & d.amask);
+      double dv[3];
+      pair_dvec_x(d, s, i, j, static_cast<int>(code >> d.abits), xi, d.x[j], dv);
+      r2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+      ok = r2 <= rc2;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    const bool nr = ok && r2 <= d.rnear2;
+    const unsigned mn = __ballot_sync(0xffffffffu, nr);
+    if (nr) {
+      const int posn = count_near + __popc(mn & lt);
+      if (posn < d.ncap_near) d.near[static_cast<size_t>(i) * d.ncap_near + posn] = code;
+    }
+    count_near += __popc(mn);
+    if (ok) {
+      const int pos = count + __popc(m & lt);
+      if (pos < d.ncap) {
+        d.nbr[rowbase + pos] = code;
+        const double r = sqrt(r2);
+        double h = 0.0;
+        if (r <= qp.swb) {
+          double Tap, dTap;
+          taper_horner(qp.tap, r, Tap, dTap);
+          const double a3 = r * r * r + shld_i[d.type[j]];
+          // z = a3^(-1/3): single-precision seed, then two Newton steps z <- z + (z/3)(1 - a3 z^3), which
+          // square the relative error each (1e-7 -> 1e-14 -> rounding level); no division
+          double z = static_cast<double>(rcbrtf(static_cast<float>(a3)));
+          for (int k = 0; k < 2; ++k) z = fma(z * (1.0 / 3.0), fma(-a3 * z, z * z, 1.0), z);
+          h = Tap * 14.4 * z;
+        }
+        const float hi = static_cast<float>(h);
+        d.hhi[rowbase + pos] = hi;
+        d.hlo[rowbase + pos] = static_cast<float>(h - static_cast<double>(hi));
+      }
+    }
+    count += __popc(m);
   }
   if (lane == 0) {
     d.nbr_cnt[i] = count;
@@ -310,8 +382,8 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
   for (int o = 16; o > 0; o >>= 1) counted += __shfl_xor_sync(0xffffffffu, counted, o);
   if (lane == 0) {
     d.fnb[i] = make_double4(gx, gy, gz, 0.0);
-    double* vi = d.vir + static_cast<size_t>(i) * kVir;
-    vi[0] += v0; vi[1] += v1; vi[2] += v2; vi[3] += v3; vi[4] += v4; vi[5] += v5;
+    double* vi = d.vir_nb + static_cast<size_t>(i) * kVir;
+    vi[0] = v0; vi[1] = v1; vi[2] = v2; vi[3] = v3; vi[4] = v4; vi[5] = v5;
     d.eatom[static_cast<size_t>(i) * kTerms + E_VDW] = ev;
     d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] = ee;
     const double chi = ff.sb[ti * SB_N + SB_CHI], eta = ff.sb[ti * SB_N + SB_ETA], qd = d.q[i];
@@ -321,19 +393,31 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
 }
 
 // ------------------------------------------------------------------------------------------------ QEq CG
-// y = (diag(eta) + H) v for one row, both right-hand sides (s, t) at once; warp per row, lane-strided entries.
+// y = (diag(eta) + H) v for one row, both right-hand sides (s, t) at once; warp per row, each lane taking four
+// consecutive entries per pass with 16-byte loads (rows start 128-byte aligned: ncap is a multiple of 32). FULL: H as
+// hi + lo (the FP64 matrix to ~1e-15); otherwise hi alone (the single-precision matrix of the inner CG iterations).
+template <bool FULL>
 __device__ inline double2 row_mv(const Dev& d, int i, double eta, const double2* v) {
   const int cnt = min(d.nbr_cnt[i], d.ncap);
   const int lane = threadIdx.x & 31;
   double ys = 0.0, yt = 0.0;
   const size_t base = static_cast<size_t>(i) * d.ncap;
-#pragma unroll 4
-  for (int e = lane; e < cnt; e += 32) {
-    const double h = d.hval[base + e];
-    const int j = static_cast<int>(d.nbr[base + e] & d.amask);
-    const double2 vj = v[j];
-    ys += h * vj.x;
-    yt += h * vj.y;
+  for (int e0 = lane * 4; e0 < cnt; e0 += 128) {
+    const uint4 c4 = *reinterpret_cast<const uint4*>(d.nbr + base + e0);
+    const float4 h4 = *reinterpret_cast<const float4*>(d.hhi + base + e0);
+    float4 l4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (FULL) l4 = *reinterpret_cast<const float4*>(d.hlo + base + e0);
+    const unsigned cc[4] = {c4.x, c4.y, c4.z, c4.w};
+    const float hh[4] = {h4.x, h4.y, h4.z, h4.w}, ll[4] = {l4.x, l4.y, l4.z, l4.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (e0 + k < cnt) {
+        const double h = FULL ? static_cast<double>(hh[k]) + static_cast<double>(ll[k]) : static_cast<double>(hh[k]);
+        const double2 vj = v[cc[k] & d.amask];
+        ys += h * vj.x;
+        yt += h * vj.y;
+      }
+    }
   }
   ys = warp_sum(ys);
   yt = warp_sum(yt);
@@ -380,10 +464,17 @@ __device__ inline void grid_totals(const double* part, int nblocks, double* tot,
 }
 
 // Persistent cooperative Jacobi-PCG for one system, s and t solved together: the stock loop of fix qeq/reaxff as
-// reproduced in plugin/adapter/fix_qeq_reaxff_metal.cpp:89-123, in FP64, each system stopping on its own test
-// sqrt(r.M^-1 r)/|b| <= tol with at most imax-1 iterations. Then calculate_Q: q = s - (sum s / sum t) t.
+// reproduced in plugin/adapter/fix_qeq_reaxff_metal.cpp:89-123, each right-hand side stopping on its own test
+// sqrt(r.M^-1 r)/|b| <= tol with at most imax-1 iterations; then calculate_Q: q = s - (sum s / sum t) t.
+// Precision (the resident refinement of src/metal/metal_backend.mm:435-530, in FP64 instead of double-single): the
+// iterations multiply by the single-precision matrix (hi: 8 bytes per entry with its index), the vectors and every dot
+// product are FP64, and the residual is recomputed with the FP64 matrix (hi + lo) whenever the iterations have
+// converged - or have reduced the residual by kRefineDrop, below which the single-precision matrix stops helping. The
+// solve ends only on that FP64 residual, so the tolerance and the reported residuals are those of the FP64 system.
 // Rows are distributed over all warps of the grid; reductions are fixed-order (per-block partials summed in block
 // order), so the result is bitwise reproducible. Only grid.sync() waits; the kernel is launched cooperatively.
+constexpr double kRefineDrop = 1e-6;
+
 __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   cg::grid_group g = cg::this_grid();
   __shared__ double sh[64 * 4];
@@ -396,86 +487,96 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   double loc[4], tot[4];
   int phase = 0;
   auto partbuf = [&]() { return a.part + static_cast<size_t>(phase & 1) * gridDim.x * 4; };
-  // r = b - A x ; d = M^-1 r
-  loc[0] = loc[1] = loc[2] = loc[3] = 0.0;
-  for (int r = gw; r < n; r += nwarps) {
-    const int i = i0 + r;
-    const double eta = a.eta[i];
-    const double2 y = row_mv(d, i, eta, a.x);
-    if (lane == 0) {
-      const double2 b = a.b[i];
-      const double2 rr = make_double2(b.x - y.x, b.y - y.y);
-      a.r[i] = rr;
-      const double2 dd = make_double2(rr.x / eta, rr.y / eta);
-      a.d[i] = dd;
-      loc[0] += b.x * b.x; loc[1] += b.y * b.y; loc[2] += rr.x * dd.x; loc[3] += rr.y * dd.y;
-    }
-  }
-  block_partials<4>(loc, partbuf(), sh);
-  g.sync();
-  grid_totals<4>(partbuf(), gridDim.x, tot, tot_sh);
-  ++phase;
-  const double bnorm_s = sqrt(tot[0]), bnorm_t = sqrt(tot[1]);
-  double sig_s = tot[2], sig_t = tot[3];
-  bool act_s = true, act_t = true;
-  int it_s = 1, it_t = 1;
-  int it;
-  bool breakdown = false;
-  for (it = 1; it < a.imax; ++it) {
-    act_s = act_s && (sqrt(sig_s) / bnorm_s > a.tol);
-    act_t = act_t && (sqrt(sig_t) / bnorm_t > a.tol);
-    if (!act_s && !act_t) break;
-    // q = A d ; partial d.q
-    loc[0] = loc[1] = 0.0;
+  double bnorm_s = 0.0, bnorm_t = 0.0, sig_s = 0.0, sig_t = 0.0;
+  bool act_s = true, act_t = true, breakdown = false;
+  int it_s = 1, it_t = 1, nref = 0;
+  for (;;) {
+    // ---- FP64 residual: r = b - A x ; d = M^-1 r ; r.d (and |b|^2 on the first pass)
+    loc[0] = loc[1] = loc[2] = loc[3] = 0.0;
     for (int r = gw; r < n; r += nwarps) {
       const int i = i0 + r;
-      const double2 y = row_mv(d, i, a.eta[i], a.d);
+      const double eta = a.eta[i];
+      const double2 y = row_mv<true>(d, i, eta, a.x);
       if (lane == 0) {
-        a.q[i] = y;
-        const double2 dd = a.d[i];
-        loc[0] += dd.x * y.x; loc[1] += dd.y * y.y;
+        const double2 b = a.b[i];
+        const double2 rr = make_double2(b.x - y.x, b.y - y.y);
+        a.r[i] = rr;
+        const double2 dd = make_double2(rr.x / eta, rr.y / eta);
+        a.d[i] = dd;
+        loc[0] += b.x * b.x; loc[1] += b.y * b.y; loc[2] += rr.x * dd.x; loc[3] += rr.y * dd.y;
       }
     }
-    block_partials<2>(loc, partbuf(), sh);
+    block_partials<4>(loc, partbuf(), sh);
     g.sync();
-    grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
+    grid_totals<4>(partbuf(), gridDim.x, tot, tot_sh);
     ++phase;
-    const double alpha_s = act_s ? sig_s / tot[0] : 0.0;
-    const double alpha_t = act_t ? sig_t / tot[1] : 0.0;
-    if (!(isfinite(alpha_s) && isfinite(alpha_t))) { breakdown = true; break; }
-    // x += alpha d ; r -= alpha q ; p = M^-1 r ; partial r.p
-    loc[0] = loc[1] = 0.0;
-    for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
-      const int i = i0 + r;
-      const double2 dd = a.d[i], qq = a.q[i];
-      double2 xx = a.x[i], rr = a.r[i];
-      xx.x += alpha_s * dd.x; xx.y += alpha_t * dd.y;
-      rr.x -= alpha_s * qq.x; rr.y -= alpha_t * qq.y;
-      a.x[i] = xx;
-      a.r[i] = rr;
-      const double eta = a.eta[i];
-      const double2 pp = make_double2(rr.x / eta, rr.y / eta);
-      a.p[i] = pp;
-      loc[0] += rr.x * pp.x; loc[1] += rr.y * pp.y;
+    ++nref;
+    if (nref == 1) { bnorm_s = sqrt(tot[0]); bnorm_t = sqrt(tot[1]); }
+    if (act_s) sig_s = tot[2];
+    if (act_t) sig_t = tot[3];
+    act_s = act_s && (sqrt(sig_s) / bnorm_s > a.tol);
+    act_t = act_t && (sqrt(sig_t) / bnorm_t > a.tol);
+    if ((!act_s || it_s >= a.imax) && (!act_t || it_t >= a.imax)) break;
+    const double stop_s = fmax(a.tol * bnorm_s, kRefineDrop * sqrt(sig_s));
+    const double stop_t = fmax(a.tol * bnorm_t, kRefineDrop * sqrt(sig_t));
+    // ---- single-precision-matrix iterations from this residual
+    for (;;) {
+      const bool in_s = act_s && it_s < a.imax && sqrt(sig_s) > stop_s;
+      const bool in_t = act_t && it_t < a.imax && sqrt(sig_t) > stop_t;
+      if (!in_s && !in_t) break;
+      // q = A d ; partial d.q
+      loc[0] = loc[1] = 0.0;
+      for (int r = gw; r < n; r += nwarps) {
+        const int i = i0 + r;
+        const double2 y = row_mv<false>(d, i, a.eta[i], a.d);
+        if (lane == 0) {
+          a.q[i] = y;
+          const double2 dd = a.d[i];
+          loc[0] += dd.x * y.x; loc[1] += dd.y * y.y;
+        }
+      }
+      block_partials<2>(loc, partbuf(), sh);
+      g.sync();
+      grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
+      ++phase;
+      const double alpha_s = in_s ? sig_s / tot[0] : 0.0;
+      const double alpha_t = in_t ? sig_t / tot[1] : 0.0;
+      if (!(isfinite(alpha_s) && isfinite(alpha_t))) { breakdown = true; break; }
+      // x += alpha d ; r -= alpha q ; p = M^-1 r ; partial r.p
+      loc[0] = loc[1] = 0.0;
+      for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+        const int i = i0 + r;
+        const double2 dd = a.d[i], qq = a.q[i];
+        double2 xx = a.x[i], rr = a.r[i];
+        xx.x += alpha_s * dd.x; xx.y += alpha_t * dd.y;
+        rr.x -= alpha_s * qq.x; rr.y -= alpha_t * qq.y;
+        a.x[i] = xx;
+        a.r[i] = rr;
+        const double eta = a.eta[i];
+        const double2 pp = make_double2(rr.x / eta, rr.y / eta);
+        a.p[i] = pp;
+        loc[0] += rr.x * pp.x; loc[1] += rr.y * pp.y;
+      }
+      block_partials<2>(loc, partbuf(), sh);
+      g.sync();
+      grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
+      ++phase;
+      const double beta_s = in_s ? tot[0] / sig_s : 0.0;
+      const double beta_t = in_t ? tot[1] / sig_t : 0.0;
+      if (in_s) { sig_s = tot[0]; ++it_s; }
+      if (in_t) { sig_t = tot[1]; ++it_t; }
+      // d = p + beta d (only for the right-hand sides still iterating)
+      for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+        const int i = i0 + r;
+        const double2 pp = a.p[i];
+        double2 dd = a.d[i];
+        if (in_s) dd.x = pp.x + beta_s * dd.x;
+        if (in_t) dd.y = pp.y + beta_t * dd.y;
+        a.d[i] = dd;
+      }
+      g.sync();
     }
-    block_partials<2>(loc, partbuf(), sh);
-    g.sync();
-    grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
-    ++phase;
-    const double beta_s = act_s ? tot[0] / sig_s : 0.0;
-    const double beta_t = act_t ? tot[1] / sig_t : 0.0;
-    if (act_s) { sig_s = tot[0]; it_s = it + 1; }
-    if (act_t) { sig_t = tot[1]; it_t = it + 1; }
-    // d = p + beta d (only for the systems still iterating)
-    for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
-      const int i = i0 + r;
-      const double2 pp = a.p[i];
-      double2 dd = a.d[i];
-      if (act_s) dd.x = pp.x + beta_s * dd.x;
-      if (act_t) dd.y = pp.y + beta_t * dd.y;
-      a.d[i] = dd;
-    }
-    g.sync();
+    if (breakdown) break;
   }
   // calculate_Q: q = s - (sum s / sum t) t
   loc[0] = loc[1] = 0.0;
@@ -488,15 +589,18 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
   ++phase;
   const double u = tot[0] / tot[1];
-  for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
-    const double2 xx = a.x[i0 + r];
-    d.q[i0 + r] = xx.x - u * xx.y;
-  }
+  if (a.write_q)
+    for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+      const double2 xx = a.x[i0 + r];
+      d.q[i0 + r] = xx.x - u * xx.y;
+    }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (a.out_brk) a.out_brk[0] = breakdown ? 1 : 0;
     a.out_iters[0] = it_s;
     a.out_iters[1] = it_t;
     a.out_rel[0] = sqrt(sig_s) / bnorm_s;
     a.out_rel[1] = sqrt(sig_t) / bnorm_t;
+    if (a.out_nref) a.out_nref[0] = nref;
     if (breakdown) atomicOr(d.status, ST_CG_BREAKDOWN);
     if (!(a.out_rel[0] <= a.tol && a.out_rel[1] <= a.tol)) atomicOr(d.status, ST_CG_NOTCONV);
   }
@@ -578,7 +682,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_seg(Dev d, CgArgs a) {
         cnt = 0;
       }
       const double eta = a.eta[i];
-      const double2 y = row_mv(d, i, eta, a.x);
+      const double2 y = row_mv<true>(d, i, eta, a.x);
       if (lane == 0) {
         const double2 b = a.b[i];
         const double2 rr = make_double2(b.x - y.x, b.y - y.y);
@@ -624,7 +728,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_seg(Dev d, CgArgs a) {
           live = __ldcg(&a.sc[s].live) != 0;
         }
         if (!live) continue;
-        const double2 y = row_mv(d, i, a.eta[i], a.d);
+        const double2 y = row_mv<true>(d, i, a.eta[i], a.d);
         if (lane == 0) {
           a.q[i] = y;
           const double2 dd = a.d[i];
@@ -710,12 +814,14 @@ __global__ void __launch_bounds__(256, 4) k_cg_seg(Dev d, CgArgs a) {
     const SysInfo& si = d.sys[s];
     const double2 sum = sys_sum2(a.x, si.begin, si.natoms);
     const double u = sum.x / sum.y;
-    for (int k = lane; k < si.natoms; k += 32) {
-      const double2 xx = a.x[si.begin + k];
-      d.q[si.begin + k] = xx.x - u * xx.y;
-    }
+    if (a.write_q)
+      for (int k = lane; k < si.natoms; k += 32) {
+        const double2 xx = a.x[si.begin + k];
+        d.q[si.begin + k] = xx.x - u * xx.y;
+      }
     if (lane == 0) {
       const SysCg& c = a.sc[s];
+      if (a.out_brk) a.out_brk[s] = c.breakdown;
       a.out_iters[2 * s] = c.it_s;
       a.out_iters[2 * s + 1] = c.it_t;
       a.out_rel[2 * s] = sqrt(c.sig_s) / c.bnorm_s;
@@ -740,6 +846,16 @@ __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, c
   a.eta[i] = ff.sb[t * SB_N + SB_ETA];
 }
 
+// A solve of given right-hand sides from given guesses (mtl::Context::qeq_solve, metal_backend.hpp:84-86): b and x0
+// hold the s system for every atom, then the t system.
+__global__ void k_qeq_prepare_given(Dev d, DevFF ff, CgArgs a, const double* b, const double* x0) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.na) return;
+  a.x[i] = x0 ? make_double2(x0[i], x0[d.na + i]) : make_double2(0.0, 0.0);
+  a.b[i] = make_double2(b[i], b[d.na + i]);
+  a.eta[i] = ff.sb[d.type[i] * SB_N + SB_ETA];
+}
+
 // the solve just finished becomes the newest history entry; not after a list overflow (the evaluation is repeated),
 // nor after a failed solve (a breakdown, or a system above its tolerance in strict mode): the call then reports an
 // error and leaves the histories as they were
@@ -761,7 +877,7 @@ __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (warp >= d.na) return;
   const double eta = ff.sb[d.type[warp] * SB_N + SB_ETA];
-  const double2 r = row_mv(d, warp, eta, v);
+  const double2 r = row_mv<true>(d, warp, eta, v);
   if ((threadIdx.x & 31) == 0) y[warp] = r;
 }
 
@@ -773,9 +889,15 @@ __global__ void k_energy_sum(Dev d, double* out, double* out_vir) {
   const SysInfo s = d.sys[sidx];
   __shared__ double sh[256];
   double v = 0.0;
-  const double* src = t < kTerms ? d.eatom + t : d.vir + (t - kTerms);
-  const int stride = t < kTerms ? kTerms : kVir;
-  for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) v += src[static_cast<size_t>(s.begin + r) * stride];
+  if (t < kTerms) {
+    for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) v += d.eatom[static_cast<size_t>(s.begin + r) * kTerms + t];
+  } else {
+    const int c = t - kTerms;
+    for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) {
+      const size_t k = static_cast<size_t>(s.begin + r) * kVir + c;
+      v += ((d.vir[k] + d.vir_h[k]) + d.vir_t[k]) + d.vir_nb[k];
+    }
+  }
   sh[threadIdx.x] = v;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {

@@ -21,14 +21,17 @@ struct MdDev {
   const int* kchunk_first;  // nsys + 1: first chunk of each system
   const int* kchunk_sys;    // system of each chunk
   int nchunks;
+  // temperature ramp of the current run (device-resident, so a captured step takes no per-step argument):
+  // ramp[0] = steps done in this run, ramp[1] = steps of the run; T = t_start + (done / steps) (t_stop - t_start)
+  double* ramp;
 };
 
 constexpr int kKeChunk = 1024;
 
 __global__ void k_md_kinetic_part(MdDev m, const SysInfo* sys, const int* type);
 __global__ void k_md_kinetic_sum(MdDev m, int nsys);
-__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys, double step_frac);
-__global__ void k_md_scale(MdDev m, const int* sys_of, int na);
+__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys);
+__global__ void k_md_scale(MdDev m, const int* sys_of, int na, int advance);
 __global__ void k_md_kick(MdDev m, const int* type, const double4* grad, double4* x, int na, int drift);
 
 }  // namespace rx

@@ -50,9 +50,10 @@ __global__ void k_md_kinetic_sum(MdDev m, int nsys) {
 }
 
 // one thread per system: advance the chain by dt/2 and produce the velocity scale factor
-__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys, double step_frac) {
+__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
+  const double step_frac = m.ramp[1] > 0.0 ? m.ramp[0] / m.ramp[1] : 0.0;
   const int M = m.chain;
   double* xi = m.xi + s * kMaxChain;
   double* vx = m.vxi + s * kMaxChain;
@@ -88,8 +89,10 @@ __global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys, double step_fr
   m.temp[s] = ke2 / (nf * kBoltz);
 }
 
-__global__ void k_md_scale(MdDev m, const int* sys_of, int na) {
+// velocities times their system's chain scale; with `advance` (the second half of a step) the ramp's step count too
+__global__ void k_md_scale(MdDev m, const int* sys_of, int na, int advance) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (advance && a == 0) m.ramp[0] += 1.0;
   if (a >= na) return;
   const double sc = m.scale[sys_of[a]];
   double4 v = m.v[a];

@@ -31,7 +31,7 @@ EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
-           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial"]
+           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -70,7 +70,7 @@ def load():
         "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
         "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
-        "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]),
+        "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -132,6 +132,9 @@ class Engine:
 
     def set_control(self, bond_cut=5.0, hbond_cut=7.5, thb_cut=0.001, thb_cutsq=0.00001, enobonds=True):
         self._check(self.lib.rx_set_control(self.h, bond_cut, hbond_cut, thb_cut, thb_cutsq, 1 if enobonds else 0))
+
+    def set_neighbor(self, skin=1.0):
+        self._check(self.lib.rx_set_neighbor(self.h, skin))
 
     def set_qeq(self, swa=0.0, swb=10.0, tol=1e-6, imax=200, strict=False):
         self._check(self.lib.rx_set_qeq(self.h, swa, swb, tol, imax, 1 if strict else 0))
@@ -198,6 +201,17 @@ class Engine:
         rel = np.zeros(2 * self.nsys)
         self._check(self.lib.rx_qeq_solve(self.h, _p(it), _p(rel)))
         return {"q": self.get_charges(), "iters": it.reshape(-1, 2), "rel": rel.reshape(-1, 2)}
+
+    def qeq_cg(self, b, x0=None):
+        """Both CG systems for given right-hand sides b (2, NA) and guesses x0 (2, NA) (mtl::Context::qeq_solve)."""
+        b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1)
+        x0 = None if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).reshape(-1)
+        x = np.zeros(2 * self.na)
+        it = np.zeros(2 * self.nsys, dtype=np.int32)
+        rel = np.zeros(2 * self.nsys)
+        st = np.zeros(2 * self.nsys, dtype=np.int32)
+        self._check(self.lib.rx_qeq_cg(self.h, _p(b), _p(x0), _p(x), _p(it), _p(rel), _p(st)))
+        return {"x": x.reshape(2, -1), "iters": it.reshape(-1, 2), "rel": rel.reshape(-1, 2), "status": st.reshape(-1, 2)}
 
     def qeq_matvec(self, v):
         v = np.ascontiguousarray(v, dtype=np.float64)

@@ -347,3 +347,48 @@ def test_vdw_variants_match_oracle(variant):
             assert np.array_equal(out["census"][k], ref["census"][k]), (variant, s["name"], k)
         assert np.abs(eng.virial()[0] - ref["virial"]).max() / n <= C3_ENERGY_PER_ATOM
     eng.close()
+
+
+def test_qeq_cg_given_rhs_and_guesses(engine, oracle):
+    """mtl::Context::qeq_solve (metal_backend.hpp:84-86) through rx_qeq_cg: the stock right-hand sides (-chi, -1) from
+    the oracle's own guesses give the oracle's s and t; iteration limit reported as status 3; the charges are left
+    alone."""
+    s = small_systems()[0]
+    n = len(s["type"])
+    engine.set_systems([s])
+    engine.set_charges(np.zeros(n))
+    engine.set_qeq(0.0, 10.0, 1e-12, 400)
+    rng = np.random.default_rng(9)
+    s0, t0 = rng.normal(scale=0.1, size=n), rng.normal(scale=0.1, size=n)
+    ref = oracle.qeq(s, tol=1e-12, imax=400, s0=s0, t0=t0)
+    b = np.stack([-oracle.chi(s["type"]), -np.ones(n)])
+    got = engine.qeq_cg(b, np.stack([s0, t0]))
+    assert np.abs(got["x"][0] - ref["s"]).max() <= 1e-10 and np.abs(got["x"][1] - ref["t"]).max() <= 1e-10
+    assert got["status"].tolist() == [[1, 1]] and got["rel"].max() <= 1e-12
+    assert np.abs(engine.get_charges()).max() == 0.0
+    engine.set_qeq(0.0, 10.0, 1e-12, 3)
+    lim = engine.qeq_cg(b)
+    assert lim["status"].tolist() == [[3, 3]] and lim["iters"].max() <= 3
+    engine.set_qeq()
+
+
+def test_set_systems_keeps_charge_history_by_tag(engine):
+    """Re-neighbouring (the same atoms handed over again, in another order) keeps each atom's charge history, so the
+    next solve starts warm: it takes no more iterations than a solve that was never interrupted, and far fewer than
+    a cold one."""
+    s = small_systems()[0]
+    engine.set_qeq(0.0, 10.0, 1e-8, 200)
+    engine.set_systems([s])
+    for _ in range(3):
+        engine.compute(qeq=True)
+    engine.compute(qeq=True)
+    warm = engine.qeq_last()["iters"].max()
+    perm = np.random.default_rng(3).permutation(len(s["type"]))
+    sp = dict(s, x=s["x"][perm], type=s["type"][perm], tag=s["tag"][perm])
+    engine.set_systems([sp])
+    engine.compute(qeq=True)
+    after = engine.qeq_last()["iters"].max()
+    engine.compute(qeq=True, cold=True)
+    cold = engine.qeq_last()["iters"].max()
+    assert after <= warm + 1 and after < cold, (warm, after, cold)
+    engine.set_qeq()
