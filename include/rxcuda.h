@@ -64,8 +64,9 @@ int rx_set_control(rx_context* ctx, double bond_cut, double hbond_cut, double th
 /* The systems of this context. natoms[nsys]; origin[3*nsys]; box[9*nsys] lattice vectors a, b, c as rows;
  * periodic[3*nsys] (must be 1: the engine is periodic in all directions); type[NA] force-field type index;
  * tag[NA] atom ids, unique within a system (the owner-computes tie-breaks of neighbor.cpp:295-310 use them).
- * The charge-equilibration histories (the warm start of the next solve) carry over for every atom whose system index
- * and tag existed before the call, wherever it now sits in the arrays; new atoms start from zero. */
+ * The charge-equilibration histories (the warm start of the next solve) carry over for every atom whose tag existed
+ * before the call in the system of the same index, atom count and lattice (the same system handed over again, e.g.
+ * after re-neighbouring), wherever the atom now sits in the arrays; other atoms and systems start from zero. */
 int rx_set_systems(rx_context* ctx, int nsys, const int* natoms, const double* origin, const double* box, const int* periodic,
                    const int* type, const int64_t* tag);
 int rx_num_atoms(const rx_context* ctx);
@@ -93,6 +94,9 @@ int rx_set_qeq(rx_context* ctx, double swa, double swb, double tol, int imax, in
  * Jacobi-preconditioned CG from the history-extrapolated guesses (Q-23), sets q = s - (sum s / sum t) t
  * (calculate_Q) and advances the histories. iters[2*nsys] and rel[2*nsys] (s then t per system) may be NULL. */
 int rx_qeq_solve(rx_context* ctx, int* iters, double* rel);
+/* Zeroes the charge-equilibration histories (the stock fix's s_hist/t_hist at initialisation): the next solve starts
+ * from s = t = 0. */
+int rx_qeq_reset(rx_context* ctx);
 /* mtl::Context::qeq_solve (metal_backend.hpp:84-86) for the caller's right-hand sides and guesses, as the resident
  * fix hands them over (fix_qeq_reaxff_metal.cpp:69-75): builds the charge matrix of the current positions, then runs
  * the CG of both systems. b[2*NA] (the s system for every atom, then the t system), x0[2*NA] (same layout; NULL = 0),
@@ -113,6 +117,13 @@ int rx_qeq_last(const rx_context* ctx, int32_t* iters, double* rel);
  * angle_sets, torsions, hbonds, nonbonded, sbo_region, lp_trunc; only with RX_COMPUTE_CENSUS), counts[4] (bonds,
  * counted non-bonded pairs, neighbor entries, H-bond triples). Any output pointer may be NULL. */
 int rx_compute(rx_context* ctx, int flags, double* energies, double* grad, int32_t* census, int64_t* counts);
+
+/* The pair side of fix acks2/reaxff (add_acks2_terms, src/cpu/acks2.cpp:11-63; pair_reaxff_metal.cpp:482-485,492):
+ * s_kin[NA] the kinetic potentials of the fix's solution (its s[N + i]), or NULL to switch the terms off. While set,
+ * every force evaluation adds the polarization coupling 23.02 q s and the bond-softness Coulomb term over the pairs
+ * within (bcut_acks2_i + bcut_acks2_j)/2 (softness = general parameter 34) to the Coulomb and polarization energies,
+ * the forces and the virial. rx_set_systems switches them off. */
+int rx_set_acks2(rx_context* ctx, const double* s_kin);
 
 /* Virial of the most recent force evaluation (rx_compute or the last rx_md_run step) per system: virial[6*nsys] in
  * LAMMPS's order xx, yy, zz, xy, xz, yz, the sum of x_a f_b over every atom and periodic image (kcal/mol) - what

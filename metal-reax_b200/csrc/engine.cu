@@ -133,7 +133,7 @@ struct Context {
   DBuf<long long> counters;
   DBuf<double> energies, virial, vir, vir_nb, vir_h, vir_t;
   // QEq
-  DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
+  DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q, cg_w;
   DBuf<double> cg_eta, cg_part, s_hist, t_hist, cg_rel;
   DBuf<int> cg_iters, cg_nlive, cg_nref, cg_brk;
   DBuf<SysCg> cg_sys;
@@ -356,6 +356,7 @@ struct Context {
     std::vector<double> old_sh, old_th;
     std::vector<long long> old_tag = htag;
     std::vector<int> old_sys = hsys_of;
+    const std::vector<SysInfo> old_info = hsys;
     const int old_nsys = nsys;
     if (na > 0 && s_hist.p && static_cast<size_t>(na) == old_tag.size()) {
       old_sh.resize(4 * static_cast<size_t>(na));
@@ -395,9 +396,18 @@ struct Context {
       if (!old_sh.empty()) {
         std::vector<std::unordered_map<long long, int>> by_sys(static_cast<size_t>(old_nsys));
         for (size_t k = 0; k < old_tag.size(); ++k) by_sys[static_cast<size_t>(old_sys[k])].emplace(old_tag[k], static_cast<int>(k));
+        // a system is the same one handed over again (and keeps its atoms' histories) when its index, atom count and
+        // lattice are unchanged; otherwise it starts cold
+        std::vector<char> same(static_cast<size_t>(nsys), 0);
+        for (int sy = 0; sy < std::min(nsys, old_nsys); ++sy) {
+          const SysInfo& o = old_info[static_cast<size_t>(sy)];
+          bool eq = o.natoms == natoms[sy];
+          for (int c = 0; c < 9; ++c) eq = eq && o.L[c] == box[9 * sy + c];
+          same[static_cast<size_t>(sy)] = eq ? 1 : 0;
+        }
         for (int a = 0; a < na; ++a) {
           const int sy = hsys_of[static_cast<size_t>(a)];
-          if (sy >= old_nsys) continue;
+          if (sy >= old_nsys || !same[static_cast<size_t>(sy)]) continue;
           const auto it = by_sys[static_cast<size_t>(sy)].find(htag[static_cast<size_t>(a)]);
           if (it == by_sys[static_cast<size_t>(sy)].end()) continue;
           for (int c = 0; c < 4; ++c) {
@@ -411,6 +421,7 @@ struct Context {
     }
     have_pos = false;
     have_virial = false;
+    acks2_on = false;
     md_ready = false;
     ncap = 0;
     bcap = 0;
@@ -532,10 +543,10 @@ struct Context {
     vir.ensure(n * kVir);
     vir_nb.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
     fown_h.ensure(n); fown_t.ensure(n);
-    cg_x.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
+    cg_x.ensure(n); cg_w.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
     cg_sys.ensure(nsys); cg_rb0.ensure(n); cg_rb1.ensure(n); cg_nlive.ensure(2);
-    cg_part.ensure(8 * static_cast<size_t>(std::max(nsm, 1)) * 32);
+    cg_part.ensure(16 * static_cast<size_t>(std::max(nsm, 1)) * 32);
   }
 
   void alloc_lists() {
@@ -627,7 +638,7 @@ struct Context {
   CgArgs cg_args() {
     CgArgs a{};
     a.imax = qeq_imax; a.tol = qeq_tol;
-    a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.eta = cg_eta.p; a.part = cg_part.p;
+    a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.w = cg_w.p; a.eta = cg_eta.p; a.part = cg_part.p;
     a.out_iters = cg_iters.p; a.out_rel = cg_rel.p; a.out_nref = cg_nref.p; a.out_brk = cg_brk.p; a.write_q = 1;
     return a;
   }
@@ -684,6 +695,10 @@ struct Context {
     tic(5, "nonbonded");
     ++launches;
     k_nonbonded<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, nbs>>>(d, dff);
+    if (acks2_on) {
+      ++launches;
+      k_acks2<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, nbs>>>(d, dff, s_kin.p);
+    }
     toc(5);
     if (conc) RXCU(cudaEventRecord(ev_join, side));
     tic(2, "bond_orders");
@@ -856,6 +871,25 @@ struct Context {
       counts[2] = sn;
       counts[3] = hb;
     }
+  }
+
+  // the pair side of fix acks2/reaxff: kinetic potentials per atom (NULL switches the terms off)
+  bool acks2_on = false;
+  DBuf<double> s_kin;
+  void set_acks2(const double* sk) {
+    require_sys();
+    drop_graph();
+    acks2_on = sk != nullptr;
+    if (!sk) return;
+    s_kin.ensure(static_cast<size_t>(na));
+    RXCU(cudaMemcpy(s_kin.p, sk, sizeof(double) * na, cudaMemcpyHostToDevice));
+  }
+
+  void qeq_reset() {
+    require_sys();
+    RXCU(cudaMemsetAsync(s_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
+    RXCU(cudaMemsetAsync(t_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
+    RXCU(cudaStreamSynchronize(stream));
   }
 
   void get_virial(double* out) {
@@ -1306,6 +1340,12 @@ int rx_set_velocities(rx_context* ctx, const double* v) { return guarded(ctx, [&
 int rx_get_velocities(rx_context* ctx, double* v) { return guarded(ctx, [&](rx::Context& c) { c.get_velocities(v); }); }
 int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature) {
   return guarded(ctx, [&](rx::Context& c) { c.md_run(nsteps, energies, temperature, 0); });
+}
+
+int rx_qeq_reset(rx_context* ctx) { return guarded(ctx, [&](rx::Context& c) { c.qeq_reset(); }); }
+
+int rx_set_acks2(rx_context* ctx, const double* s_kin) {
+  return guarded(ctx, [&](rx::Context& c) { c.set_acks2(s_kin); });
 }
 
 int rx_set_neighbor(rx_context* ctx, double skin) {

@@ -29,8 +29,9 @@ struct CgArgs {
   double2* d;
   double2* p;
   double2* q;
+  double2* w;      // A p (single-system CG)
   double* eta;
-  double* part;    // 2 * 4 * gridDim.x partial sums (double-buffered)
+  double* part;    // 2 * 8 * gridDim.x partial sums (double-buffered)
   int* out_iters;
   double* out_rel;
   int* out_nref;   // FP64 residual passes of the last single-system solve (may be null)
@@ -49,6 +50,7 @@ __global__ void k_nbr_check(Dev d);
 __global__ void k_neighbors(Dev d);
 __global__ void k_pairs(Dev d, DevFF ff, QeqParams qp);
 __global__ void k_nonbonded(Dev d, DevFF ff);
+__global__ void k_acks2(Dev d, DevFF ff, const double* s_kin);
 __global__ void k_cg_grid(Dev d, CgArgs a);
 __global__ void k_cg_seg(Dev d, CgArgs a);
 __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, const double* t_hist);

@@ -392,6 +392,75 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
   }
 }
 
+// ------------------------------------------------------------------------------------------------ ACKS2 pair terms
+// The pair side of the ACKS2 charge model (src/cpu/acks2.cpp:11-63), FP64, one warp per atom over its full row, with
+// the kinetic potentials s_kin of fix acks2/reaxff as input: the polarization coupling 23.02 q_i s_i, and over the
+// entries within xcut = (bcut_i + bcut_j)/2 the bond-softness Coulomb E = -23.02/2 bs (s_i - s_j)^2,
+// bs = softness d^3 (1 - d)^6, d = r / xcut (softness = gp[34]). The gradient of i takes every entry of its row; the
+// energy takes the owner-computes counted entries, as k_nonbonded. Adds to the non-bonded branch's arrays (the same
+// stream, after k_nonbonded).
+__global__ void k_acks2(Dev d, DevFF ff, const double* s_kin) {
+  if (lists_failed(d)) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= d.na) return;
+  const int i = warp;
+  const SysInfo s = d.sys[d.sys_of[i]];
+  const int ti = d.type[i];
+  const int cnt = min(d.nbr_cnt[i], d.ncap);
+  const double softness = ff.gp[34];
+  const double bcut_i = ff.sb[ti * SB_N + SB_BCUT_ACKS2], s_i = s_kin[i];
+  const long long tag_i = d.tag[i];
+  const int center = (d.S * d.S * d.S - 1) / 2;
+  double gx = 0, gy = 0, gz = 0, ee = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
+  for (int e = lane; e < cnt; e += 32) {
+    const unsigned code = d.nbr[static_cast<size_t>(i) * d.ncap + e];
+    const int j = static_cast<int>(code & d.amask);
+    const int sidx = static_cast<int>(code >> d.abits);
+    const double xcut = 0.5 * (bcut_i + ff.sb[d.type[j] * SB_N + SB_BCUT_ACKS2]);
+    double dv[3];
+    pair_dvec(d, s, i, j, sidx, dv);
+    const double dist = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+    if (!(dist <= xcut)) continue;
+    const double dd = dist / xcut, om = 1.0 - dd, om2 = om * om;
+    const double bs = softness * (dd * dd * dd) * (om2 * om2 * om2);
+    if (!(bs > 0.0)) continue;
+    const double effpot = s_i - s_kin[j];
+    double dbs = softness * 3.0 / xcut * (dd * dd) * (om2 * om2 * om) * (1.0 - 3.0 * dd);
+    dbs = 23.02 * (-0.5 * dbs * effpot * effpot) / dist;
+    gx -= dbs * dv[0]; gy -= dbs * dv[1]; gz -= dbs * dv[2];
+    const double c = -0.5 * dbs;
+    v0 += c * dv[0] * dv[0]; v1 += c * dv[1] * dv[1]; v2 += c * dv[2] * dv[2];
+    v3 += c * dv[0] * dv[1]; v4 += c * dv[0] * dv[2]; v5 += c * dv[1] * dv[2];
+    bool count = false;
+    if (sidx == center) count = j > i;
+    else {
+      const long long tag_j = d.tag[j];
+      if (tag_i < tag_j) count = true;
+      else if (tag_i == tag_j) {
+        const double SMALL = 1e-4;
+        if (dv[2] > SMALL) count = true;
+        else if (fabs(dv[2]) < SMALL) {
+          if (dv[1] > SMALL) count = true;
+          else if (fabs(dv[1]) < SMALL && dv[0] > SMALL) count = true;
+        }
+      }
+    }
+    if (count) ee += -0.5 * 23.02 * bs * effpot * effpot;
+  }
+  gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); ee = warp_sum(ee);
+  v0 = warp_sum(v0); v1 = warp_sum(v1); v2 = warp_sum(v2); v3 = warp_sum(v3); v4 = warp_sum(v4); v5 = warp_sum(v5);
+  if (lane == 0) {
+    double4 f = d.fnb[i];
+    f.x += gx; f.y += gy; f.z += gz;
+    d.fnb[i] = f;
+    d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] += ee;
+    d.eatom[static_cast<size_t>(i) * kTerms + E_POL] += 23.02 * d.q[i] * s_i;
+    double* vi = d.vir_nb + static_cast<size_t>(i) * kVir;
+    vi[0] += v0; vi[1] += v1; vi[2] += v2; vi[3] += v3; vi[4] += v4; vi[5] += v5;
+  }
+}
+
 // ------------------------------------------------------------------------------------------------ QEq CG
 // y = (diag(eta) + H) v for one row, both right-hand sides (s, t) at once; warp per row, each lane taking four
 // consecutive entries per pass with 16-byte loads (rows start 128-byte aligned: ncap is a multiple of 32). FULL: H as
@@ -477,8 +546,8 @@ constexpr double kRefineDrop = 1e-6;
 
 __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   cg::grid_group g = cg::this_grid();
-  __shared__ double sh[64 * 4];
-  __shared__ double tot_sh[64 * 4];
+  __shared__ double sh[32 * 8];
+  __shared__ double tot_sh[32 * 8];
   const int wpb = blockDim.x >> 5;
   const int gw = blockIdx.x * wpb + (threadIdx.x >> 5);
   const int nwarps = gridDim.x * wpb;
@@ -487,11 +556,12 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   double loc[4], tot[4];
   int phase = 0;
   auto partbuf = [&]() { return a.part + static_cast<size_t>(phase & 1) * gridDim.x * 4; };
+  auto partbuf8 = [&]() { return a.part + static_cast<size_t>(phase & 1) * gridDim.x * 8; };
   double bnorm_s = 0.0, bnorm_t = 0.0, sig_s = 0.0, sig_t = 0.0;
   bool act_s = true, act_t = true, breakdown = false;
   int it_s = 1, it_t = 1, nref = 0;
   for (;;) {
-    // ---- FP64 residual: r = b - A x ; d = M^-1 r ; r.d (and |b|^2 on the first pass)
+    // ---- FP64 residual: r = b - A x ; p = M^-1 r ; r.p (and |b|^2 on the first pass)
     loc[0] = loc[1] = loc[2] = loc[3] = 0.0;
     for (int r = gw; r < n; r += nwarps) {
       const int i = i0 + r;
@@ -501,9 +571,9 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
         const double2 b = a.b[i];
         const double2 rr = make_double2(b.x - y.x, b.y - y.y);
         a.r[i] = rr;
-        const double2 dd = make_double2(rr.x / eta, rr.y / eta);
-        a.d[i] = dd;
-        loc[0] += b.x * b.x; loc[1] += b.y * b.y; loc[2] += rr.x * dd.x; loc[3] += rr.y * dd.y;
+        const double2 pp = make_double2(rr.x / eta, rr.y / eta);
+        a.p[i] = pp;
+        loc[0] += b.x * b.x; loc[1] += b.y * b.y; loc[2] += rr.x * pp.x; loc[3] += rr.y * pp.y;
       }
     }
     block_partials<4>(loc, partbuf(), sh);
@@ -519,62 +589,72 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
     if ((!act_s || it_s >= a.imax) && (!act_t || it_t >= a.imax)) break;
     const double stop_s = fmax(a.tol * bnorm_s, kRefineDrop * sqrt(sig_s));
     const double stop_t = fmax(a.tol * bnorm_t, kRefineDrop * sqrt(sig_t));
-    // ---- single-precision-matrix iterations from this residual
+    // ---- single-precision-matrix iterations from this residual, two grid barriers each: the product is taken of
+    // the preconditioned residual p (w = A p) and A d follows from the recurrence q = w + beta q, with
+    // d.q = p.w + beta (p.q + d.w) + beta^2 d.q from four partial sums of the same pass
+    double beta_s = 0.0, beta_t = 0.0;
+    bool first = true;   // d and q hold nothing yet (d = p, q = w)
     for (;;) {
       const bool in_s = act_s && it_s < a.imax && sqrt(sig_s) > stop_s;
       const bool in_t = act_t && it_t < a.imax && sqrt(sig_t) > stop_t;
       if (!in_s && !in_t) break;
-      // q = A d ; partial d.q
-      loc[0] = loc[1] = 0.0;
+      // w = A p ; partial p.w, p.q, d.w, d.q (q, d of the previous iteration; unused while beta = 0)
+      double l8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       for (int r = gw; r < n; r += nwarps) {
         const int i = i0 + r;
-        const double2 y = row_mv<false>(d, i, a.eta[i], a.d);
+        const double2 w = row_mv<false>(d, i, a.eta[i], a.p);
         if (lane == 0) {
-          a.q[i] = y;
-          const double2 dd = a.d[i];
-          loc[0] += dd.x * y.x; loc[1] += dd.y * y.y;
+          a.w[i] = w;
+          const double2 pp = a.p[i];
+          l8[0] += pp.x * w.x; l8[1] += pp.y * w.y;
+          if (!first) {
+            const double2 qq = a.q[i], dd = a.d[i];
+            l8[2] += pp.x * qq.x; l8[3] += pp.y * qq.y;
+            l8[4] += dd.x * w.x; l8[5] += dd.y * w.y;
+            l8[6] += dd.x * qq.x; l8[7] += dd.y * qq.y;
+          }
         }
       }
-      block_partials<2>(loc, partbuf(), sh);
+      block_partials<8>(l8, partbuf8(), sh);
       g.sync();
-      grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
+      double t8[8];
+      grid_totals<8>(partbuf8(), gridDim.x, t8, tot_sh);
       ++phase;
-      const double alpha_s = in_s ? sig_s / tot[0] : 0.0;
-      const double alpha_t = in_t ? sig_t / tot[1] : 0.0;
+      const double dq_s = first ? t8[0] : t8[0] + beta_s * (t8[2] + t8[4]) + beta_s * beta_s * t8[6];
+      const double dq_t = first ? t8[1] : t8[1] + beta_t * (t8[3] + t8[5]) + beta_t * beta_t * t8[7];
+      const double alpha_s = in_s ? sig_s / dq_s : 0.0;
+      const double alpha_t = in_t ? sig_t / dq_t : 0.0;
       if (!(isfinite(alpha_s) && isfinite(alpha_t))) { breakdown = true; break; }
-      // x += alpha d ; r -= alpha q ; p = M^-1 r ; partial r.p
+      // d = p + beta d ; q = w + beta q ; x += alpha d ; r -= alpha q ; p = M^-1 r ; partial r.p
       loc[0] = loc[1] = 0.0;
       for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
         const int i = i0 + r;
-        const double2 dd = a.d[i], qq = a.q[i];
-        double2 xx = a.x[i], rr = a.r[i];
-        xx.x += alpha_s * dd.x; xx.y += alpha_t * dd.y;
-        rr.x -= alpha_s * qq.x; rr.y -= alpha_t * qq.y;
+        const double2 pp = a.p[i], ww = a.w[i];
+        double2 dd = first ? pp : a.d[i], qq = first ? ww : a.q[i], xx = a.x[i], rr = a.r[i];
+        if (in_s) {
+          if (!first) { dd.x = pp.x + beta_s * dd.x; qq.x = ww.x + beta_s * qq.x; }
+          xx.x += alpha_s * dd.x; rr.x -= alpha_s * qq.x;
+        }
+        if (in_t) {
+          if (!first) { dd.y = pp.y + beta_t * dd.y; qq.y = ww.y + beta_t * qq.y; }
+          xx.y += alpha_t * dd.y; rr.y -= alpha_t * qq.y;
+        }
+        a.d[i] = dd;
+        a.q[i] = qq;
         a.x[i] = xx;
         a.r[i] = rr;
         const double eta = a.eta[i];
-        const double2 pp = make_double2(rr.x / eta, rr.y / eta);
-        a.p[i] = pp;
-        loc[0] += rr.x * pp.x; loc[1] += rr.y * pp.y;
+        const double2 np = make_double2(in_s ? rr.x / eta : pp.x, in_t ? rr.y / eta : pp.y);
+        a.p[i] = np;
+        loc[0] += rr.x * np.x; loc[1] += rr.y * np.y;
       }
       block_partials<2>(loc, partbuf(), sh);
       g.sync();
       grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
       ++phase;
-      const double beta_s = in_s ? tot[0] / sig_s : 0.0;
-      const double beta_t = in_t ? tot[1] / sig_t : 0.0;
-      if (in_s) { sig_s = tot[0]; ++it_s; }
-      if (in_t) { sig_t = tot[1]; ++it_t; }
-      // d = p + beta d (only for the right-hand sides still iterating)
-      for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
-        const int i = i0 + r;
-        const double2 pp = a.p[i];
-        double2 dd = a.d[i];
-        if (in_s) dd.x = pp.x + beta_s * dd.x;
-        if (in_t) dd.y = pp.y + beta_t * dd.y;
-        a.d[i] = dd;
-      }
-      g.sync();
+      if (in_s) { beta_s = tot[0] / sig_s; sig_s = tot[0]; ++it_s; }
+      if (in_t) { beta_t = tot[1] / sig_t; sig_t = tot[1]; ++it_t; }
+      first = false;
     }
     if (breakdown) break;
   }

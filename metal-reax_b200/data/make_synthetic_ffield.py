@@ -146,7 +146,10 @@ OFFDIAG_LG = {(1, 2): 110.0, (1, 3): -1.0, (2, 3): 60.0}
 # src/io/ffield_parser.cpp:207-230): "vdw3" inner wall + shielding (the default), "vdw1" shielding only (no inner
 # wall: rcore2 = acore2 = 0), "vdw2" inner wall only (gamma_w <= 0.5), "lg" the default with lgvdw data (read with
 # `lgvdw yes`; gp[35] = 0.5 so that lgre = sqrt(lgre_i lgre_j))
-VARIANTS = ("vdw3", "vdw1", "vdw2", "lg")
+# "acks2": the default with ACKS2 bond-softness cut-offs on the atom lines (bcut_acks2, line 3 column 7) and the
+# softness gp[34] = 2.0, for the pair side of the ACKS2 charge model
+ACKS2_BCUT = {"C": 5.5, "H": 4.5, "O": 5.0}
+VARIANTS = ("vdw3", "vdw1", "vdw2", "lg", "acks2")
 
 
 def render(variant="vdw3"):
@@ -162,6 +165,10 @@ def render(variant="vdw3"):
             a[2][1] = 0.4
     elif variant == "lg":
         general[35] = 0.5
+    elif variant == "acks2":
+        general[34] = 2.0
+        for a in atoms:
+            a[3][6] = ACKS2_BCUT[a[0]]
     title = "Synthetic C/H/O ReaxFF parameter set (not the published CHO file; see make_synthetic_ffield.py)"
     out = [title if variant == "vdw3" else title + " variant " + variant]
     out.append(f"{len(general):3d}       ! Number of general parameters")

@@ -31,7 +31,7 @@ EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
-           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg"]
+           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -70,7 +70,7 @@ def load():
         "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
         "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
-        "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]),
+        "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]), "rx_set_acks2": (_I, [_V, _V]), "rx_qeq_reset": (_I, [_V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -190,6 +190,12 @@ class Engine:
             out["counts"] = cnt
         return out
 
+    def set_acks2(self, s_kin):
+        """Kinetic potentials of fix acks2/reaxff (one per atom), or None to switch the ACKS2 pair terms off."""
+        sk = None if s_kin is None else np.ascontiguousarray(s_kin, dtype=np.float64)
+        self._check(self.lib.rx_set_acks2(self.h, _p(sk)))
+        self._s_kin = sk
+
     def virial(self):
         """LAMMPS-order virial (xx, yy, zz, xy, xz, yz) of the last force evaluation, per system."""
         v = np.zeros(6 * self.nsys)
@@ -201,6 +207,10 @@ class Engine:
         rel = np.zeros(2 * self.nsys)
         self._check(self.lib.rx_qeq_solve(self.h, _p(it), _p(rel)))
         return {"q": self.get_charges(), "iters": it.reshape(-1, 2), "rel": rel.reshape(-1, 2)}
+
+    def qeq_reset(self):
+        """Zero the charge histories: the next solve starts cold."""
+        self._check(self.lib.rx_qeq_reset(self.h))
 
     def qeq_cg(self, b, x0=None):
         """Both CG systems for given right-hand sides b (2, NA) and guesses x0 (2, NA) (mtl::Context::qeq_solve)."""

@@ -14,7 +14,7 @@ import numpy as np
 
 SB_FIELDS = ["r_s", "valency", "mass", "r_vdw", "epsilon", "gamma", "r_pi", "valency_e", "nlp_opt", "alpha", "gamma_w",
              "valency_boc", "p_ovun5", "chi", "eta", "p_hbond", "r_pi_pi", "p_lp2", "b_o_131", "b_o_132", "b_o_133",
-             "p_ovun2", "p_val3", "valency_val", "p_val5", "rcore2", "ecore2", "acore2", "heavy", "c2species"]
+             "p_ovun2", "p_val3", "valency_val", "p_val5", "rcore2", "ecore2", "acore2", "heavy", "c2species", "bcut_acks2"]
 TB_FIELDS = ["p_bo1", "p_bo2", "p_bo3", "p_bo4", "p_bo5", "p_bo6", "r_s", "r_p", "r_pp", "p_boc3", "p_boc4", "p_boc5",
              "p_be1", "p_be2", "De_s", "De_p", "De_pp", "p_ovun1", "D", "alpha", "r_vdW", "gamma_w", "rcore", "ecore",
              "acore", "lgcij", "lgre", "gamma", "v13cor", "ovc", "triple_stab"]

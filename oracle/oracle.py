@@ -86,18 +86,23 @@ class COracle:
                       _ptr(a["thb"]), _ptr(a["fbp_on"]), _ptr(a["fbp"]), _ptr(a["hbp_on"]), _ptr(a["hbp"]), 1 if lgvdw else 0)
         self.ctl = _Ctl(bond_cut, hbond_cut, thb_cut, thb_cutsq, 1 if enobonds else 0, shell)
         self.lib.rxo_single_point.argtypes = [_V, _V, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V, _V, ctypes.c_char_p, _I]
+        self.lib.rxo_single_point_acks2.argtypes = [_V, _V, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V, _V, _V, ctypes.c_char_p,
+                                                    _I]
         self.lib.rxo_qeq.argtypes = [_V, _V, _V, _I, _V, _V, _V, _D, _D, _D, _I, _V, _V, _V, _V, _V, _V, _V, ctypes.c_char_p, _I]
         self.lib.rxo_qeq_matvec.argtypes = [_V, _V, _V, _I, _V, _V, _V, _D, _D, _V, _V, ctypes.c_char_p, _I]
 
     def chi(self, types):
         return np.array([self.tables["sbp"][t]["chi"] for t in types])
 
-    def single_point(self, system, q=None):
+    def single_point(self, system, q=None, s_kin=None):
+        """Energies, gradient, census, counts and virial; with s_kin (the ACKS2 kinetic potentials, one per atom) the
+        pair side of the ACKS2 charge model is added."""
         n = len(system["type"])
         x = np.ascontiguousarray(system["x"], dtype=np.float64)
         ty = np.ascontiguousarray(system["type"], dtype=np.int32)
         tg = np.ascontiguousarray(system["tag"], dtype=np.int64)
         qq = None if q is None else np.ascontiguousarray(q, dtype=np.float64)
+        sk = None if s_kin is None else np.ascontiguousarray(s_kin, dtype=np.float64)
         e = np.zeros(13)
         g = np.zeros(3 * n)
         cen = np.zeros(7 * n, dtype=np.int32)
@@ -105,8 +110,9 @@ class COracle:
         vir = np.zeros(6)
         err = ctypes.create_string_buffer(512)
         box = _box_struct(system)
-        rc = self.lib.rxo_single_point(ctypes.byref(self.ff), ctypes.byref(self.ctl), ctypes.byref(box), n, _ptr(x), _ptr(ty),
-                                       _ptr(tg), _ptr(qq), _ptr(e), _ptr(g), _ptr(cen), _ptr(cnt), _ptr(vir), err, 512)
+        rc = self.lib.rxo_single_point_acks2(ctypes.byref(self.ff), ctypes.byref(self.ctl), ctypes.byref(box), n, _ptr(x),
+                                             _ptr(ty), _ptr(tg), _ptr(qq), _ptr(sk), _ptr(e), _ptr(g), _ptr(cen), _ptr(cnt),
+                                             _ptr(vir), err, 512)
         if rc:
             raise RuntimeError("oracle: " + err.value.decode())
         return {"e": e, "grad": g.reshape(n, 3), "census": cen.reshape(7, n), "counts": cnt, "virial": vir}
@@ -160,7 +166,7 @@ class RefOracle:
         self.bond_cut, self.hbond_cut, self.enobonds, self.shell = bond_cut, hbond_cut, enobonds, shell
         self.lgvdw = lgvdw
         self.lib.ref_single_point.argtypes = [ctypes.c_char_p, _V, _V, _V, _I, _V, _V, _V, _V, _D, _D, _D, _I, _I, _V, _V, _V,
-                                              _V, _V, ctypes.c_char_p, _I]
+                                              _V, _V, _V, ctypes.c_char_p, _I]
         self.lib.ref_table_dump.argtypes = [ctypes.c_char_p, _I, ctypes.c_char_p, ctypes.c_long]
         self.lib.ref_table_dump.restype = ctypes.c_long
 
@@ -171,11 +177,12 @@ class RefOracle:
             raise RuntimeError(buf.value.decode())
         return buf.value.decode()
 
-    def single_point(self, system, q=None):
+    def single_point(self, system, q=None, s_kin=None):
         n = len(system["type"])
         x = np.ascontiguousarray(system["x"], dtype=np.float64)
         ty = np.ascontiguousarray(system["type"], dtype=np.int32)
         tg = np.ascontiguousarray(system["tag"], dtype=np.int64)
+        sk = None if s_kin is None else np.ascontiguousarray(s_kin, dtype=np.float64)
         org = np.ascontiguousarray(system["origin"], dtype=np.float64)
         box = np.ascontiguousarray(system["box"], dtype=np.float64)
         per = np.ascontiguousarray(system["periodic"], dtype=np.int32)
@@ -188,7 +195,7 @@ class RefOracle:
         err = ctypes.create_string_buffer(512)
         rc = self.lib.ref_single_point(self.text, _ptr(org), _ptr(box), _ptr(per), n, _ptr(x), _ptr(ty), _ptr(tg), _ptr(qq),
                                        self.bond_cut, self.hbond_cut, self.shell, 1 if self.enobonds else 0,
-                                       1 if self.lgvdw else 0, _ptr(e), _ptr(g),
+                                       1 if self.lgvdw else 0, _ptr(sk), _ptr(e), _ptr(g),
                                        _ptr(cen), _ptr(cnt), _ptr(vir), err, 512)
         if rc:
             raise RuntimeError("reference: " + err.value.decode())

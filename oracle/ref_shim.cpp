@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "reaxmetal/acks2.hpp"
 #include "reaxmetal/bonded.hpp"
 #include "reaxmetal/forcefield.hpp"
 #include "reaxmetal/neighbor.hpp"
@@ -51,6 +52,7 @@ long ref_table_dump(const char* ffield_text, int portable, char* out, long outle
 //   box9: lattice vectors a, b, c (row-major); origin3; periodic3 (0/1)
 //   x: 3n owned coordinates, type: n force-field type indices (0-based), tag: n atom ids
 //   lgvdw: 1 reads and evaluates the force field as `pair_style reaxff lgvdw yes`
+//   s_kin: NULL, or n kinetic potentials of fix acks2/reaxff (its s[N + i]): the ACKS2 pair terms are added
 //   q: n charges or NULL (NULL: the non-bonded terms are skipped, as energy_tool does without charges)
 //   e13: energies in EnergyTerm order (bond, over, under, lone_pair, valence, penalty, coalition, hbond,
 //        torsion, conjugation, vdw, coulomb, polarization), kcal/mol
@@ -62,8 +64,8 @@ long ref_table_dump(const char* ffield_text, int portable, char* out, long outle
 //            order xx, yy, zz, xy, xz, yz, f = -grad
 int ref_single_point(const char* ffield_text, const double* origin3, const double* box9, const int* periodic3, int n,
                      const double* x, const int* type, const long long* tag, const double* q, double bond_cut,
-                     double hbond_cut, double shell, int enobonds, int lgvdw, double* e13, double* grad, int* census,
-                     long long* counts, double* virial6, char* err, int errlen) {
+                     double hbond_cut, double shell, int enobonds, int lgvdw, const double* s_kin, double* e13,
+                     double* grad, int* census, long long* counts, double* virial6, char* err, int errlen) {
   try {
     FfieldOptions fo;
     fo.lgvdw = lgvdw != 0;
@@ -99,6 +101,11 @@ int ref_single_point(const char* ffield_text, const double* origin3, const doubl
       no.lgvdw = lgvdw != 0;
       std::vector<double> qv(q, q + n);
       nb = compute_nonbonded_core(ff, cut, a, f, qv, no);
+      if (s_kin) {   // the pair side of fix acks2/reaxff, as pair_reaxff_metal.cpp:492 adds it for cpu64
+        std::vector<double> sk(a.nall());
+        for (std::size_t i = 0; i < a.nall(); ++i) sk[i] = s_kin[a.owner[i]];
+        add_acks2_terms(ff, cut, a, f, qv, sk.data(), nb);
+      }
     }
     for (std::size_t t = 0; t < kEnergyTermCount; ++t) e13[t] = r.e.e[t] + nb.e.e[t];
     std::vector<double> g(3 * static_cast<std::size_t>(n), 0.0);

@@ -1196,9 +1196,57 @@ static int setup(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, int n
   return 0;
 }
 
+/* The pair-side ACKS2 terms (src/cpu/acks2.cpp:11-63): the polarization coupling 23.02 q_i s_i per owned atom, and
+ * the bond-softness Coulomb over the counted far-list pairs within xcut = (bcut_i + bcut_j)/2,
+ * E = -23.02/2 bs (s_i - s_j)^2, bs = softness d^3 (1 - d)^6, d = r / xcut, softness = gp[34]. */
+static void acks2_terms(const rxo_ff* ff, const atomset* a, const farlist* far, const double* q, const double* s_kin,
+                        double* e13, double* f) {
+  const int n = a->nlocal;
+  const double softness = ff->ngp > 34 ? ff->gp[34] : 0.0;
+  double e_ele = 0.0, e_pol = 0.0;
+  for (int i = 0; i < n; ++i) {
+    if (a->type[i] < 0) continue;
+    e_pol += KCAL_TO_EV * q[i] * s_kin[i];
+  }
+  for (int i = 0; i < n; ++i) {
+    const int ti = a->type[i];
+    if (ti < 0) continue;
+    for (long long pj = far->row_start[i]; pj < far->row_start[i + 1]; ++pj) {
+      const int j = far->nbr[pj];
+      const int tj = a->type[j];
+      if (tj < 0) continue;
+      const double xcut = 0.5 * (SB(ti, SB_BCUT_ACKS2) + SB(tj, SB_BCUT_ACKS2));
+      const double dist = far->dist[pj];
+      if (!(dist <= xcut)) continue;
+      const double* dv = far->dvec + 3 * pj;
+      if (classify(j, n, a->tag[i], a->tag[j], dv) == 0) continue;
+      const double d = dist / xcut;
+      const double bs = softness * pow(d, 3.0) * pow(1.0 - d, 6.0);
+      if (!(bs > 0.0)) continue;
+      const double effpot = s_kin[i] - s_kin[a->owner[j]];
+      e_ele += -0.5 * KCAL_TO_EV * bs * effpot * effpot;
+      double dbs = softness * 3.0 / xcut * pow(d, 2.0) * pow(1.0 - d, 5.0) * (1.0 - 3.0 * d);
+      dbs = -0.5 * dbs * effpot * effpot;
+      dbs = KCAL_TO_EV * dbs / dist;
+      for (int c = 0; c < 3; ++c) {
+        f[3 * i + c] += -dbs * dv[c];
+        f[3 * j + c] += +dbs * dv[c];
+      }
+    }
+  }
+  e13[11] += e_ele;
+  e13[12] += e_pol;
+}
+
 int rxo_single_point(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, int n, const double* x, const int* type,
                      const long long* tag, const double* q, double* e13, double* grad, int* census, long long* counts,
                      double* virial6, char* err, int errlen) {
+  return rxo_single_point_acks2(ff, ctl, box, n, x, type, tag, q, NULL, e13, grad, census, counts, virial6, err, errlen);
+}
+
+int rxo_single_point_acks2(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, int n, const double* x,
+                           const int* type, const long long* tag, const double* q, const double* s_kin, double* e13,
+                           double* grad, int* census, long long* counts, double* virial6, char* err, int errlen) {
   atomset a;
   farlist far;
   int rc = setup(ff, ctl, box, n, x, type, tag, &a, &far, err, errlen);
@@ -1210,6 +1258,7 @@ int rxo_single_point(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, i
   long long nbonds = 0, npairs = 0;
   rc = bonded_core(ff, ctl, &a, &far, e13, f, census, &nbonds, err, errlen);
   if (!rc && q) nonbonded_core(ff, &a, &far, q, e13, f, census, &npairs);
+  if (!rc && q && s_kin) acks2_terms(ff, &a, &far, q, s_kin, e13, f);
   if (!rc) {
     memset(grad, 0, sizeof(double) * 3 * (size_t)n);
     for (int i = 0; i < N; ++i)

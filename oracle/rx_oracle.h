@@ -21,7 +21,7 @@ enum {
   SB_ALPHA, SB_GAMMA_W, SB_VALENCY_BOC, SB_P_OVUN5, SB_CHI, SB_ETA, SB_P_HBOND,
   SB_R_PI_PI, SB_P_LP2, SB_B_O_131, SB_B_O_132, SB_B_O_133,
   SB_P_OVUN2, SB_P_VAL3, SB_VALENCY_VAL, SB_P_VAL5, SB_RCORE2, SB_ECORE2, SB_ACORE2,
-  SB_HEAVY, SB_C2SPECIES, SB_NFIELDS
+  SB_HEAVY, SB_C2SPECIES, SB_BCUT_ACKS2, SB_NFIELDS
 };
 
 /* per-pair ("two body") fields, symmetric n x n */
@@ -81,6 +81,12 @@ typedef struct {
 int rxo_single_point(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, int n, const double* x, const int* type,
                      const long long* tag, const double* q, double* e13, double* grad, int* census, long long* counts,
                      double* virial6, char* err, int errlen);
+
+/* The same single point with the pair-side terms of the ACKS2 charge model added (src/cpu/acks2.cpp:11-63): s_kin[n]
+ * the kinetic potentials of the owned atoms (an image takes its owner's). NULL s_kin is rxo_single_point. */
+int rxo_single_point_acks2(const rxo_ff* ff, const rxo_ctl* ctl, const rxo_box* box, int n, const double* x,
+                           const int* type, const long long* tag, const double* q, const double* s_kin, double* e13,
+                           double* grad, int* census, long long* counts, double* virial6, char* err, int errlen);
 
 /* Charge equilibration: solves H s = -chi and H t = -1 with the stock Jacobi-preconditioned CG (tolerance
  * sqrt(r.M^-1 r)/|b| <= tol, at most imax - 1 iterations) from the initial guesses s0/t0 (n each), then

@@ -39,3 +39,8 @@ def small_systems():
 def force_metrics(g_ref, g):
     d = np.asarray(g) - np.asarray(g_ref)
     return float(np.abs(d).max()), float(np.sqrt((d ** 2).sum(axis=1).mean()))
+
+
+def acks2_potentials(n, seed=17):
+    """Seeded stand-ins for the kinetic potentials of fix acks2/reaxff (its s[N + i]), one per atom."""
+    return np.random.default_rng(seed).normal(scale=0.5, size=n)

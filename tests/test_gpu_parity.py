@@ -98,6 +98,7 @@ def test_qeq_charges_match_oracle(engine, oracle):
 def test_qeq_tol_1e6_within_c3(engine, oracle):
     s = small_systems()[0]
     engine.set_systems([s])
+    engine.qeq_reset()
     engine.set_qeq(0.0, 10.0, 1e-6, 200)
     got = engine.qeq_solve()
     ref = oracle.qeq(s, tol=1e-6, imax=200)
@@ -140,11 +141,13 @@ def test_batched_charges_equal_alone_and_oracle(engine, oracle):
     ss = [systems.random_cho(k) for k in (0, 4, 9, 21, 33, 40)]
     engine.set_qeq(0.0, 10.0, 1e-12, 400)
     engine.set_systems(ss)
+    engine.qeq_reset()
     both = engine.qeq_solve()
     off = 0
     for k, s in enumerate(ss):
         n = len(s["type"])
         engine.set_systems([s])
+        engine.qeq_reset()
         alone = engine.qeq_solve()
         assert np.array_equal(alone["q"], both["q"][off:off + n]), s["name"]
         assert np.array_equal(alone["iters"][0], both["iters"][k])
@@ -392,3 +395,40 @@ def test_set_systems_keeps_charge_history_by_tag(engine):
     cold = engine.qeq_last()["iters"].max()
     assert after <= warm + 1 and after < cold, (warm, after, cold)
     engine.set_qeq()
+
+
+def test_acks2_pair_terms_match_oracle():
+    """The pair side of fix acks2/reaxff (src/cpu/acks2.cpp:11-63) through rx_set_acks2: with kinetic potentials set,
+    the Coulomb and polarization energies, forces and virial match the oracle's under the same bars as the
+    single-point test; switched off again, the plain evaluation returns."""
+    import make_synthetic_ffield
+    import rxcuda
+    import systems
+    from helpers import acks2_potentials
+    from oracle.oracle import COracle
+    text = make_synthetic_ffield.render("acks2")
+    orc = COracle(text, shell=15.0)
+    eng = rxcuda.Engine(0)
+    eng.set_forcefield(text)
+    eng.set_control()
+    for s in (systems.water_box(4), systems.random_cho(7)):
+        n = len(s["type"])
+        q = fixed_charges(s)
+        sk = acks2_potentials(n)
+        ref = orc.single_point(s, q, s_kin=sk)
+        plain = orc.single_point(s, q)
+        eng.set_systems([s])
+        eng.set_charges(q)
+        eng.set_acks2(sk)
+        out = eng.compute(census=True)
+        e = out["e"][0]
+        assert abs(e[12] - ref["e"][12]) <= 1e-9 * max(1.0, abs(ref["e"][12])), s["name"]
+        assert abs(e[11] - ref["e"][11]) <= 1e-5 * max(1.0, abs(ref["e"][11])), s["name"]
+        assert abs(e.sum() - ref["e"].sum()) / n <= C3_ENERGY_PER_ATOM
+        fmax, frms = force_metrics(ref["grad"], out["grad"])
+        assert fmax <= C3_FORCE_MAX and frms <= C3_FORCE_RMS, (s["name"], fmax, frms)
+        assert np.abs(eng.virial()[0] - ref["virial"]).max() / n <= C3_ENERGY_PER_ATOM
+        eng.set_acks2(None)
+        off = eng.compute()
+        assert abs(off["e"][0][12] - plain["e"][12]) <= 1e-9 * max(1.0, abs(plain["e"][12]))
+    eng.close()

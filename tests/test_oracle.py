@@ -36,17 +36,18 @@ def test_python_reader_matches_reference_dump():
 
 
 @pytest.mark.parametrize("name", ["water192", "cho3_108", "cho7_78", "cho11_141", "carbon200",
-                                  "water192_vdw1", "water192_vdw2", "water192_lg"])
+                                  "water192_vdw1", "water192_vdw2", "water192_lg", "water192_acks2"])
 def test_oracle_matches_golden(name):
     """The C restatement against the reference's own outputs (energies, gradient, census, counts and the fdotr
-    virial), including the force-field variants that switch the non-bonded branches (vdW types 1 and 2, lgvdw)."""
+    virial), including the force-field variants that switch the non-bonded branches (vdW types 1 and 2, lgvdw) and the
+    pair side of the ACKS2 charge model."""
     from oracle.oracle import COracle
     import make_synthetic_ffield
     s, z = _golden_system(GOLDEN / (name + ".npz"))
     variant = name.rsplit("_", 1)[-1]
     variant = variant if variant in make_synthetic_ffield.VARIANTS else "vdw3"
     orc = COracle(make_synthetic_ffield.render(variant), shell=15.0, lgvdw=(variant == "lg"))
-    r = orc.single_point(s, z["q"])
+    r = orc.single_point(s, z["q"], s_kin=z["s_kin"] if "s_kin" in z.files else None)
     assert np.array_equal(r["census"], z["census"])
     assert np.array_equal(r["counts"], z["counts"])
     assert np.abs(r["e"] - z["e"]).max() <= 1e-9 * max(1.0, np.abs(z["e"]).max())
