@@ -125,6 +125,9 @@ int rx_compute(rx_context* ctx, int flags, double* energies, double* grad, int32
  * the forces and the virial. rx_set_systems switches them off. */
 int rx_set_acks2(rx_context* ctx, const double* s_kin);
 
+/* Gradient dE/dx[3*NA] of the most recent force evaluation (rx_compute or the last step of rx_md_run). */
+int rx_get_gradient(rx_context* ctx, double* grad);
+
 /* Virial of the most recent force evaluation (rx_compute or the last rx_md_run step) per system: virial[6*nsys] in
  * LAMMPS's order xx, yy, zz, xy, xz, yz, the sum of x_a f_b over every atom and periodic image (kcal/mol) - what
  * virial_fdotr_compute() makes of the owned + ghost forces the reference's pair style hands LAMMPS
@@ -167,6 +170,21 @@ int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature
 int rx_qeq_solve_static(int n, const int* row_start, const int* col, const double* val, const double* eta, const double* chi,
                         double* s, double* t, double* q, double tol, int imax, int* iters, double* rel, void* stream,
                         char* err, int errlen);
+
+/* Serving (continuous batching). rx_update_systems replaces the context's systems by nkeep of the current ones
+ * (keep[k] = current system index, in their new order) followed by nnew new systems described as for rx_set_systems
+ * (natoms[nnew], origin[3*nnew], box[9*nnew], periodic[3*nnew] or NULL, type/tag for the new atoms), with positions
+ * x[3*NA_new] and velocities v[3*NA_new] (NULL = 0) of the new atoms. Kept systems carry their positions, velocities,
+ * charges, charge histories and chain state on the device; every system's neighbor rows are rebuilt at the next
+ * evaluation, and the next rx_md_run starts with a force evaluation. Per-system targets set by rx_md_targets are
+ * cleared. No counterpart in the reference (its systems live in LAMMPS). */
+int rx_update_systems(rx_context* ctx, int nkeep, const int* keep, int nnew, const int* natoms, const double* origin,
+                      const double* box, const int* periodic, const int* type, const int64_t* tag, const double* x,
+                      const double* v);
+/* Per-system NVT settings for serving: t_target[nsys] target temperatures in K (NULL: the common ramp of
+ * rx_md_setup) and active[nsys] (NULL: all; 0 freezes a system: its atoms and its chain are not advanced, its
+ * forces are still evaluated). */
+int rx_md_targets(rx_context* ctx, const double* t_target, const int* active);
 
 /* Number of this engine's own kernels launched on the context so far (library kernels, e.g. the radix sort of the cell
  * lists, are not counted). */

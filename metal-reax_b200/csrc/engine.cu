@@ -105,6 +105,7 @@ struct Context {
   std::vector<SysInfo> hsys;
   std::vector<int> hsys_of;
   std::vector<long long> htag;
+  std::vector<int> htype;
   DBuf<SysInfo> sys;
   DBuf<int> sys_of, type, cell_key, cell_key_sorted, cell_atoms, atom_iota, cell_start, sys_flag;
   DBuf<double4> xs;
@@ -128,6 +129,7 @@ struct Context {
   // atoms
   DBuf<double> Deltap, Deltap_boc, cdtot, W, eatom;
   DBuf<double4> dDp_self, fown, fdb, fnb, grad, fown_h, fown_t;
+  DBuf<unsigned long long> fix_h;
   DBuf<AtomQ> aq;
   DBuf<int> census, status;
   DBuf<long long> counters;
@@ -391,6 +393,7 @@ struct Context {
     s_hist.ensure(4 * static_cast<size_t>(na));
     t_hist.ensure(4 * static_cast<size_t>(na));
     htag.assign(tags, tags + na);
+    htype.assign(types, types + na);
     {
       std::vector<double> sh(4 * static_cast<size_t>(na), 0.0), th(4 * static_cast<size_t>(na), 0.0);
       if (!old_sh.empty()) {
@@ -421,6 +424,7 @@ struct Context {
     }
     have_pos = false;
     have_virial = false;
+    forces_valid = false;
     acks2_on = false;
     md_ready = false;
     ncap = 0;
@@ -542,7 +546,7 @@ struct Context {
     virial.ensure(static_cast<size_t>(nsys) * kVir);
     vir.ensure(n * kVir);
     vir_nb.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
-    fown_h.ensure(n); fown_t.ensure(n);
+    fown_h.ensure(n); fown_t.ensure(n); fix_h.ensure(3 * n);
     cg_x.ensure(n); cg_w.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
     cg_sys.ensure(nsys); cg_rb0.ensure(n); cg_rb1.ensure(n); cg_nlive.ensure(2);
@@ -583,7 +587,7 @@ struct Context {
     d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p;
     d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
     d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.vir_nb = vir_nb.p; d.vir_h = vir_h.p; d.vir_t = vir_t.p;
-    d.fown_h = fown_h.p; d.fown_t = fown_t.p; d.bcdbo_h = bcdbo_h.p; d.bfn_h = bfn_h.p; d.bacc_t = bacc_t.p; d.bfn_t = bfn_t.p; d.census = census.p; d.status = status.p;
+    d.fown_h = fown_h.p; d.fown_t = fown_t.p; d.fix_h = fix_h.p; d.bcdbo_h = bcdbo_h.p; d.bfn_h = bfn_h.p; d.bacc_t = bacc_t.p; d.bfn_t = bfn_t.p; d.census = census.p; d.status = status.p;
     d.counters = counters.p;
     return d;
   }
@@ -714,10 +718,9 @@ struct Context {
       RXCU(cudaStreamWaitEvent(side_t, ev_fork2, 0));
     }
     tic(3, "bonded_terms");
-    launches += 3;
+    launches += 2;
     k_bonded_atom<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
     k_hbond<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, hs>>>(d, dff, ctl);
-    k_hbond_acceptor<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, hs>>>(d, dff, ctl);
     toc(3);
     tic(4, "torsion");
     ++launches;
@@ -799,6 +802,7 @@ struct Context {
       check_status(st, do_qeq);
       break;
     }
+    forces_valid = true;
     collect_times();
   }
 
@@ -811,6 +815,7 @@ struct Context {
   }
 
   bool have_virial = false;
+  bool forces_valid = false;   // the gradient buffer holds the forces of the current positions and systems
   void energy_sums() {
     have_virial = true;
     ++launches;
@@ -826,6 +831,7 @@ struct Context {
     force_rebuild();
     RXCU(cudaStreamSynchronize(stream));
     have_pos = true;
+    forces_valid = false;
   }
   void get_positions(double* xout) {
     require_sys();
@@ -890,6 +896,15 @@ struct Context {
     RXCU(cudaMemsetAsync(s_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
     RXCU(cudaMemsetAsync(t_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
     RXCU(cudaStreamSynchronize(stream));
+  }
+
+  void get_gradient(double* g_out) {
+    require_sys();
+    if (!have_virial) throw Error(RX_ERR_STATE, "no force evaluation yet");
+    double4* g = stage(static_cast<size_t>(na));
+    RXCU(cudaMemcpyAsync(g, grad.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, stream));
+    RXCU(cudaStreamSynchronize(stream));
+    for (int a = 0; a < na; ++a) { g_out[3 * a] = g[a].x; g_out[3 * a + 1] = g[a].y; g_out[3 * a + 2] = g[a].z; }
   }
 
   void get_virial(double* out) {
@@ -1005,11 +1020,18 @@ struct Context {
     mass.ensure(static_cast<size_t>(ff.nt));
     RXCU(cudaMemcpy(mass.p, mass_in, sizeof(double) * ff.nt, cudaMemcpyHostToDevice));
     v.ensure(static_cast<size_t>(na));
-    ke.ensure(static_cast<size_t>(nsys)); temp.ensure(static_cast<size_t>(nsys)); scale.ensure(static_cast<size_t>(nsys));
-    xi.ensure(static_cast<size_t>(nsys) * kMaxChain); vxi.ensure(static_cast<size_t>(nsys) * kMaxChain);
+    md_layout(dt, t0, t1, tdamp, chain);
     RXCU(cudaMemset(xi.p, 0, sizeof(double) * nsys * kMaxChain));
     RXCU(cudaMemset(vxi.p, 0, sizeof(double) * nsys * kMaxChain));
     RXCU(cudaMemset(v.p, 0, sizeof(double4) * na));
+    md_step = 0;
+  }
+
+  // the per-system integrator arrays of the current systems (velocities and chain state are left to the caller)
+  void md_layout(double dt, double t0, double t1, double tdamp, int chain) {
+    v.ensure(static_cast<size_t>(na));
+    ke.ensure(static_cast<size_t>(nsys)); temp.ensure(static_cast<size_t>(nsys)); scale.ensure(static_cast<size_t>(nsys));
+    xi.ensure(static_cast<size_t>(nsys) * kMaxChain); vxi.ensure(static_cast<size_t>(nsys) * kMaxChain);
     std::vector<int> first(static_cast<size_t>(nsys) + 1, 0), csys;
     for (int s = 0; s < nsys; ++s) {
       const int nc = (hsys[s].natoms + kKeChunk - 1) / kKeChunk;
@@ -1022,10 +1044,157 @@ struct Context {
     if (nchunks > 0) RXCU(cudaMemcpy(ksys.p, csys.data(), sizeof(int) * csys.size(), cudaMemcpyHostToDevice));
     ramp.ensure(2);
     RXCU(cudaMemset(ramp.p, 0, sizeof(double) * 2));
-    md = MdDev{v.p, mass.p, ke.p, temp.p, scale.p, xi.p, vxi.p, dt, t0, t1, tdamp, chain, kpart.p, kfirst.p, ksys.p, nchunks, ramp.p};
+    md = MdDev{v.p, mass.p, ke.p, temp.p, scale.p, xi.p, vxi.p, dt, t0, t1, tdamp, chain, kpart.p, kfirst.p, ksys.p, nchunks, ramp.p,
+               nullptr, nullptr};
     md_ready = true;
-    md_step = 0;
     drop_graph();
+  }
+
+  // Continuous batching: the systems become `nkeep` of the current ones (keep[k] = current index, in their new order)
+  // followed by `nnew` new ones. Kept systems carry their positions, velocities, charges, charge histories and chain
+  // state; new systems take x_new / v_new. Every system's rows are rebuilt at the next evaluation.
+  void update_systems(int nkeep, const int* keep, int nnew, const int* natoms, const double* origin, const double* box,
+                      const int* periodic, const int* types, const int64_t* tags, const double* x_new, const double* v_new) {
+    require_ff();
+    if (host_only) throw Error(RX_ERR_STATE, "host-only context (created with device < 0)");
+    if (nkeep < 0 || nnew < 0 || nkeep + nnew <= 0) throw Error(RX_ERR_INVALID, "update_systems: no systems");
+    if (nkeep > 0 && (!keep || nsys == 0)) throw Error(RX_ERR_INVALID, "update_systems: nothing to keep");
+    if (nnew > 0 && (!natoms || !origin || !box || !types || !tags || !x_new)) throw Error(RX_ERR_INVALID, "update_systems: null input");
+    std::vector<char> seen(static_cast<size_t>(nsys), 0);
+    for (int k = 0; k < nkeep; ++k) {
+      if (keep[k] < 0 || keep[k] >= nsys || seen[static_cast<size_t>(keep[k])]) throw Error(RX_ERR_INVALID, "update_systems: bad keep list");
+      seen[static_cast<size_t>(keep[k])] = 1;
+    }
+    const int ns = nkeep + nnew;
+    std::vector<int> nat(static_cast<size_t>(ns)), per(3 * static_cast<size_t>(ns), 1), ty;
+    std::vector<double> org(3 * static_cast<size_t>(ns)), bx(9 * static_cast<size_t>(ns));
+    std::vector<int64_t> tg;
+    std::vector<int> src;   // new atom -> old atom (kept systems)
+    for (int k = 0; k < nkeep; ++k) {
+      const SysInfo& o = hsys[static_cast<size_t>(keep[k])];
+      nat[static_cast<size_t>(k)] = o.natoms;
+      for (int c = 0; c < 3; ++c) org[3 * k + c] = o.origin[c];
+      for (int c = 0; c < 9; ++c) bx[9 * k + c] = o.L[c];
+      for (int a = 0; a < o.natoms; ++a) {
+        src.push_back(o.begin + a);
+        ty.push_back(htype[static_cast<size_t>(o.begin + a)]);
+        tg.push_back(htag[static_cast<size_t>(o.begin + a)]);
+      }
+    }
+    const size_t nkept_atoms = src.size();
+    long long nadd = 0;
+    for (int k = 0; k < nnew; ++k) {
+      nat[static_cast<size_t>(nkeep + k)] = natoms[k];
+      for (int c = 0; c < 3; ++c) org[3 * (nkeep + k) + c] = origin[3 * k + c];
+      for (int c = 0; c < 9; ++c) bx[9 * (nkeep + k) + c] = box[9 * k + c];
+      if (periodic)
+        for (int c = 0; c < 3; ++c) per[3 * (nkeep + k) + c] = periodic[3 * k + c];
+      if (natoms[k] <= 0) throw Error(RX_ERR_INVALID, "every system needs at least one atom");
+      nadd += natoms[k];
+    }
+    ty.insert(ty.end(), types, types + nadd);
+    tg.insert(tg.end(), tags, tags + nadd);
+    // the state to carry, before the buffers are resized
+    const int old_na = na, old_nsys = nsys;
+    const bool had_md = md_ready;
+    const MdDev md_old = md;
+    DBuf<double4> ox, ov;
+    DBuf<double> oq, osh, oth;
+    std::vector<double> oxi, ovxi;
+    if (nkeep > 0) {
+      ox.ensure(static_cast<size_t>(old_na)); oq.ensure(static_cast<size_t>(old_na));
+      osh.ensure(4 * static_cast<size_t>(old_na)); oth.ensure(4 * static_cast<size_t>(old_na));
+      RXCU(cudaMemcpy(ox.p, x.p, sizeof(double4) * old_na, cudaMemcpyDeviceToDevice));
+      RXCU(cudaMemcpy(oq.p, q.p, sizeof(double) * old_na, cudaMemcpyDeviceToDevice));
+      RXCU(cudaMemcpy(osh.p, s_hist.p, sizeof(double) * 4 * old_na, cudaMemcpyDeviceToDevice));
+      RXCU(cudaMemcpy(oth.p, t_hist.p, sizeof(double) * 4 * old_na, cudaMemcpyDeviceToDevice));
+      if (had_md) {
+        ov.ensure(static_cast<size_t>(old_na));
+        RXCU(cudaMemcpy(ov.p, v.p, sizeof(double4) * old_na, cudaMemcpyDeviceToDevice));
+        oxi.resize(static_cast<size_t>(old_nsys) * kMaxChain);
+        ovxi.resize(oxi.size());
+        RXCU(cudaMemcpy(oxi.data(), xi.p, sizeof(double) * oxi.size(), cudaMemcpyDeviceToHost));
+        RXCU(cudaMemcpy(ovxi.data(), vxi.p, sizeof(double) * ovxi.size(), cudaMemcpyDeviceToHost));
+      }
+    }
+    const bool had_forces = forces_valid;
+    DBuf<double4> og;
+    if (nkeep > 0 && had_forces) {
+      og.ensure(static_cast<size_t>(old_na));
+      RXCU(cudaMemcpy(og.p, grad.p, sizeof(double4) * old_na, cudaMemcpyDeviceToDevice));
+    }
+    set_systems(ns, nat.data(), org.data(), bx.data(), per.data(), ty.data(), tg.data());
+    if (nadd > 0) {   // new systems start with cold charge histories
+      RXCU(cudaMemset(s_hist.p + 4 * nkept_atoms, 0, sizeof(double) * 4 * nadd));
+      RXCU(cudaMemset(t_hist.p + 4 * nkept_atoms, 0, sizeof(double) * 4 * nadd));
+    }
+    // positions: new systems from the caller, kept ones gathered from the saved state
+    {
+      std::vector<double4> h(static_cast<size_t>(nadd));
+      for (long long a = 0; a < nadd; ++a) h[static_cast<size_t>(a)] = make_double4(x_new[3 * a], x_new[3 * a + 1], x_new[3 * a + 2], 0.0);
+      if (nadd > 0) RXCU(cudaMemcpy(x.p + nkept_atoms, h.data(), sizeof(double4) * nadd, cudaMemcpyHostToDevice));
+    }
+    DBuf<int> srcd;
+    if (nkept_atoms > 0) {
+      srcd.ensure(nkept_atoms);
+      RXCU(cudaMemcpy(srcd.p, src.data(), sizeof(int) * nkept_atoms, cudaMemcpyHostToDevice));
+      ++launches;
+      k_gather_state<<<blocks(static_cast<long long>(nkept_atoms), 256), 256, 0, stream>>>(
+          static_cast<int>(nkept_atoms), srcd.p, ox.p, oq.p, osh.p, oth.p, x.p, q.p, s_hist.p, t_hist.p);
+    }
+    if (had_forces && nkeep > 0 && nadd == 0) {   // only removals: the kept systems' forces stay valid
+      ++launches;
+      k_gather_vel<<<blocks(static_cast<long long>(nkept_atoms), 256), 256, 0, stream>>>(static_cast<int>(nkept_atoms), srcd.p, og.p, grad.p);
+    }
+    if (had_md) {
+      md_layout(md_old.dt, md_old.t_start, md_old.t_stop, md_old.t_damp, md_old.chain);
+      RXCU(cudaMemsetAsync(v.p, 0, sizeof(double4) * na, stream));
+      if (nkept_atoms > 0) {
+        ++launches;
+        k_gather_vel<<<blocks(static_cast<long long>(nkept_atoms), 256), 256, 0, stream>>>(static_cast<int>(nkept_atoms), srcd.p, ov.p, v.p);
+      }
+      if (v_new && nadd > 0) {
+        std::vector<double4> h(static_cast<size_t>(nadd));
+        for (long long a = 0; a < nadd; ++a) h[static_cast<size_t>(a)] = make_double4(v_new[3 * a], v_new[3 * a + 1], v_new[3 * a + 2], 0.0);
+        RXCU(cudaMemcpyAsync(v.p + nkept_atoms, h.data(), sizeof(double4) * nadd, cudaMemcpyHostToDevice, stream));
+      }
+      std::vector<double> nxi(static_cast<size_t>(nsys) * kMaxChain, 0.0), nvxi(nxi.size(), 0.0);
+      for (int k = 0; k < nkeep; ++k)
+        for (int c = 0; c < kMaxChain; ++c) {
+          nxi[static_cast<size_t>(k) * kMaxChain + c] = oxi[static_cast<size_t>(keep[k]) * kMaxChain + c];
+          nvxi[static_cast<size_t>(k) * kMaxChain + c] = ovxi[static_cast<size_t>(keep[k]) * kMaxChain + c];
+        }
+      RXCU(cudaMemcpyAsync(xi.p, nxi.data(), sizeof(double) * nxi.size(), cudaMemcpyHostToDevice, stream));
+      RXCU(cudaMemcpyAsync(vxi.p, nvxi.data(), sizeof(double) * nvxi.size(), cudaMemcpyHostToDevice, stream));
+    }
+    RXCU(cudaStreamSynchronize(stream));
+    RXCU(cudaGetLastError());
+    have_pos = true;
+    forces_valid = had_forces && nkeep > 0 && nadd == 0;
+    force_rebuild();
+    RXCU(cudaStreamSynchronize(stream));
+  }
+
+  // per-system targets and activity (serving); NULL restores the common ramp / all active
+  DBuf<double> t_sys_buf;
+  DBuf<int> active_buf;
+  void md_targets(const double* t_target, const int* active) {
+    if (!md_ready) throw Error(RX_ERR_STATE, "call rx_md_setup first");
+    if (t_target) {
+      for (int s = 0; s < nsys; ++s)
+        if (!(t_target[s] > 0.0)) throw Error(RX_ERR_INVALID, "target temperatures must be positive");
+      t_sys_buf.ensure(static_cast<size_t>(nsys));
+      RXCU(cudaMemcpy(t_sys_buf.p, t_target, sizeof(double) * nsys, cudaMemcpyHostToDevice));
+    }
+    if (active) {
+      active_buf.ensure(static_cast<size_t>(nsys));
+      RXCU(cudaMemcpy(active_buf.p, active, sizeof(int) * nsys, cudaMemcpyHostToDevice));
+    }
+    const double* ts = t_target ? t_sys_buf.p : nullptr;
+    const int* ac = active ? active_buf.p : nullptr;
+    if (ts != md.t_sys || ac != md.active) drop_graph();   // a captured step holds the pointers, not the values
+    md.t_sys = ts;
+    md.active = ac;
   }
 
   void set_velocities(const double* vin) {
@@ -1052,10 +1221,10 @@ struct Context {
   void enqueue_step() {
     thermostat_half(0);
     ++launches;
-    k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 1);
+    k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, sys_of.p, grad.p, x.p, na, 1);
     enqueue_eval(true);
     ++launches;
-    k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, grad.p, x.p, na, 0);
+    k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, sys_of.p, grad.p, x.p, na, 0);
     thermostat_half(1);
   }
 
@@ -1125,7 +1294,7 @@ struct Context {
     const long long span = total_steps_hint > 0 ? total_steps_hint : nsteps;
     const double rh[2] = {0.0, static_cast<double>(span)};
     RXCU(cudaMemcpyAsync(ramp.p, rh, sizeof rh, cudaMemcpyHostToDevice, stream));
-    if (md_step == 0) evaluate(true);   // forces of the initial configuration
+    if (!forces_valid) evaluate(true);   // forces of the initial configuration
     int done = 0;
     while (done < nsteps) {
       const int chunk = std::min(nsteps - done, kChunk);
@@ -1352,11 +1521,28 @@ int rx_set_neighbor(rx_context* ctx, double skin) {
   return guarded(ctx, [&](rx::Context& c) { c.set_neighbor(skin); });
 }
 
+int rx_get_gradient(rx_context* ctx, double* grad) {
+  return guarded(ctx, [&](rx::Context& c) {
+    if (!grad) throw rx::Error(RX_ERR_INVALID, "null gradient array");
+    c.get_gradient(grad);
+  });
+}
+
 int rx_get_virial(rx_context* ctx, double* virial) {
   return guarded(ctx, [&](rx::Context& c) {
     if (!virial) throw rx::Error(RX_ERR_INVALID, "null virial array");
     c.get_virial(virial);
   });
+}
+
+int rx_update_systems(rx_context* ctx, int nkeep, const int* keep, int nnew, const int* natoms, const double* origin,
+                      const double* box, const int* periodic, const int* type, const int64_t* tag, const double* x,
+                      const double* v) {
+  return guarded(ctx, [&](rx::Context& c) { c.update_systems(nkeep, keep, nnew, natoms, origin, box, periodic, type, tag, x, v); });
+}
+
+int rx_md_targets(rx_context* ctx, const double* t_target, const int* active) {
+  return guarded(ctx, [&](rx::Context& c) { c.md_targets(t_target, active); });
 }
 
 int64_t rx_kernel_launches(const rx_context* ctx) { return (ctx && ctx->c) ? ctx->c->launches : 0; }

@@ -65,7 +65,6 @@ __global__ void k_bo_correct(Dev d, DevFF ff);
 __global__ void k_atom_quantities(Dev d, DevFF ff);
 __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl);
 __global__ void k_hbond(Dev d, DevFF ff, DevCtl ctl);
-__global__ void k_hbond_acceptor(Dev d, DevFF ff, DevCtl ctl);
 __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl);
 __global__ void k_fold(Dev d);
 __global__ void k_dbond(Dev d);

@@ -6,7 +6,6 @@
 //   k_bo_correct       corrected bond orders + the 11 C*dbo coefficients (terms.hpp:66-132)
 //   k_atom_quantities  Delta, Delta_e, nlp, ... of every atom (terms.hpp:141-164)
 //   k_bonded_atom      per centre atom: bond energy, lone pair, C2, over/under, valence/penalty/coalition, H-bonds
-//   k_hbond_acceptor   gradient on the acceptor of every H-bond triple (the same triple evaluated from its acceptor)
 //   k_torsion          torsion + 4-body conjugation per central bond
 //   k_fold             torsion contributions to second neighbors + CdDelta totals
 //   k_dbond            Add_dBond_to_Forces, own part (src/cpu/bonded.cpp:717-766)
@@ -560,29 +559,24 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
   ea[E_ANG] = e_ang; ea[E_PEN] = e_pen; ea[E_COA] = e_coa;
 }
 
-// Hydrogen bonds (src/cpu/bonded.cpp:654-715) of one triple: donor bond slot bi of hydrogen j, acceptor k at the
-// canonical vector dvjk (x_k - x_j) and distance r_jk. Every gate of the reference is taken in FP64 (types, tags,
-// BO >= HB_THRESHOLD, parameters present, r_jk <= hbond_cut by the caller); the term itself is FP32. sin^4(theta/2)
-// is formed as ((1 - cos theta) / 2)^2, the same quantity as the reference's sin(acos(c) / 2)^4.
+// Hydrogen bonds (src/cpu/bonded.cpp:654-715) of one triple: the donor bond of hydrogen j (its data loaded once per
+// bond: partner ia, its type and tag, BO, the bond vector), acceptor k at the canonical vector vk (x_k - x_j) and
+// distance r_jk. Every gate of the reference is taken in FP64 (types, tags, BO >= HB_THRESHOLD, parameters present,
+// r_jk <= hbond_cut by the caller); the term itself is FP32. sin^4(theta/2) is formed as ((1 - cos theta) / 2)^2, the
+// same quantity as the reference's sin(acos(c) / 2)^4.
+struct HbDonor { int type_i; long long tag_i; float BO, vi[3], d_ji; };
 struct HbOut { float e, CEhb1, CEhb2, CEhb3, dti[3], dtj[3], dtk[3]; };
-__device__ inline bool hbond_triple(const Dev& d, const DevFF& ff, int tj, int type_k, long long tag_k, size_t bi,
-                                    const float* vk, float r_jk, HbOut& o) {
-  const int ia = static_cast<int>(d.bcode[bi] & d.amask);
-  const int type_i = d.type[ia];
-  if (static_cast<int>(SBp(ff, type_i)[SB_P_HBOND]) != 2) return false;
-  const double BOd = d.bBO[bi].x;
-  if (!(BOd >= kHbThreshold)) return false;
-  if (d.tag[ia] == tag_k) return false;
-  const size_t key = (static_cast<size_t>(type_i) * ff.nt + tj) * ff.nt + type_k;
+__device__ inline bool hbond_triple(const DevFF& ff, const HbDonor& dn, int tj, int type_k, long long tag_k, const float* vk,
+                                    float r_jk, HbOut& o) {
+  if (dn.tag_i == tag_k) return false;
+  const size_t key = (static_cast<size_t>(dn.type_i) * ff.nt + tj) * ff.nt + type_k;
   if (!ff.hb_on[key]) return false;
   const double* hb = ff.hb + key * HB_NFIELDS;
   if (hb[HB_R0] <= 0.0) return false;
   const float r0 = static_cast<float>(hb[HB_R0]), p1 = static_cast<float>(hb[HB_P_HB1]);
   const float p2 = static_cast<float>(hb[HB_P_HB2]), p3 = static_cast<float>(hb[HB_P_HB3]);
-  const float BO = static_cast<float>(BOd);
-  const double4 dvi = d.bdv[bi];
-  const float vi[3] = {static_cast<float>(dvi.x), static_cast<float>(dvi.y), static_cast<float>(dvi.z)};
-  const float d_ji = static_cast<float>(dvi.w);
+  const float* vi = dn.vi;
+  const float d_ji = dn.d_ji;
   // reaxff_valence_angles.cpp:36-70 (calculate_theta / calculate_dcos_theta) in FP32
   const float inv = 1.0f / (d_ji * r_jk);
   const float dotv = vi[0] * vk[0] + vi[1] * vk[1] + vi[2] * vk[2];
@@ -598,7 +592,7 @@ __device__ inline bool hbond_triple(const Dev& d, const DevFF& ff, int tj, int t
   const float half = 0.5f * (1.0f - c);
   const float sin_xhz4 = half * half;
   const float cos_xhz1 = 1.0f - c;
-  const float exp_hb2 = __expf(-p2 * BO);
+  const float exp_hb2 = __expf(-p2 * dn.BO);
   const float exp_hb3 = __expf(-p3 * (r0 / r_jk + r_jk / r0 - 2.0f));
   o.e = p1 * (1.0f - exp_hb2) * exp_hb3 * sin_xhz4;
   o.CEhb1 = p1 * p2 * exp_hb2 * exp_hb3 * sin_xhz4;
@@ -607,9 +601,17 @@ __device__ inline bool hbond_triple(const Dev& d, const DevFF& ff, int tj, int t
   return true;
 }
 
+// Fixed-point accumulation (2^32 units): integer additions commute, so contributions added with atomics in any order
+// give the same bits every run - the deterministic scatter of the acceptor gradients.
+constexpr double kFixScale = 4294967296.0;
+__device__ inline void fix_add(unsigned long long* acc, double v) {
+  atomicAdd(acc, static_cast<unsigned long long>(__double2ll_rn(v * kFixScale)));
+}
+
 // One warp per hydrogen j (p_hbond = 1): for every donor bond of j, the lanes walk j's near row for acceptors
-// (p_hbond = 2, r <= hbond_cut). Energy, the gradient of j and the coefficient / gradient of the donor bond are
-// reduced over the warp in fixed order; the donor's share goes to j's slot for the donor to gather.
+// (p_hbond = 2, r <= hbond_cut); each triple is evaluated once. Energy, the gradient of j and the coefficient /
+// gradient of the donor bond are reduced over the warp in fixed order (the donor's share goes to j's slot for the
+// donor to gather); the acceptor's gradient is added to its fixed-point accumulator (zeroed by k_pairs).
 __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
   if (lists_failed(d)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -617,7 +619,7 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
   if (warp >= d.na) return;
   const int j = warp;
   const int tj = d.type[j];
-  {   // this kernel's accumulators of atom j start at zero (the acceptor kernel adds to fown_h after it)
+  {   // this kernel's accumulators of atom j start at zero
     const int nbj = min(d.bcnt[j], d.bcap);
     for (int k = lane; k < nbj; k += 32) {
       d.bcdbo_h[static_cast<size_t>(j) * d.bcap + k] = 0.0;
@@ -644,11 +646,21 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
   int ntrip = 0;
   for (int pi = 0; pi < nb; ++pi) {
     const size_t bi = base + pi;
-    {  // donor gates that do not depend on the acceptor (warp-uniform)
+    HbDonor dn;
+    {  // donor gates that do not depend on the acceptor (warp-uniform), and the donor's data
       const int ia = static_cast<int>(d.bcode[bi] & d.amask);
-      if (static_cast<int>(SBp(ff, d.type[ia])[SB_P_HBOND]) != 2 || !(d.bBO[bi].x >= kHbThreshold)) continue;
+      dn.type_i = d.type[ia];
+      const double BOd = d.bBO[bi].x;
+      if (static_cast<int>(SBp(ff, dn.type_i)[SB_P_HBOND]) != 2 || !(BOd >= kHbThreshold)) continue;
+      dn.tag_i = d.tag[ia];
+      dn.BO = static_cast<float>(BOd);
+      const double4 dvi = d.bdv[bi];
+      dn.vi[0] = static_cast<float>(dvi.x); dn.vi[1] = static_cast<float>(dvi.y); dn.vi[2] = static_cast<float>(dvi.z);
+      dn.d_ji = static_cast<float>(dvi.w);
     }
     double c1 = 0.0, fi0 = 0.0, fi1 = 0.0, fi2 = 0.0;
+    const double4 dvi = d.bdv[bi];
+    const double pi3[3] = {dvi.x, dvi.y, dvi.z};
     for (int e0 = 0; e0 < cnt; e0 += 32) {
       const int ee = e0 + lane;
       if (ee >= cnt) continue;
@@ -665,7 +677,7 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
       const float vk[3] = {static_cast<float>(dvjk[0]), static_cast<float>(dvjk[1]), static_cast<float>(dvjk[2])};
       const float r_jk = static_cast<float>(r_jkd);
       HbOut o;
-      if (!hbond_triple(d, ff, tj, type_k, d.tag[ka], bi, vk, r_jk, o)) continue;
+      if (!hbond_triple(ff, dn, tj, type_k, d.tag[ka], vk, r_jk, o)) continue;
       ++ntrip;
       e += o.e;
       c1 += o.CEhb1;
@@ -674,11 +686,10 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
       fj0 += o.CEhb2 * o.dtj[0] + c3 * vk[0];
       fj1 += o.CEhb2 * o.dtj[1] + c3 * vk[1];
       fj2 += o.CEhb2 * o.dtj[2] + c3 * vk[2];
-      // virial of the triple about the hydrogen: donor at the bond vector, acceptor at vk
       const float gk[3] = {o.CEhb2 * o.dtk[0] - c3 * vk[0], o.CEhb2 * o.dtk[1] - c3 * vk[1], o.CEhb2 * o.dtk[2] - c3 * vk[2]};
       const float gi[3] = {o.CEhb2 * o.dti[0], o.CEhb2 * o.dti[1], o.CEhb2 * o.dti[2]};
-      const double4 dvi = d.bdv[bi];
-      const double pi3[3] = {dvi.x, dvi.y, dvi.z};
+      for (int c = 0; c < 3; ++c) fix_add(d.fix_h + 3 * static_cast<size_t>(ka) + c, static_cast<double>(gk[c]));
+      // virial of the triple about the hydrogen: donor at the bond vector, acceptor at vk
       vir_add(vir, pi3, gi);
       vir_add(vir, vk, gk);
     }
@@ -697,54 +708,6 @@ __global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
     for (int c = 0; c < kVir; ++c) d.vir_h[static_cast<size_t>(j) * kVir + c] = vir[c];
     d.eatom[static_cast<size_t>(j) * kTerms + E_HB] = e;
     d.census[3 * d.na + j] = ntrip;
-  }
-}
-
-// The gradient on the acceptor k of every H-bond triple: each triple is evaluated again from the acceptor's side
-// (one warp per acceptor, lanes over its near row), with bitwise the same inputs (the hydrogen's bond slot, the
-// canonical j -> k vector), so the acceptor gathers its own gradient without writing to any other atom.
-__global__ void __launch_bounds__(128) k_hbond_acceptor(Dev d, DevFF ff, DevCtl ctl) {
-  if (lists_failed(d)) return;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= d.na) return;
-  const int k = warp;
-  const int type_k = d.type[k];
-  if (!(ctl.hbond_cut > 0) || static_cast<int>(SBp(ff, type_k)[SB_P_HBOND]) != 2) return;
-  const SysInfo s = d.sys[d.sys_of[k]];
-  const int cnt = min(d.near_cnt[k], d.ncap_near);
-  const double hc2 = ctl.hbond_cut * ctl.hbond_cut;
-  const long long tag_k = d.tag[k];
-  double f0 = 0, f1 = 0, f2 = 0;
-  for (int e = lane; e < cnt; e += 32) {
-    const unsigned code = d.near[static_cast<size_t>(k) * d.ncap_near + e];
-    const int h = static_cast<int>(code & d.amask);
-    const int tj = d.type[h];
-    if (static_cast<int>(SBp(ff, tj)[SB_P_HBOND]) != 1) continue;
-    double dkh[3];
-    pair_dvec(d, s, k, h, static_cast<int>(code >> d.abits), dkh);
-    const double dvjk[3] = {-dkh[0], -dkh[1], -dkh[2]};
-    const double r2 = dot3(dvjk, dvjk);
-    if (!(r2 <= hc2)) continue;
-    const double r_jkd = sqrt(r2);
-    if (!(r_jkd <= ctl.hbond_cut)) continue;
-    const float vk[3] = {static_cast<float>(dvjk[0]), static_cast<float>(dvjk[1]), static_cast<float>(dvjk[2])};
-    const float r_jk = static_cast<float>(r_jkd);
-    const int nb = min(d.bcnt[h], d.bcap);
-    for (int pi = 0; pi < nb; ++pi) {
-      HbOut o;
-      if (!hbond_triple(d, ff, tj, type_k, tag_k, static_cast<size_t>(h) * d.bcap + pi, vk, r_jk, o)) continue;
-      const float c3 = o.CEhb3 / r_jk;
-      f0 += o.CEhb2 * o.dtk[0] + c3 * vk[0];
-      f1 += o.CEhb2 * o.dtk[1] + c3 * vk[1];
-      f2 += o.CEhb2 * o.dtk[2] + c3 * vk[2];
-    }
-  }
-  f0 = warp_sum(f0); f1 = warp_sum(f1); f2 = warp_sum(f2);
-  if (lane == 0) {
-    double4 f = d.fown_h[k];
-    f.x += f0; f.y += f1; f.z += f2;
-    d.fown_h[k] = f;
   }
 }
 
@@ -1049,6 +1012,8 @@ __global__ void k_force_final(Dev d) {
   const size_t base = static_cast<size_t>(a) * d.bcap;
   const double4 f1 = d.fown[a], fh = d.fown_h[a], ft = d.fown_t[a], f2 = d.fdb[a], f3 = d.fnb[a];
   double g[3] = {f1.x + fh.x + ft.x + f2.x + f3.x, f1.y + fh.y + ft.y + f2.y + f3.y, f1.z + fh.z + ft.z + f2.z + f3.z};
+  for (int c = 0; c < 3; ++c)   // H-bond acceptor gradient, fixed point
+    g[c] += static_cast<double>(static_cast<long long>(d.fix_h[3 * static_cast<size_t>(a) + c])) * (1.0 / kFixScale);
   for (int k = 0; k < nb; ++k) {
     const size_t b = base + k;
     const int p = static_cast<int>(d.bcode[b] & d.amask);

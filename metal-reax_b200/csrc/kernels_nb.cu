@@ -196,6 +196,7 @@ __global__ void __launch_bounds__(128) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   const int warp = gid >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
+  if (lane < 3) d.fix_h[3 * static_cast<size_t>(warp) + lane] = 0ull;   // the H-bond acceptor accumulators of this step
   if (lists_failed(d)) return;
   const int i = warp;
   const SysInfo s = d.sys[d.sys_of[i]];

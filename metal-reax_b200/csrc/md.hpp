@@ -24,6 +24,10 @@ struct MdDev {
   // temperature ramp of the current run (device-resident, so a captured step takes no per-step argument):
   // ramp[0] = steps done in this run, ramp[1] = steps of the run; T = t_start + (done / steps) (t_stop - t_start)
   double* ramp;
+  // serving: per-system target temperature (null: the ramp above for every system) and per-system activity
+  // (null: all active; 0: the system is frozen - its atoms and its chain are not advanced)
+  const double* t_sys;
+  const int* active;
 };
 
 constexpr int kKeChunk = 1024;
@@ -32,6 +36,10 @@ __global__ void k_md_kinetic_part(MdDev m, const SysInfo* sys, const int* type);
 __global__ void k_md_kinetic_sum(MdDev m, int nsys);
 __global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys);
 __global__ void k_md_scale(MdDev m, const int* sys_of, int na, int advance);
-__global__ void k_md_kick(MdDev m, const int* type, const double4* grad, double4* x, int na, int drift);
+__global__ void k_md_kick(MdDev m, const int* type, const int* sys_of, const double4* grad, double4* x, int na, int drift);
+
+__global__ void k_gather_state(int n, const int* src, const double4* ox, const double* oq, const double* osh,
+                               const double* oth, double4* x, double* q, double* sh, double* th);
+__global__ void k_gather_vel(int n, const int* src, const double4* ov, double4* v);
 
 }  // namespace rx

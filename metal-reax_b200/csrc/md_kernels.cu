@@ -53,11 +53,15 @@ __global__ void k_md_kinetic_sum(MdDev m, int nsys) {
 __global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
+  if (m.active && !m.active[s]) {
+    m.scale[s] = 1.0;
+    return;
+  }
   const double step_frac = m.ramp[1] > 0.0 ? m.ramp[0] / m.ramp[1] : 0.0;
   const int M = m.chain;
   double* xi = m.xi + s * kMaxChain;
   double* vx = m.vxi + s * kMaxChain;
-  const double T = m.t_start + step_frac * (m.t_stop - m.t_start);
+  const double T = m.t_sys ? m.t_sys[s] : m.t_start + step_frac * (m.t_stop - m.t_start);
   const double kT = kBoltz * T;
   const double nf = 3.0 * sys[s].natoms - 3.0;
   const double tau2 = m.t_damp * m.t_damp;
@@ -101,9 +105,10 @@ __global__ void k_md_scale(MdDev m, const int* sys_of, int na, int advance) {
 }
 
 // v += dt/2 * F/m (F = -grad); with drift: x += dt * v
-__global__ void k_md_kick(MdDev m, const int* type, const double4* grad, double4* x, int na, int drift) {
+__global__ void k_md_kick(MdDev m, const int* type, const int* sys_of, const double4* grad, double4* x, int na, int drift) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= na) return;
+  if (m.active && !m.active[sys_of[a]]) return;
   const double c = 0.5 * m.dt * kFtm2v / m.mass[type[a]];
   const double4 g = grad[a];
   double4 v = m.v[a];
@@ -114,6 +119,26 @@ __global__ void k_md_kick(MdDev m, const int* type, const double4* grad, double4
     p.x += m.dt * v.x; p.y += m.dt * v.y; p.z += m.dt * v.z;
     x[a] = p;
   }
+}
+
+// continuous batching: carry the state of kept atoms (new index a, old index src[a]) into the re-laid-out arrays
+__global__ void k_gather_state(int n, const int* src, const double4* ox, const double* oq, const double* osh,
+                               const double* oth, double4* x, double* q, double* sh, double* th) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const int o = src[a];
+  x[a] = ox[o];
+  q[a] = oq[o];
+  for (int k = 0; k < 4; ++k) {
+    sh[4 * static_cast<size_t>(a) + k] = osh[4 * static_cast<size_t>(o) + k];
+    th[4 * static_cast<size_t>(a) + k] = oth[4 * static_cast<size_t>(o) + k];
+  }
+}
+
+__global__ void k_gather_vel(int n, const int* src, const double4* ov, double4* v) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  v[a] = ov[src[a]];
 }
 
 }  // namespace rx

@@ -31,7 +31,7 @@ EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
-           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset"]
+           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset", "rx_update_systems", "rx_md_targets", "rx_get_gradient"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -70,7 +70,8 @@ def load():
         "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
         "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
-        "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]), "rx_set_acks2": (_I, [_V, _V]), "rx_qeq_reset": (_I, [_V]),
+        "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]), "rx_set_acks2": (_I, [_V, _V]), "rx_qeq_reset": (_I, [_V]), "rx_md_targets": (_I, [_V, _V, _V]), "rx_get_gradient": (_I, [_V, _V]),
+        "rx_update_systems": (_I, [_V, _I, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -155,6 +156,38 @@ class Engine:
         x = np.ascontiguousarray(np.concatenate([np.asarray(s["x"], dtype=np.float64).reshape(-1, 3) for s in systems]))
         self.set_positions(x)
 
+    def update_systems(self, keep, new_systems, new_velocities=None):
+        """Continuous batching: keep the listed current systems (their device state carried, in this order) and append
+        new ones (dicts as for set_systems, velocities per new system or None)."""
+        keep = np.ascontiguousarray(keep, dtype=np.int32)
+        nn = len(new_systems)
+        if nn:
+            natoms = np.array([len(s["type"]) for s in new_systems], dtype=np.int32)
+            origin = np.ascontiguousarray(np.concatenate([np.asarray(s["origin"], dtype=np.float64) for s in new_systems]))
+            box = np.ascontiguousarray(np.concatenate([np.asarray(s["box"], dtype=np.float64).reshape(9) for s in new_systems]))
+            per = np.ascontiguousarray(np.concatenate([np.asarray(s["periodic"], dtype=np.int32) for s in new_systems]))
+            ty = np.ascontiguousarray(np.concatenate([np.asarray(s["type"], dtype=np.int32) for s in new_systems]))
+            tg = np.ascontiguousarray(np.concatenate([np.asarray(s["tag"], dtype=np.int64) for s in new_systems]))
+            x = np.ascontiguousarray(np.concatenate([np.asarray(s["x"], dtype=np.float64).reshape(-1, 3) for s in new_systems]))
+            v = None
+            if new_velocities is not None:
+                v = np.ascontiguousarray(np.concatenate([np.asarray(vv, dtype=np.float64).reshape(-1, 3) for vv in new_velocities]))
+        else:
+            natoms = origin = box = per = ty = tg = x = v = None
+        self._check(self.lib.rx_update_systems(self.h, len(keep), _p(keep), nn, _p(natoms), _p(origin), _p(box), _p(per),
+                                               _p(ty), _p(tg), _p(x), _p(v)))
+        old = self.natoms
+        kept = [int(old[k]) for k in keep]
+        self.natoms = np.array(kept + ([] if not nn else list(natoms)), dtype=np.int32)
+        self.nsys = len(self.natoms)
+        self.na = int(self.natoms.sum())
+        self.offsets = np.concatenate([[0], np.cumsum(self.natoms)])
+
+    def md_targets(self, t_target=None, active=None):
+        t = None if t_target is None else np.ascontiguousarray(t_target, dtype=np.float64)
+        a = None if active is None else np.ascontiguousarray(active, dtype=np.int32)
+        self._check(self.lib.rx_md_targets(self.h, _p(t), _p(a)))
+
     def set_positions(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
         if x.size != 3 * self.na:
@@ -195,6 +228,12 @@ class Engine:
         sk = None if s_kin is None else np.ascontiguousarray(s_kin, dtype=np.float64)
         self._check(self.lib.rx_set_acks2(self.h, _p(sk)))
         self._s_kin = sk
+
+    def gradient(self):
+        """dE/dx of the last force evaluation (rx_compute or the last MD step)."""
+        g = np.zeros(3 * self.na)
+        self._check(self.lib.rx_get_gradient(self.h, _p(g)))
+        return g.reshape(-1, 3)
 
     def virial(self):
         """LAMMPS-order virial (xx, yy, zz, xy, xz, yz) of the last force evaluation, per system."""

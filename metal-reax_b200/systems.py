@@ -100,6 +100,56 @@ def _rsa(n, L, dmin, rng, max_tries=200000):
     return out
 
 
+def _rsa_batched(n, L, dmin, rng, max_rounds=10000):
+    """Random sequential addition in a periodic cube (minimum separation dmin), accepting candidates in batches: a
+    candidate is kept when no accepted atom and no earlier candidate of its batch lies within dmin (k-d tree with
+    periodic bounds). The same acceptance rule as _rsa, vectorised for the large serving systems."""
+    from scipy.spatial import cKDTree
+    out = np.empty((0, 3))
+    for _ in range(max_rounds):
+        need = n - len(out)
+        if need <= 0:
+            break
+        cand = rng.uniform(0.0, L, size=(max(8, need + need // 4), 3)) % L
+        ok = np.ones(len(cand), dtype=bool)
+        if len(out):
+            ok &= np.isinf(cKDTree(out, boxsize=L).query(cand, k=1, distance_upper_bound=dmin)[0])
+        for a, b in sorted(cKDTree(cand, boxsize=L).query_pairs(dmin)):
+            if ok[a]:
+                ok[b] = False
+        out = np.concatenate([out, cand[ok][:need]])
+    if len(out) < n:
+        raise RuntimeError("random packing failed")
+    return out
+
+
+def serving_request(k, seed=4242, nmin=100, nmax=5000, dmin=0.9):
+    """The k-th request of the serving workload: a fresh CHO system built as random_cho but with n log-uniform in
+    [nmin, nmax]; half the requests are single points (energy, forces, charges), half NVT runs of 10-1000 steps at
+    300-3000 K. Returns (system, kind, steps, T)."""
+    rng = np.random.default_rng([seed, k])
+    n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+    frac = rng.dirichlet([1.0, 1.0, 1.0])
+    raw = frac * n
+    cnt = np.floor(raw).astype(int)
+    for idx in np.argsort(-(raw - cnt), kind="stable")[: n - cnt.sum()]:
+        cnt[idx] += 1
+    types = np.repeat(np.arange(3, dtype=np.int32), cnt)
+    rng.shuffle(types)
+    density = rng.uniform(0.5, 1.2)
+    L = (MASS[types].sum() * AMU_G / density) ** (1.0 / 3.0) * 1e8
+    x = _rsa_batched(n, L, dmin, rng)
+    kind = "sp" if rng.uniform() < 0.5 else "md"
+    steps = int(rng.integers(10, 1001)) if kind == "md" else 0
+    T = float(rng.uniform(300.0, 3000.0)) if kind == "md" else 0.0
+    return _finish("req%d_%d" % (k, n), L, x, types), kind, steps, T
+
+
+def poisson_arrivals(nreq, rate=200.0, seed=4242):
+    """Arrival times [s] of a Poisson request stream."""
+    return np.cumsum(np.random.default_rng([seed, 1 << 20]).exponential(1.0 / rate, size=nreq))
+
+
 def random_carbon(n=30000, density=1.0, seed=4000, dmin=1.2):
     L = (n * 12.0 * AMU_G / density) ** (1.0 / 3.0) * 1e8
     rng = np.random.default_rng(seed)
