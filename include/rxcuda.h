@@ -137,9 +137,13 @@ int rx_get_gradient(rx_context* ctx, double* grad);
 int rx_get_virial(rx_context* ctx, double* virial);
 
 /* Nose-Hoover chain NVT (the LAMMPS `fix nvt temp Tstart Tstop Tdamp` the reference's examples run), velocity Verlet
- * with dt [fs]. mass[ntypes] g/mol per force-field type. Charges are re-equilibrated before every force evaluation. */
+ * with dt [fs]. mass[ntypes] g/mol per force-field type. Charges are re-equilibrated before every force evaluation
+ * unless rx_md_charges switched that off. chain = 0 runs plain NVE (`fix nve`). */
 int rx_md_setup(rx_context* ctx, const double* mass, double dt, double t_start, double t_stop, double t_damp, int chain);
 int rx_set_velocities(rx_context* ctx, const double* v);  /* v[3*NA] A/fs */
+/* on = 0: rx_md_run keeps the charges as set (a run without a charge fix, as the reference's one-element carbon
+ * example; q = 0 there); on = 1 (default): charges re-equilibrated before every force evaluation. */
+int rx_md_charges(rx_context* ctx, int on);
 int rx_get_velocities(rx_context* ctx, double* v);
 /* nsteps steps of every system; energies (13*nsys, last step) and temperature (nsys) may be NULL */
 int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature);
@@ -185,6 +189,22 @@ int rx_update_systems(rx_context* ctx, int nkeep, const int* keep, int nnew, con
  * rx_md_setup) and active[nsys] (NULL: all; 0 freezes a system: its atoms and its chain are not advanced, its
  * forces are still evaluated). */
 int rx_md_targets(rx_context* ctx, const double* t_target, const int* active);
+
+/* Launch-shape tuning (no counterpart in the reference, whose Metal kernels use a fixed threadgroup of 64). None of
+ * these changes a result bit. RX_TUNE_*_TPB: threads per block of a warp-per-atom kernel (64, 128, 256: atoms per
+ * block x 32) or of the thread-per-atom bonded kernels (32, 64, 128); RX_TUNE_LONE_GRID_MIN: a context holding one
+ * system of more atoms takes the single-system CG (all SMs on its rows, default 4096; a batch always takes the
+ * segmented CG, so a system alone and in a batch give the same bits only below this size). rx_autotune times every
+ * candidate shape on the current systems (reps launches each, CUDA events) and keeps the fastest; chosen[5] (may be
+ * NULL) receives pairs, bonds, non-bonded, H-bond and per-atom shapes. */
+#define RX_TUNE_PAIRS_TPB 1
+#define RX_TUNE_BONDS_TPB 2
+#define RX_TUNE_NONBONDED_TPB 3
+#define RX_TUNE_HBOND_TPB 4
+#define RX_TUNE_ATOM_TPB 5
+#define RX_TUNE_LONE_GRID_MIN 6
+int rx_set_tuning(rx_context* ctx, int key, int value);
+int rx_autotune(rx_context* ctx, int reps, int* chosen);
 
 /* Number of this engine's own kernels launched on the context so far (library kernels, e.g. the radix sort of the cell
  * lists, are not counted). */

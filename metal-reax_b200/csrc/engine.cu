@@ -83,10 +83,17 @@ struct Context {
   // one captured MD step (replayed for every step of rx_md_run); dropped whenever a buffer or a parameter it holds
   // changes
   cudaGraphExec_t md_graph = nullptr;
+  // one captured evaluation without / with the charge solve (rx_compute, the batch evaluations)
+  cudaGraphExec_t eval_graph[2] = {nullptr, nullptr};
+  long long eval_launches[2] = {0, 0};
   bool graphs_ok = true;                // false after a capture failed: steps are then launched one by one
   void drop_graph() {
     if (md_graph) cudaGraphExecDestroy(md_graph);
     md_graph = nullptr;
+    for (auto& g : eval_graph) {
+      if (g) cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
   }
   std::string err;
 
@@ -635,7 +642,7 @@ struct Context {
     RXCU(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, key_bits, stream));
     k_cell_start<<<blocks(na + 1, 256), 256, 0, stream>>>(d, cell_key_sorted.p);
     k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d);
-    k_pairs<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, qp);
+    k_pairs<<<blocks(static_cast<long long>(na) * 32, tune.tpb_pairs), tune.tpb_pairs, 0, stream>>>(d, dff, qp);
     toc(0);
   }
 
@@ -647,9 +654,15 @@ struct Context {
     return a;
   }
 
+  // Launch shapes (atoms per block of the warp-per-atom and thread-per-atom kernels, the size above which a lone
+  // system takes the single-system CG): none changes a result bit, so rx_autotune may pick them by measurement.
+  struct Tune {
+    int tpb_pairs = 128, tpb_nb = 128, tpb_hb = 128, tpb_bonds = 128, tpb_atom = 64;
+    int lone_grid_min = 4096;
+  } tune;
   int grid_per_sm = 0, seg_per_sm = 0;
   void launch_cg(const Dev& d, CgArgs a) {
-    if (nsys == 1 && na > 4096) {   // one large system: all SMs on its rows, block partials summed in block order
+    if (nsys == 1 && na > tune.lone_grid_min) {   // one large system: all SMs on its rows, block partials in block order
       const int threads = 256;
       if (!grid_per_sm) RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k_cg_grid, threads, 0));
       int grid = std::max(1, std::min(grid_per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
@@ -698,7 +711,7 @@ struct Context {
     }
     tic(5, "nonbonded");
     ++launches;
-    k_nonbonded<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, nbs>>>(d, dff);
+    k_nonbonded<<<blocks(static_cast<long long>(na) * 32, tune.tpb_nb), tune.tpb_nb, 0, nbs>>>(d, dff);
     if (acks2_on) {
       ++launches;
       k_acks2<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, nbs>>>(d, dff, s_kin.p);
@@ -707,7 +720,7 @@ struct Context {
     if (conc) RXCU(cudaEventRecord(ev_join, side));
     tic(2, "bond_orders");
     launches += 4;
-    k_bonds<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, ctl);
+    k_bonds<<<blocks(static_cast<long long>(na) * 32, tune.tpb_bonds), tune.tpb_bonds, 0, stream>>>(d, dff, ctl);
     k_bond_sym<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d);
     k_bo_correct<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d, dff);
     k_atom_quantities<<<blocks(na, 128), 128, 0, stream>>>(d, dff);
@@ -719,12 +732,12 @@ struct Context {
     }
     tic(3, "bonded_terms");
     launches += 2;
-    k_bonded_atom<<<blocks(na, 64), 64, 0, stream>>>(d, dff, ctl);
-    k_hbond<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, hs>>>(d, dff, ctl);
+    k_bonded_atom<<<blocks(na, tune.tpb_atom), tune.tpb_atom, 0, stream>>>(d, dff, ctl);
+    k_hbond<<<blocks(static_cast<long long>(na) * 32, tune.tpb_hb), tune.tpb_hb, 0, hs>>>(d, dff, ctl);
     toc(3);
     tic(4, "torsion");
     ++launches;
-    k_torsion<<<blocks(na, 64), 64, 0, ts>>>(d, dff, ctl);
+    k_torsion<<<blocks(na, tune.tpb_atom), tune.tpb_atom, 0, ts>>>(d, dff, ctl);
     toc(4);
     if (conc) {
       RXCU(cudaEventRecord(ev_join_h, side_h));
@@ -789,7 +802,14 @@ struct Context {
     if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
     for (int attempt = 0;; ++attempt) {
       RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * kStatusWords, stream));
-      enqueue_eval(do_qeq);
+      const int gi = do_qeq ? 1 : 0;
+      if (graphs_ok && !timing && !eval_graph[gi]) capture(eval_graph[gi], eval_launches[gi], [&] { enqueue_eval(do_qeq); });
+      if (graphs_ok && !timing && eval_graph[gi]) {
+        RXCU(cudaGraphLaunch(eval_graph[gi], stream));
+        launches += eval_launches[gi];
+      } else {
+        enqueue_eval(do_qeq);
+      }
       if (do_qeq) fetch_qeq_counts();
       int st[kStatusWords];
       RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
@@ -820,6 +840,73 @@ struct Context {
     have_virial = true;
     ++launches;
     k_energy_sum<<<dim3(nsys, kTerms + kVir), 256, 0, stream>>>(dev(), energies.p, virial.p);
+  }
+
+  // ------------------------------------------------------------------ autotuning
+  // Times every candidate launch shape of the tunable kernels on the current systems (CUDA events around `reps`
+  // launches each, after one full evaluation that makes their inputs current) and keeps the fastest; then evaluates
+  // again so that every array is consistent. Returns the chosen shapes.
+  void autotune(int reps, int* out) {
+    require_ff();
+    require_sys();
+    if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
+    if (reps < 1) reps = 3;
+    const bool tm = timing;
+    timing = false;
+    evaluate(true);
+    const Dev d = dev();
+    cudaEvent_t a, b;
+    RXCU(cudaEventCreate(&a));
+    RXCU(cudaEventCreate(&b));
+    auto time_it = [&](auto&& launch) {
+      launch();   // warm
+      RXCU(cudaEventRecord(a, stream));
+      for (int r = 0; r < reps; ++r) launch();
+      RXCU(cudaEventRecord(b, stream));
+      RXCU(cudaEventSynchronize(b));
+      float ms = 0.f;
+      RXCU(cudaEventElapsedTime(&ms, a, b));
+      return ms;
+    };
+    const long long nw = static_cast<long long>(na) * 32;
+    auto pick = [&](int* slot, std::initializer_list<int> cands, auto&& launch_with) {
+      float best = 1e30f;
+      int arg = *slot;
+      for (int t : cands) {
+        const float ms = time_it([&] { launch_with(t); });
+        if (ms < best) { best = ms; arg = t; }
+      }
+      *slot = arg;
+    };
+    pick(&tune.tpb_pairs, {64, 128, 256}, [&](int t) { k_pairs<<<blocks(nw, t), t, 0, stream>>>(d, dff, qp); });
+    pick(&tune.tpb_bonds, {64, 128, 256}, [&](int t) { k_bonds<<<blocks(nw, t), t, 0, stream>>>(d, dff, ctl); });
+    pick(&tune.tpb_nb, {64, 128, 256}, [&](int t) { k_nonbonded<<<blocks(nw, t), t, 0, stream>>>(d, dff); });
+    pick(&tune.tpb_hb, {64, 128, 256}, [&](int t) { k_hbond<<<blocks(nw, t), t, 0, stream>>>(d, dff, ctl); });
+    pick(&tune.tpb_atom, {32, 64, 128}, [&](int t) {
+      k_bonded_atom<<<blocks(na, t), t, 0, stream>>>(d, dff, ctl);
+      k_torsion<<<blocks(na, t), t, 0, stream>>>(d, dff, ctl);
+    });
+    RXCU(cudaEventDestroy(a));
+    RXCU(cudaEventDestroy(b));
+    RXCU(cudaGetLastError());
+    drop_graph();
+    timing = tm;
+    evaluate(true);
+    if (out) { out[0] = tune.tpb_pairs; out[1] = tune.tpb_bonds; out[2] = tune.tpb_nb; out[3] = tune.tpb_hb; out[4] = tune.tpb_atom; }
+  }
+
+  void set_tuning(int key, int value) {
+    auto check = [&](bool ok) { if (!ok) throw Error(RX_ERR_INVALID, "tuning value out of range"); };
+    switch (key) {
+      case RX_TUNE_PAIRS_TPB: check(value == 64 || value == 128 || value == 256); tune.tpb_pairs = value; break;
+      case RX_TUNE_BONDS_TPB: check(value == 64 || value == 128 || value == 256); tune.tpb_bonds = value; break;
+      case RX_TUNE_NONBONDED_TPB: check(value == 64 || value == 128 || value == 256); tune.tpb_nb = value; break;
+      case RX_TUNE_HBOND_TPB: check(value == 64 || value == 128 || value == 256); tune.tpb_hb = value; break;
+      case RX_TUNE_ATOM_TPB: check(value == 32 || value == 64 || value == 128); tune.tpb_atom = value; break;
+      case RX_TUNE_LONE_GRID_MIN: check(value >= 0); tune.lone_grid_min = value; break;
+      default: throw Error(RX_ERR_INVALID, "unknown tuning key");
+    }
+    drop_graph();
   }
 
   // ------------------------------------------------------------------ state I/O
@@ -1015,8 +1102,8 @@ struct Context {
   void md_setup(const double* mass_in, double dt, double t0, double t1, double tdamp, int chain) {
     require_ff();
     require_sys();
-    if (!(dt > 0) || !(t0 > 0) || !(t1 > 0) || !(tdamp > 0) || chain < 1 || chain > kMaxChain)
-      throw Error(RX_ERR_INVALID, "md_setup: need dt, temperatures, damping > 0 and 1 <= chain <= 8");
+    if (!(dt > 0) || !(t0 > 0) || !(t1 > 0) || !(tdamp > 0) || chain < 0 || chain > kMaxChain)
+      throw Error(RX_ERR_INVALID, "md_setup: need dt, temperatures, damping > 0 and 0 <= chain <= 8");
     mass.ensure(static_cast<size_t>(ff.nt));
     RXCU(cudaMemcpy(mass.p, mass_in, sizeof(double) * ff.nt, cudaMemcpyHostToDevice));
     v.ensure(static_cast<size_t>(na));
@@ -1218,20 +1305,22 @@ struct Context {
   }
 
   // one velocity-Verlet step with the chain applied for dt/2 on each side (see md_kernels.cu), enqueued only
+  bool md_qeq = true;   // charges re-equilibrated at every step of rx_md_run
   void enqueue_step() {
     thermostat_half(0);
     ++launches;
     k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, sys_of.p, grad.p, x.p, na, 1);
-    enqueue_eval(true);
+    enqueue_eval(md_qeq);
     ++launches;
     k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, sys_of.p, grad.p, x.p, na, 0);
     thermostat_half(1);
   }
 
-  // Capture one step into a CUDA graph (every kernel argument of a step is fixed; what changes from step to step lives
-  // in device memory). Returns false, with graphs switched off for this context, if the capture is refused.
-  long long step_launches = 0;   // this engine's kernels in one captured step
-  bool capture_step() {
+  // Capture the launches `fn` enqueues into a CUDA graph (every kernel argument is fixed at capture; what changes
+  // from call to call lives in device memory). On failure graphs are switched off for this context and the launches
+  // go out one by one.
+  template <class F>
+  bool capture(cudaGraphExec_t& exec, long long& count, F&& fn) {
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       (void)cudaGetLastError();
@@ -1241,22 +1330,24 @@ struct Context {
     const long long l0 = launches;
     bool ok = true;
     try {
-      enqueue_step();
+      fn();
     } catch (const Error&) {
       ok = false;
     }
-    step_launches = launches - l0;
+    count = launches - l0;
     launches = l0;   // the capture itself launched nothing
     const cudaError_t e = cudaStreamEndCapture(stream, &g);
-    ok = ok && e == cudaSuccess && g && cudaGraphInstantiate(&md_graph, g, 0) == cudaSuccess;
+    ok = ok && e == cudaSuccess && g && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
     if (g) cudaGraphDestroy(g);
     if (!ok) {
-      md_graph = nullptr;
+      exec = nullptr;
       (void)cudaGetLastError();
       graphs_ok = false;
     }
     return ok;
   }
+  long long step_launches = 0;   // this engine's kernels in one captured MD step
+  bool capture_step() { return capture(md_graph, step_launches, [&] { enqueue_step(); }); }
 
   // state that a chunk of steps changes, saved before the chunk so that an overflow (lists grown, chunk repeated)
   // restarts from it
@@ -1294,7 +1385,7 @@ struct Context {
     const long long span = total_steps_hint > 0 ? total_steps_hint : nsteps;
     const double rh[2] = {0.0, static_cast<double>(span)};
     RXCU(cudaMemcpyAsync(ramp.p, rh, sizeof rh, cudaMemcpyHostToDevice, stream));
-    if (!forces_valid) evaluate(true);   // forces of the initial configuration
+    if (!forces_valid) evaluate(md_qeq);   // forces of the initial configuration
     int done = 0;
     while (done < nsteps) {
       const int chunk = std::min(nsteps - done, kChunk);
@@ -1315,7 +1406,7 @@ struct Context {
             }
           }
         }
-        fetch_qeq_counts();
+        if (md_qeq) fetch_qeq_counts();
         int st[kStatusWords];
         RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
         RXCU(cudaStreamSynchronize(stream));
@@ -1325,7 +1416,7 @@ struct Context {
           force_rebuild();
           continue;
         }
-        check_status(st, true);
+        check_status(st, md_qeq);
         break;
       }
       done += chunk;
@@ -1511,6 +1602,13 @@ int rx_md_run(rx_context* ctx, int nsteps, double* energies, double* temperature
   return guarded(ctx, [&](rx::Context& c) { c.md_run(nsteps, energies, temperature, 0); });
 }
 
+int rx_autotune(rx_context* ctx, int reps, int* chosen) {
+  return guarded(ctx, [&](rx::Context& c) { c.autotune(reps, chosen); });
+}
+int rx_set_tuning(rx_context* ctx, int key, int value) {
+  return guarded(ctx, [&](rx::Context& c) { c.set_tuning(key, value); });
+}
+
 int rx_qeq_reset(rx_context* ctx) { return guarded(ctx, [&](rx::Context& c) { c.qeq_reset(); }); }
 
 int rx_set_acks2(rx_context* ctx, const double* s_kin) {
@@ -1539,6 +1637,13 @@ int rx_update_systems(rx_context* ctx, int nkeep, const int* keep, int nnew, con
                       const double* box, const int* periodic, const int* type, const int64_t* tag, const double* x,
                       const double* v) {
   return guarded(ctx, [&](rx::Context& c) { c.update_systems(nkeep, keep, nnew, natoms, origin, box, periodic, type, tag, x, v); });
+}
+
+int rx_md_charges(rx_context* ctx, int on) {
+  return guarded(ctx, [&](rx::Context& c) {
+    c.md_qeq = on != 0;
+    c.drop_graph();
+  });
 }
 
 int rx_md_targets(rx_context* ctx, const double* t_target, const int* active) {

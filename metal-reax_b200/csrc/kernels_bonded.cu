@@ -612,7 +612,7 @@ __device__ inline void fix_add(unsigned long long* acc, double v) {
 // (p_hbond = 2, r <= hbond_cut); each triple is evaluated once. Energy, the gradient of j and the coefficient /
 // gradient of the donor bond are reduced over the warp in fixed order (the donor's share goes to j's slot for the
 // donor to gather); the acceptor's gradient is added to its fixed-point accumulator (zeroed by k_pairs).
-__global__ void __launch_bounds__(128) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
+__global__ void __launch_bounds__(256) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
   if (lists_failed(d)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;

@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d) {
 // charge-matrix entry H = 14.4 Tap(r) / cbrt(r^3 + (gamma_i gamma_j)^-1.5) for r <= swb (ENGINE_SPEC 7; fix_qeq_reaxff
 // compute_H) stored as hi + lo single-precision parts, and the near row (entries within max(bond_cut, hbond_cut)) the
 // bond and H-bond kernels scan. Also clears the per-system rebuild flags for the next evaluation.
-__global__ void __launch_bounds__(128) k_pairs(Dev d, DevFF ff, QeqParams qp) {
+__global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (gid < d.nsys) d.sys_flag[gid] = 0;
   const int warp = gid >> 5;

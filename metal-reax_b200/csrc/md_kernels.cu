@@ -1,4 +1,4 @@
-// Velocity Verlet with a Nose-Hoover chain thermostat (NVT), per system.
+// Velocity Verlet with a Nose-Hoover chain thermostat (NVT), per system; chain length 0 is plain NVE.
 //
 // The reference leaves time integration to LAMMPS (`fix nvt temp Tstart Tstop Tdamp`). This is the
 // Martyna-Tuckerman-Klein chain (Mol. Phys. 87, 1117 (1996)) applied for dt/2 before the first velocity half-kick
@@ -57,8 +57,16 @@ __global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys) {
     m.scale[s] = 1.0;
     return;
   }
-  const double step_frac = m.ramp[1] > 0.0 ? m.ramp[0] / m.ramp[1] : 0.0;
   const int M = m.chain;
+  if (M == 0) {   // NVE: no thermostat; the current kinetic energy and temperature only
+    const double nf0 = 3.0 * sys[s].natoms - 3.0;
+    const double ke = system_ke(m, s);
+    m.scale[s] = 1.0;
+    m.ke[s] = ke;
+    m.temp[s] = nf0 > 0.0 ? 2.0 * ke / (nf0 * kBoltz) : 0.0;
+    return;
+  }
+  const double step_frac = m.ramp[1] > 0.0 ? m.ramp[0] / m.ramp[1] : 0.0;
   double* xi = m.xi + s * kMaxChain;
   double* vx = m.vxi + s * kMaxChain;
   const double T = m.t_sys ? m.t_sys[s] : m.t_start + step_frac * (m.t_stop - m.t_start);

@@ -26,12 +26,13 @@ CENSUS = ["bonds", "angle_sets", "torsions", "hbonds", "nonbonded", "sbo_region"
 RX_COMPUTE_QEQ = 1
 RX_COMPUTE_CENSUS = 2
 RX_COMPUTE_QEQ_COLD = 4
+TUNE = {"pairs_tpb": 1, "bonds_tpb": 2, "nonbonded_tpb": 3, "hbond_tpb": 4, "atom_tpb": 5, "lone_grid_min": 6}
 STATUS = {0: "ok", 1: "invalid", 2: "ffield", 3: "capacity", 4: "cuda", 5: "not_converged", 6: "state", 7: "timeout"}
 EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_forcefield_dump", "rx_forcefield_params",
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
-           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset", "rx_update_systems", "rx_md_targets", "rx_get_gradient"]
+           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset", "rx_update_systems", "rx_md_targets", "rx_get_gradient", "rx_md_charges", "rx_autotune", "rx_set_tuning"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -70,7 +71,8 @@ def load():
         "rx_phase_times": (_I, [_V, ctypes.c_char_p, ctypes.c_long, _V, _I]),
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
         "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
-        "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]), "rx_set_acks2": (_I, [_V, _V]), "rx_qeq_reset": (_I, [_V]), "rx_md_targets": (_I, [_V, _V, _V]), "rx_get_gradient": (_I, [_V, _V]),
+        "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]), "rx_set_acks2": (_I, [_V, _V]), "rx_qeq_reset": (_I, [_V]), "rx_md_targets": (_I, [_V, _V, _V]), "rx_get_gradient": (_I, [_V, _V]), "rx_md_charges": (_I, [_V, _I]), "rx_autotune": (_I, [_V, _I, _V]),
+        "rx_set_tuning": (_I, [_V, _I, _I]),
         "rx_update_systems": (_I, [_V, _I, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V]),
     }
     for name, (res, args) in sig.items():
@@ -182,6 +184,19 @@ class Engine:
         self.nsys = len(self.natoms)
         self.na = int(self.natoms.sum())
         self.offsets = np.concatenate([[0], np.cumsum(self.natoms)])
+
+    def autotune(self, reps=3):
+        """Pick the fastest launch shapes on the current systems; returns them."""
+        out = np.zeros(5, dtype=np.int32)
+        self._check(self.lib.rx_autotune(self.h, reps, _p(out)))
+        return dict(zip(["pairs_tpb", "bonds_tpb", "nonbonded_tpb", "hbond_tpb", "atom_tpb"], out.tolist()))
+
+    def set_tuning(self, key, value):
+        self._check(self.lib.rx_set_tuning(self.h, TUNE[key], int(value)))
+
+    def md_charges(self, on=True):
+        """False: MD keeps the charges as set (no charge fix)."""
+        self._check(self.lib.rx_md_charges(self.h, 1 if on else 0))
 
     def md_targets(self, t_target=None, active=None):
         t = None if t_target is None else np.ascontiguousarray(t_target, dtype=np.float64)

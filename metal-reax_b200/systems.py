@@ -150,11 +150,15 @@ def poisson_arrivals(nreq, rate=200.0, seed=4242):
     return np.cumsum(np.random.default_rng([seed, 1 << 20]).exponential(1.0 / rate, size=nreq))
 
 
-def random_carbon(n=30000, density=1.0, seed=4000, dmin=1.2):
-    L = (n * 12.0 * AMU_G / density) ** (1.0 / 3.0) * 1e8
+def random_carbon(n=30000, density=1.0, seed=4000, dmin=1.2, amu=12.0):
+    """n carbon atoms uniformly random at `density` g/cm3 with RSA rejection of pairs closer than dmin (the algorithm of
+    the reference's examples/graphitization/make_box.py:14-26; with amu = 12.011, 30,000 atoms at 1.0 g/cm3 give its
+    84.265 A box). Large boxes use the batched acceptance of _rsa_batched."""
+    L = (n * amu * AMU_G / density) ** (1.0 / 3.0) * 1e8
     rng = np.random.default_rng(seed)
-    x = _rsa(n, L, dmin, rng)
-    return _finish("carbon%d" % n, L, x, np.zeros(n, dtype=np.int32))
+    x = _rsa(n, L, dmin, rng) if n <= 2000 else _rsa_batched(n, L, dmin, rng)
+    s = _finish("carbon%d" % n, L, x, np.zeros(n, dtype=np.int32))
+    return s
 
 
 def random_cho(k, nmin=64, nmax=1024, dmin=0.9):
