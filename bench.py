@@ -107,8 +107,8 @@ class Clocks:
 def model_bytes(N, P, D, I, R=0):
     """Algorithmic HBM bytes of one MD step, the fixed model of the hot-path scope table (independent of the
     implementation): 128 N + 8 P + P (4 + 8 I) + 12 P R + 256 D, with N atoms, P counted half pairs within the
-    non-bonded cut-off, D directed bonds, I fused s/t CG iterations, R FP64 residual refinements (none here: the whole
-    CG runs in FP64)."""
+    non-bonded cut-off, D directed bonds, I fused s/t CG iterations, R FP64 residual passes of the solve (the CG
+    iterates on the single-precision matrix and checks / refines with the FP64 one)."""
     return 128 * N + 8 * P + P * (4 + 8 * I) + 12 * P * R + 256 * D
 
 
@@ -116,7 +116,7 @@ def phase_model_bytes(name, N, P, D, I):
     """The same model split over the timed phases (N-proportional terms stay with the step)."""
     return {
         "neighbors": 4 * P + 4 * P,                 # pair list written (4 B) + H value written once (4 B)
-        "qeq": 8 * P * I,                           # H value + index read once per fused s/t iteration
+        "qeq": 8 * P * I,                           # H value + index read once per fused s/t iteration (+ 12 P R below)
         "nonbonded": 4 * P,                         # pair list read
         "bond_orders": 128 * D,
         "bonded_terms": 64 * D,
@@ -125,11 +125,13 @@ def phase_model_bytes(name, N, P, D, I):
     }.get(name, 0)
 
 
-def phase_impl_bytes(name, N, E, D, I):
-    """Bytes this implementation must move per phase (E = neighbor-row entries, both directions; FP64 H values)."""
+def phase_impl_bytes(name, N, E, D, I, R=1, EV=None):
+    """Bytes this implementation moves per phase: E neighbor-row entries (both directions) filtered every step from EV
+    Verlet-row entries; the charge matrix as single-precision hi + lo parts."""
+    EV = EV if EV is not None else E
     return {
-        "neighbors": 12 * E + 64 * N,               # row entry (4 B) + FP64 H value (8 B) written; positions
-        "qeq": I * (12 * E + 160 * N),              # every entry + value read once per pass; ~10 vectors of 16 B/atom
+        "neighbors": 4 * EV + 12 * E + 64 * N,      # Verlet codes read; row code + hi + lo written; positions
+        "qeq": I * (8 * E + 112 * N) + R * (12 * E + 64 * N),   # code + hi per iteration; code + hi + lo per FP64 pass
         "nonbonded": 4 * E + 64 * N,
     }.get(name, phase_model_bytes(name, N, E // 2, D, I))
 
@@ -178,28 +180,58 @@ def make_engine(device, s, v):
     return e
 
 
+def host_cpu():
+    """Model name and logical core count of this host."""
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count()
+
+
 def cpu_baseline_sample(seconds=15.0):
-    """The reference's own cpu64 engine (oracle/_ref) + the C restatement of the stock QEq, one core, on 648-atom
-    water single points repeated for about `seconds`."""
+    """The reference's own cpu64 engine (oracle/_ref) + the C restatement of the stock QEq CG (warm-started from the
+    previous step's solution, as the fix does), one core, on MD steps of the 24,000-atom water workload repeated for
+    about `seconds` (the cpu64 engine is single-threaded by design)."""
     from oracle.oracle import COracle, RefOracle
     text = ffield_text()
-    s = systems.water_box(6)
+    s, v = workload()
     n = len(s["type"])
     co = COracle(text, shell=12.0)
     kind = "reference" if RefOracle.available() else "port"
     ref = RefOracle(text, shell=12.0) if kind == "reference" else co
+    m = np.asarray(MASS)[s["type"]][:, None]
+    ftm2v = 1.0 / 48.88821291 / 48.88821291
+    x, vel = s["x"].copy(), v.copy()
+    sq, tq = np.zeros(n), np.zeros(n)
+
+    def grad(xx):
+        nonlocal sq, tq
+        qr = co.qeq(dict(s, x=xx), tol=QEQ["tol"], imax=QEQ["imax"], s0=sq, t0=tq)
+        sq, tq = qr["s"], qr["t"]
+        return ref.single_point(dict(s, x=xx), qr["q"])["grad"]
+
+    g = grad(x)
     count = 0
     t0 = time.perf_counter()
     while True:
-        qr = co.qeq(s, tol=QEQ["tol"], imax=QEQ["imax"])
-        ref.single_point(s, qr["q"])
+        vel -= 0.5 * DT * ftm2v * g / m
+        x = x + DT * vel
+        g = grad(x)
+        vel -= 0.5 * DT * ftm2v * g / m
         count += 1
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
+    model, ncpu = host_cpu()
     return {"value": n * count / dt, "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": "%d x (QEq + energy/forces) of 216 H2O (648 atoms), %.1f s, %s" % (count, dt,
-                      "reference cpu64 engine + C restatement of the stock QEq CG" if kind == "reference" else "C restatement")}
+            "host": {"cpu": model, "logical_cores": ncpu},
+            "sample": "%d MD steps of the 24,000-atom water workload (QEq + energy/forces + velocity Verlet), %.1f s, %s" % (
+                count, dt, "reference cpu64 engine + C restatement of the stock QEq CG" if kind == "reference" else "C restatement")}
 
 
 def e2e_run(device, s, v, steps, warmup):
@@ -294,6 +326,7 @@ def run_engine(args, rank, world, local_rank):
     phases = {k: v_ / prof_steps for k, v_ in eng.phase_times().items()}
     eng.set_timing(False)
     I = int(eng.qeq_last()["iters"].max())       # fused s/t CG iterations of the last MD step's solve
+    R = max(1, eng.qeq_refinements())            # its FP64 residual passes
     out = eng.compute(counts=True)
     P = int(out["counts"][1])
     E = int(out["counts"][2])
@@ -301,11 +334,11 @@ def run_engine(args, rank, world, local_rank):
     peak, peak_kind = measured_peak()
     dom = max(phases, key=phases.get) if phases else "qeq"
     t_dom = phases.get(dom)
-    dom_bytes = phase_model_bytes(dom, n, P, D, I)
-    impl_bytes = phase_impl_bytes(dom, n, E, D, I)
+    dom_bytes = phase_model_bytes(dom, n, P, D, I) + (12 * P * R if dom == "qeq" else 0)
+    impl_bytes = phase_impl_bytes(dom, n, E, D, I, R)
     achieved = dom_bytes / (t_dom * 1e-3) / 1e9 if t_dom else None
     achieved_impl = impl_bytes / (t_dom * 1e-3) / 1e9 if t_dom else None
-    step_bytes = model_bytes(n, P, D, I)
+    step_bytes = model_bytes(n, P, D, I, R)
     step_achieved = step_bytes / (ms_step * 1e-3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -313,7 +346,8 @@ def run_engine(args, rank, world, local_rank):
         "data": "synthetic (seeded water box, synthetic CHO force field)",
         "config": {"workload": WORKLOAD, "atoms_per_gpu": n, "systems_per_gpu": 1, "qeq_tol": QEQ["tol"], "dt_fs": DT,
                    "T_K": TEMP, "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "per-step working set larger than L2 (neighbor rows + charge matrix ~160 MB)"},
+                   "l2": "per-step working set larger than L2 (Verlet + neighbor rows + charge matrix ~230 MB)",
+                   "neighbor_skin_A": 1.0},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": PHASE_KERNEL.get(dom, dom), "phase": dom, "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
@@ -321,11 +355,11 @@ def run_engine(args, rank, world, local_rank):
                      "bytes_model": "scope-table model: 8 B per counted half pair per fused CG iteration",
                      "impl": {"bytes": impl_bytes, "achieved": achieved_impl,
                               "frac": (achieved_impl / peak) if achieved_impl else None,
-                              "note": "full rows (both directions), FP64 charge-matrix values: 12 B per row entry"},
+                              "note": "full rows (both directions); charge matrix as single-precision hi + lo"},
                      "peak_kind": peak_kind, "phase_ms_per_step": phases},
         "step_roofline": {"bytes_alg": step_bytes, "achieved": step_achieved, "peak": peak, "unit": "GB/s",
                           "frac": step_achieved / peak, "frac_of_nominal_8TBs": step_achieved / 8000.0,
-                          "N": n, "P": P, "E": E, "D": D, "I": I, "R": 0},
+                          "N": n, "P": P, "E": E, "D": D, "I": I, "R": R},
         "clocks": ck,
     }
     eng.close()
@@ -335,6 +369,8 @@ def run_engine(args, rank, world, local_rank):
             line["e2e"] = {"value": e2e_value, "unit": UNIT, **e2e_bytes}
         if not args.no_batch:
             line["batch"] = batch_run(local_rank)
+        if args.serve_requests > 0:
+            line["serve"] = serve_run(local_rank, args.serve_requests)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(args.cpu_seconds)
     elif rank == 0:
@@ -373,6 +409,7 @@ def batch_run(device, reps=20, world=1, rank=0):
         return e
 
     eng = engine_for(ss)
+    tuned = eng.autotune()
     for _ in range(3):
         eng.compute(qeq=True, cold=True)
     lat = []
@@ -386,6 +423,7 @@ def batch_run(device, reps=20, world=1, rank=0):
     batched = na / (np.median(lat_ms) * 1e-3)
     singles = [engine_for([s]) for s in ss]
     for e in singles:
+        e.set_tuning("lone_grid_min", 0)   # a lone system on its fastest charge solve (all SMs on its rows)
         e.compute(qeq=True, cold=True)
     best = None
     for _ in range(2):
@@ -401,8 +439,22 @@ def batch_run(device, reps=20, world=1, rank=0):
             "unit": "atom-evals/s", "batched": batched, "per_system": per_system, "speedup": batched / per_system,
             "latency_ms": {"p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
                            "reps": reps},
-            "qeq_iters_max": int(it.max()), "per_system_pass_ms": best * 1e3,
-            "note": "host wall clock through the C ABI (H2D of nothing, D2H of energies and gradient each evaluation)"}
+            "qeq_iters_max": int(it.max()), "per_system_pass_ms": best * 1e3, "autotuned": tuned,
+            "note": "host wall clock through the C ABI (D2H of energies and gradient each evaluation); batched: one "
+                    "captured evaluation graph over all systems; per system: one context each, lone-system CG"}
+
+
+def serve_run(device, nreq=400, rate=200.0, chunk=10):
+    """The serving form on a bounded sample: the first `nreq` requests of the Poisson stream (200 req/s, seed 4242;
+    fresh CHO systems of 100-5000 atoms; half single points, half NVT runs of 10-1000 steps at 300-3000 K), served
+    with continuous batching and HBM-budget admission. Requests are generated before the clock starts."""
+    import serving
+    reqs = serving.make_requests(nreq, rate=rate)
+    srv = serving.Server(ffield_text(), device=device, chunk=chunk)
+    st = srv.run(reqs)
+    st.update({"workload": "serve_cho_poisson%d" % int(rate), "requests_total": nreq, "rate_per_s": rate, "chunk_steps": chunk,
+               "unit": "atom-steps/s (MD atom-steps + single-point atoms)"})
+    return st
 
 
 # ---------------------------------------------------------------------------------------------------- reference arm
@@ -467,6 +519,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (C ABI) run")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batching measurement")
+    ap.add_argument("--serve-requests", type=int, default=300,
+                    help="requests of the serving sample (0 skips it; the full serving workload is 10000)")
     ap.add_argument("--qeq-passes", type=int, default=0,
                     help="profiling case: after the warm-up steps, one charge solve of exactly this many matrix passes "
                          "(tolerance 0), then print the counts and exit")
@@ -475,6 +529,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.gpus != world:
+        print("bench.py: --gpus %d but %d rank(s) were launched; start N > 1 under torchrun with --nproc-per-node N"
+              % (args.gpus, world), file=sys.stderr)
+        sys.exit(2)
     if args.impl == "reference":
         run_reference(args, rank)
         return

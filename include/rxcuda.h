@@ -110,6 +110,9 @@ int rx_qeq_matvec(rx_context* ctx, const double* v, double* y);
 /* CG iteration counts and final relative residuals (s, t per system, as rx_qeq_solve reports them) of the most recent
  * charge solve of any entry point (rx_compute with RX_COMPUTE_QEQ, rx_md_run steps, rx_qeq_solve). */
 int rx_qeq_last(const rx_context* ctx, int32_t* iters, double* rel);
+/* FP64 residual passes of the most recent single-system charge solve (the first residual, each refinement, and the
+ * final check); -1 without one. */
+int rx_qeq_refinements(rx_context* ctx);
 
 /* PairReaxFFMetal::compute (pair_reaxff_metal.cpp:412-524) for every system: energies[13*nsys] in the reference's
  * EnergyTerm order (bond, over, under, lone_pair, valence, penalty, coalition, hbond, torsion, conjugation, vdw,

@@ -1527,6 +1527,13 @@ int rx_set_systems(rx_context* ctx, int nsys, const int* natoms, const double* o
 
 int rx_num_atoms(const rx_context* ctx) { return (ctx && ctx->c) ? ctx->c->na : 0; }
 
+int rx_qeq_refinements(rx_context* ctx) {
+  if (!ctx || !ctx->c || ctx->c->host_only || !ctx->c->cg_nref.p) return -1;
+  int v = 0;
+  if (cudaMemcpy(&v, ctx->c->cg_nref.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  return v;
+}
+
 int rx_qeq_last(const rx_context* ctx, int32_t* iters, double* rel) {
   if (!ctx || !ctx->c) return RX_ERR_STATE;
   const rx::Context& c = *ctx->c;

@@ -470,6 +470,7 @@ template <bool FULL>
 __device__ inline double2 row_mv(const Dev& d, int i, double eta, const double2* v) {
   const int cnt = min(d.nbr_cnt[i], d.ncap);
   const int lane = threadIdx.x & 31;
+  const double2 vi = v[i];   // issued before the row so that its latency hides behind it
   double ys = 0.0, yt = 0.0;
   const size_t base = static_cast<size_t>(i) * d.ncap;
   for (int e0 = lane * 4; e0 < cnt; e0 += 128) {
@@ -491,7 +492,6 @@ __device__ inline double2 row_mv(const Dev& d, int i, double eta, const double2*
   }
   ys = warp_sum(ys);
   yt = warp_sum(yt);
-  const double2 vi = v[i];
   return make_double2(eta * vi.x + __shfl_sync(0xffffffffu, ys, 0), eta * vi.y + __shfl_sync(0xffffffffu, yt, 0));
 }
 
@@ -547,8 +547,8 @@ constexpr double kRefineDrop = 1e-6;
 
 __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   cg::grid_group g = cg::this_grid();
-  __shared__ double sh[32 * 8];
-  __shared__ double tot_sh[32 * 8];
+  __shared__ double sh[32 * 4];
+  __shared__ double tot_sh[32 * 4];
   const int wpb = blockDim.x >> 5;
   const int gw = blockIdx.x * wpb + (threadIdx.x >> 5);
   const int nwarps = gridDim.x * wpb;
@@ -557,7 +557,6 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   double loc[4], tot[4];
   int phase = 0;
   auto partbuf = [&]() { return a.part + static_cast<size_t>(phase & 1) * gridDim.x * 4; };
-  auto partbuf8 = [&]() { return a.part + static_cast<size_t>(phase & 1) * gridDim.x * 8; };
   double bnorm_s = 0.0, bnorm_t = 0.0, sig_s = 0.0, sig_t = 0.0;
   bool act_s = true, act_t = true, breakdown = false;
   int it_s = 1, it_t = 1, nref = 0;
@@ -590,72 +589,64 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
     if ((!act_s || it_s >= a.imax) && (!act_t || it_t >= a.imax)) break;
     const double stop_s = fmax(a.tol * bnorm_s, kRefineDrop * sqrt(sig_s));
     const double stop_t = fmax(a.tol * bnorm_t, kRefineDrop * sqrt(sig_t));
-    // ---- single-precision-matrix iterations from this residual, two grid barriers each: the product is taken of
-    // the preconditioned residual p (w = A p) and A d follows from the recurrence q = w + beta q, with
-    // d.q = p.w + beta (p.q + d.w) + beta^2 d.q from four partial sums of the same pass
-    double beta_s = 0.0, beta_t = 0.0;
-    bool first = true;   // d and q hold nothing yet (d = p, q = w)
+    // ---- single-precision-matrix iterations from this residual (d = p on entry)
+    for (int r = gw * 32 + lane; r < n; r += nwarps * 32) a.d[i0 + r] = a.p[i0 + r];
+    g.sync();
     for (;;) {
       const bool in_s = act_s && it_s < a.imax && sqrt(sig_s) > stop_s;
       const bool in_t = act_t && it_t < a.imax && sqrt(sig_t) > stop_t;
       if (!in_s && !in_t) break;
-      // w = A p ; partial p.w, p.q, d.w, d.q (q, d of the previous iteration; unused while beta = 0)
-      double l8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      // q = A d ; partial d.q
+      loc[0] = loc[1] = 0.0;
       for (int r = gw; r < n; r += nwarps) {
         const int i = i0 + r;
-        const double2 w = row_mv<false>(d, i, a.eta[i], a.p);
+        const double2 y = row_mv<false>(d, i, a.eta[i], a.d);
         if (lane == 0) {
-          a.w[i] = w;
-          const double2 pp = a.p[i];
-          l8[0] += pp.x * w.x; l8[1] += pp.y * w.y;
-          if (!first) {
-            const double2 qq = a.q[i], dd = a.d[i];
-            l8[2] += pp.x * qq.x; l8[3] += pp.y * qq.y;
-            l8[4] += dd.x * w.x; l8[5] += dd.y * w.y;
-            l8[6] += dd.x * qq.x; l8[7] += dd.y * qq.y;
-          }
+          a.q[i] = y;
+          const double2 dd = a.d[i];
+          loc[0] += dd.x * y.x; loc[1] += dd.y * y.y;
         }
-      }
-      block_partials<8>(l8, partbuf8(), sh);
-      g.sync();
-      double t8[8];
-      grid_totals<8>(partbuf8(), gridDim.x, t8, tot_sh);
-      ++phase;
-      const double dq_s = first ? t8[0] : t8[0] + beta_s * (t8[2] + t8[4]) + beta_s * beta_s * t8[6];
-      const double dq_t = first ? t8[1] : t8[1] + beta_t * (t8[3] + t8[5]) + beta_t * beta_t * t8[7];
-      const double alpha_s = in_s ? sig_s / dq_s : 0.0;
-      const double alpha_t = in_t ? sig_t / dq_t : 0.0;
-      if (!(isfinite(alpha_s) && isfinite(alpha_t))) { breakdown = true; break; }
-      // d = p + beta d ; q = w + beta q ; x += alpha d ; r -= alpha q ; p = M^-1 r ; partial r.p
-      loc[0] = loc[1] = 0.0;
-      for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
-        const int i = i0 + r;
-        const double2 pp = a.p[i], ww = a.w[i];
-        double2 dd = first ? pp : a.d[i], qq = first ? ww : a.q[i], xx = a.x[i], rr = a.r[i];
-        if (in_s) {
-          if (!first) { dd.x = pp.x + beta_s * dd.x; qq.x = ww.x + beta_s * qq.x; }
-          xx.x += alpha_s * dd.x; rr.x -= alpha_s * qq.x;
-        }
-        if (in_t) {
-          if (!first) { dd.y = pp.y + beta_t * dd.y; qq.y = ww.y + beta_t * qq.y; }
-          xx.y += alpha_t * dd.y; rr.y -= alpha_t * qq.y;
-        }
-        a.d[i] = dd;
-        a.q[i] = qq;
-        a.x[i] = xx;
-        a.r[i] = rr;
-        const double eta = a.eta[i];
-        const double2 np = make_double2(in_s ? rr.x / eta : pp.x, in_t ? rr.y / eta : pp.y);
-        a.p[i] = np;
-        loc[0] += rr.x * np.x; loc[1] += rr.y * np.y;
       }
       block_partials<2>(loc, partbuf(), sh);
       g.sync();
       grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
       ++phase;
-      if (in_s) { beta_s = tot[0] / sig_s; sig_s = tot[0]; ++it_s; }
-      if (in_t) { beta_t = tot[1] / sig_t; sig_t = tot[1]; ++it_t; }
-      first = false;
+      const double alpha_s = in_s ? sig_s / tot[0] : 0.0;
+      const double alpha_t = in_t ? sig_t / tot[1] : 0.0;
+      if (!(isfinite(alpha_s) && isfinite(alpha_t))) { breakdown = true; break; }
+      // x += alpha d ; r -= alpha q ; p = M^-1 r ; partial r.p
+      loc[0] = loc[1] = 0.0;
+      for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+        const int i = i0 + r;
+        const double2 dd = a.d[i], qq = a.q[i];
+        double2 xx = a.x[i], rr = a.r[i];
+        xx.x += alpha_s * dd.x; xx.y += alpha_t * dd.y;
+        rr.x -= alpha_s * qq.x; rr.y -= alpha_t * qq.y;
+        a.x[i] = xx;
+        a.r[i] = rr;
+        const double eta = a.eta[i];
+        const double2 pp = make_double2(rr.x / eta, rr.y / eta);
+        a.p[i] = pp;
+        loc[0] += rr.x * pp.x; loc[1] += rr.y * pp.y;
+      }
+      block_partials<2>(loc, partbuf(), sh);
+      g.sync();
+      grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
+      ++phase;
+      const double beta_s = in_s ? tot[0] / sig_s : 0.0;
+      const double beta_t = in_t ? tot[1] / sig_t : 0.0;
+      if (in_s) { sig_s = tot[0]; ++it_s; }
+      if (in_t) { sig_t = tot[1]; ++it_t; }
+      // d = p + beta d (only for the right-hand sides still iterating)
+      for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+        const int i = i0 + r;
+        const double2 pp = a.p[i];
+        double2 dd = a.d[i];
+        if (in_s) dd.x = pp.x + beta_s * dd.x;
+        if (in_t) dd.y = pp.y + beta_t * dd.y;
+        a.d[i] = dd;
+      }
+      g.sync();
     }
     if (breakdown) break;
   }
