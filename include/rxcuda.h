@@ -62,7 +62,9 @@ int rx_forcefield_params(rx_context* ctx, int* ntypes, double* chi, double* eta,
 int rx_set_control(rx_context* ctx, double bond_cut, double hbond_cut, double thb_cut, double thb_cutsq, int enobonds);
 
 /* The systems of this context. natoms[nsys]; origin[3*nsys]; box[9*nsys] lattice vectors a, b, c as rows;
- * periodic[3*nsys] (must be 1: the engine is periodic in all directions); type[NA] force-field type index;
+ * periodic[3*nsys] (NULL = all periodic) as Box::periodic (include/reaxmetal/system.hpp:29): along a non-periodic
+ * direction no image is taken and atoms are never wrapped (the engine re-fits that direction's extent at every
+ * rx_set_positions; an atom that drifts more than 50 A beyond it stops the evaluation); type[NA] force-field type index;
  * tag[NA] atom ids, unique within a system (the owner-computes tie-breaks of neighbor.cpp:295-310 use them).
  * The charge-equilibration histories (the warm start of the next solve) carry over for every atom whose tag existed
  * before the call in the system of the same index, atom count and lattice (the same system handed over again, e.g.
@@ -138,6 +140,13 @@ int rx_get_gradient(rx_context* ctx, double* grad);
  * the pair's virial from this array instead of calling virial_fdotr_compute(). Computed on the device from relative
  * positions inside each interaction, in fixed order. */
 int rx_get_virial(rx_context* ctx, double* virial);
+
+/* The 14-slot energy vector LAMMPS's `pair_style reaxff` exposes (to_lammps_pvector, src/core/energy_terms.cpp:35-72;
+ * pair_reaxff.cpp:501-514) from the 13 energies of one system: eb, ea (over + under), elp, emol (0), ev, epen, ecoa,
+ * ehb, et, eco, ew, ep, efi (0), eqeq (polarization); and the pair's eng_vdwl (every term but Coulomb and
+ * polarization) and eng_coul (Coulomb + polarization) (pair_reaxff_metal.cpp:515-519). Any output may be NULL; needs
+ * no context. */
+int rx_pvector(const double* energies13, double* pvector14, double* eng_vdwl, double* eng_coul);
 
 /* Nose-Hoover chain NVT (the LAMMPS `fix nvt temp Tstart Tstop Tdamp` the reference's examples run), velocity Verlet
  * with dt [fs]. mass[ntypes] g/mol per force-field type. Charges are re-equilibrated before every force evaluation

@@ -33,6 +33,7 @@ enum Status : int {
   ST_NEAR_OVERFLOW = 64,
   ST_CG_NOTCONV = 128,   // a system's charge solve ended above its tolerance (iteration limit)
   ST_VERLET_OVERFLOW = 256,
+  ST_NONPERIODIC_ESCAPE = 512,   // an atom left the padded extent of a non-periodic direction
 };
 // status words: [0] bits, [1] max neighbor-row count, [2] max bond count, [3] max near-row count, [4] max Verlet-row count
 constexpr int kStatusWords = 8;
@@ -48,6 +49,7 @@ struct SysInfo {
   int shift_base; // first entry of this system's lattice-shift table (S^3 entries)
   double h[3];    // distances between opposite faces (heights) along each lattice direction
   int ortho;      // lattice vectors mutually orthogonal
+  int per[3];     // periodic directions; along the others the lattice vector is the engine's own padded extent
 };
 
 struct DevFF {

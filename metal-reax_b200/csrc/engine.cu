@@ -113,6 +113,7 @@ struct Context {
   std::vector<int> hsys_of;
   std::vector<long long> htag;
   std::vector<int> htype;
+  std::vector<SysInfo> huser;   // systems as the caller gave them
   DBuf<SysInfo> sys;
   DBuf<int> sys_of, type, cell_key, cell_key_sorted, cell_atoms, atom_iota, cell_start, sys_flag;
   DBuf<double4> xs;
@@ -353,9 +354,6 @@ struct Context {
     for (int s = 0; s < n_sys; ++s) {
       if (natoms[s] <= 0) throw Error(RX_ERR_INVALID, "every system needs at least one atom");
       total += natoms[s];
-      if (periodic)
-        for (int k = 0; k < 3; ++k)
-          if (!periodic[3 * s + k]) throw Error(RX_ERR_INVALID, "the engine handles fully periodic systems only");
     }
     if (total > (1LL << 30)) throw Error(RX_ERR_INVALID, "too many atoms");
     for (long long a = 0; a < total; ++a)
@@ -376,12 +374,14 @@ struct Context {
     nsys = n_sys;
     na = static_cast<int>(total);
     hsys.assign(static_cast<size_t>(nsys), SysInfo{});
+    huser.clear();
     hsys_of.resize(static_cast<size_t>(na));
     int begin = 0;
     for (int s = 0; s < nsys; ++s) {
       SysInfo& si = hsys[static_cast<size_t>(s)];
       for (int c = 0; c < 3; ++c) si.origin[c] = origin[3 * s + c];
       for (int c = 0; c < 9; ++c) si.L[c] = box[9 * s + c];
+      for (int c = 0; c < 3; ++c) si.per[c] = periodic ? (periodic[3 * s + c] != 0) : 1;
       si.begin = begin;
       si.natoms = natoms[s];
       for (int a = 0; a < natoms[s]; ++a) hsys_of[static_cast<size_t>(begin + a)] = s;
@@ -429,6 +429,7 @@ struct Context {
       RXCU(cudaMemcpy(s_hist.p, sh.data(), sizeof(double) * sh.size(), cudaMemcpyHostToDevice));
       RXCU(cudaMemcpy(t_hist.p, th.data(), sizeof(double) * th.size(), cudaMemcpyHostToDevice));
     }
+    huser = hsys;   // the caller's lattices and origins (non-periodic directions are re-fitted from the positions)
     have_pos = false;
     have_virial = false;
     forces_valid = false;
@@ -778,6 +779,8 @@ struct Context {
   void check_status(const int* st, bool do_qeq) {
     if (st[0] & ST_SHIFT_RANGE) throw Error(RX_ERR_INVALID, "a periodic image outside the shift encoding was requested");
     if (st[0] & ST_NONFINITE) throw Error(RX_ERR_INVALID, "non-finite coordinate");
+    if (st[0] & ST_NONPERIODIC_ESCAPE)
+      throw Error(RX_ERR_INVALID, "an atom left the extent laid out for a non-periodic direction; set the positions again");
     if (st[0] & ST_SYM_MISSING) throw Error(RX_ERR_INVALID, "inconsistent bond list (a bond without its reverse)");
     if (do_qeq) {
       if (st[0] & ST_CG_BREAKDOWN) throw Error(RX_ERR_NOT_CONVERGED, "charge equilibration: CG breakdown");
@@ -910,8 +913,60 @@ struct Context {
   }
 
   // ------------------------------------------------------------------ state I/O
+  // Non-periodic directions (Box::periodic, include/reaxmetal/system.hpp:29): the engine lays the system out in a
+  // lattice whose vector along such a direction is stretched to the atoms' extent plus rc + skin + kNpPad on both
+  // sides, so that no periodic image along it comes within the cut-offs, and atoms are never wrapped along it. An atom
+  // that later leaves that extent stops the evaluation (set the positions again to re-fit).
+  static constexpr double kNpPad = 50.0;
+  void fit_nonperiodic(const double* xin, int sys_from = 0) {
+    bool any = false;
+    for (int sy = sys_from; sy < nsys; ++sy) {
+      const SysInfo& u = huser[static_cast<size_t>(sy)];
+      SysInfo& si = hsys[static_cast<size_t>(sy)];
+      if (u.per[0] && u.per[1] && u.per[2]) continue;
+      any = true;
+      // fractional coordinates in the caller's lattice
+      const double* L = u.L;
+      double R[9];
+      {
+        const double* a = L; const double* b = L + 3; const double* c = L + 6;
+        const double bc[3] = {b[1] * c[2] - b[2] * c[1], b[2] * c[0] - b[0] * c[2], b[0] * c[1] - b[1] * c[0]};
+        const double ca[3] = {c[1] * a[2] - c[2] * a[1], c[2] * a[0] - c[0] * a[2], c[0] * a[1] - c[1] * a[0]};
+        const double ab[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+        const double det = a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2];
+        if (!(det > 0) || !std::isfinite(det)) throw Error(RX_ERR_INVALID, "box must be right-handed and non-degenerate");
+        for (int k = 0; k < 3; ++k) { R[k] = bc[k] / det; R[3 + k] = ca[k] / det; R[6 + k] = ab[k] / det; }
+        const double hk[3] = {det / std::sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]), det / std::sqrt(ca[0] * ca[0] + ca[1] * ca[1] + ca[2] * ca[2]),
+                              det / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2])};
+        for (int c2 = 0; c2 < 3; ++c2) si.origin[c2] = u.origin[c2];
+        for (int c2 = 0; c2 < 9; ++c2) si.L[c2] = u.L[c2];
+        const double reach = ff.nonb_cut + skin + kNpPad;
+        for (int k = 0; k < 3; ++k) {
+          if (u.per[k]) continue;
+          double fmin = HUGE_VAL, fmax = -HUGE_VAL;
+          for (int a2 = u.begin; a2 < u.begin + u.natoms; ++a2) {
+            const double* r = xin + 3 * static_cast<size_t>(a2);
+            const double f = R[3 * k] * (r[0] - u.origin[0]) + R[3 * k + 1] * (r[1] - u.origin[1]) + R[3 * k + 2] * (r[2] - u.origin[2]);
+            if (!std::isfinite(f)) throw Error(RX_ERR_INVALID, "non-finite coordinate");
+            fmin = std::min(fmin, f);
+            fmax = std::max(fmax, f);
+          }
+          const double m = reach / hk[k];                 // margin in the caller's fractional units
+          const double scale = (fmax - fmin) + 2.0 * m;   // new length along k in units of the caller's vector
+          const double t = fmin - m;
+          for (int c2 = 0; c2 < 3; ++c2) {
+            si.origin[c2] += t * L[3 * k + c2];
+            si.L[3 * k + c2] = scale * L[3 * k + c2];
+          }
+        }
+      }
+    }
+    if (any) layout_systems();
+  }
+
   void set_positions(const double* xin) {
     require_sys();
+    fit_nonperiodic(xin);
     double4* h = stage(static_cast<size_t>(na));
     for (int a = 0; a < na; ++a) h[a] = make_double4(xin[3 * a], xin[3 * a + 1], xin[3 * a + 2], 0.0);
     RXCU(cudaMemcpyAsync(x.p, h, sizeof(double4) * na, cudaMemcpyHostToDevice, stream));
@@ -1162,6 +1217,7 @@ struct Context {
       nat[static_cast<size_t>(k)] = o.natoms;
       for (int c = 0; c < 3; ++c) org[3 * k + c] = o.origin[c];
       for (int c = 0; c < 9; ++c) bx[9 * k + c] = o.L[c];
+      for (int c = 0; c < 3; ++c) per[3 * k + c] = o.per[c];
       for (int a = 0; a < o.natoms; ++a) {
         src.push_back(o.begin + a);
         ty.push_back(htype[static_cast<size_t>(o.begin + a)]);
@@ -1214,6 +1270,11 @@ struct Context {
     if (nadd > 0) {   // new systems start with cold charge histories
       RXCU(cudaMemset(s_hist.p + 4 * nkept_atoms, 0, sizeof(double) * 4 * nadd));
       RXCU(cudaMemset(t_hist.p + 4 * nkept_atoms, 0, sizeof(double) * 4 * nadd));
+    }
+    {   // new systems with non-periodic directions are laid out around their own atoms
+      std::vector<double> xall(3 * static_cast<size_t>(na), 0.0);
+      std::copy(x_new, x_new + 3 * nadd, xall.begin() + 3 * static_cast<long long>(nkept_atoms));
+      fit_nonperiodic(xall.data(), nkeep);
     }
     // positions: new systems from the caller, kept ones gathered from the saved state
     {
@@ -1526,6 +1587,24 @@ int rx_set_systems(rx_context* ctx, int nsys, const int* natoms, const double* o
 }
 
 int rx_num_atoms(const rx_context* ctx) { return (ctx && ctx->c) ? ctx->c->na : 0; }
+
+// The LAMMPS pair-style energy vector of `pair_style reaxff` (src/core/energy_terms.cpp:35-50 mirrors
+// pair_reaxff.cpp:501-514): 14 slots eb, ea (over + under), elp, emol (0), ev, epen, ecoa, ehb, et, eco, ew, ep, efi (0),
+// eqeq (polarization); eng_vdwl = every term but Coulomb and polarization, eng_coul = Coulomb + polarization
+// (pair_reaxff_metal.cpp:515-519).
+int rx_pvector(const double* e, double* pv, double* eng_vdwl, double* eng_coul) {
+  if (!e) return RX_ERR_INVALID;
+  using namespace rx;
+  if (pv) {
+    const double v[14] = {e[E_BOND], e[E_OV] + e[E_UN], e[E_LP], 0.0, e[E_ANG], e[E_PEN], e[E_COA], e[E_HB], e[E_TOR],
+                          e[E_CON], e[E_VDW], e[E_ELE], 0.0, e[E_POL]};
+    for (int k = 0; k < 14; ++k) pv[k] = v[k];
+  }
+  if (eng_vdwl)
+    *eng_vdwl = e[E_BOND] + e[E_OV] + e[E_UN] + e[E_LP] + e[E_ANG] + e[E_PEN] + e[E_COA] + e[E_HB] + e[E_TOR] + e[E_CON] + e[E_VDW];
+  if (eng_coul) *eng_coul = e[E_ELE] + e[E_POL];
+  return RX_OK;
+}
 
 int rx_qeq_refinements(rx_context* ctx) {
   if (!ctx || !ctx->c || ctx->c->host_only || !ctx->c->cg_nref.p) return -1;

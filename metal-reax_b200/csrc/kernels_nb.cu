@@ -45,6 +45,10 @@ __global__ void k_wrap_bin(Dev d) {
   for (int k = 0; k < 3; ++k) {
     const double fl = floor(f[k]);
     if (fl != 0.0) {
+      if (!s.per[k]) {   // never wrapped: the atom has left the extent the engine laid out for this direction
+        atomicOr(d.status, ST_NONPERIODIC_ESCAPE);
+        continue;
+      }
       for (int c = 0; c < 3; ++c) r[c] -= fl * s.L[3 * k + c];
       moved = true;
     }

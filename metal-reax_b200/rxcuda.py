@@ -32,7 +32,7 @@ EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
-           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset", "rx_update_systems", "rx_md_targets", "rx_get_gradient", "rx_md_charges", "rx_autotune", "rx_set_tuning", "rx_qeq_refinements"]
+           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset", "rx_update_systems", "rx_md_targets", "rx_get_gradient", "rx_md_charges", "rx_autotune", "rx_set_tuning", "rx_qeq_refinements", "rx_pvector"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -72,7 +72,7 @@ def load():
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
         "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
         "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]), "rx_set_acks2": (_I, [_V, _V]), "rx_qeq_reset": (_I, [_V]), "rx_md_targets": (_I, [_V, _V, _V]), "rx_get_gradient": (_I, [_V, _V]), "rx_md_charges": (_I, [_V, _I]), "rx_autotune": (_I, [_V, _I, _V]),
-        "rx_set_tuning": (_I, [_V, _I, _I]), "rx_qeq_refinements": (_I, [_V]),
+        "rx_set_tuning": (_I, [_V, _I, _I]), "rx_qeq_refinements": (_I, [_V]), "rx_pvector": (_I, [_V, _V, _V, _V]),
         "rx_update_systems": (_I, [_V, _I, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V]),
     }
     for name, (res, args) in sig.items():
@@ -85,6 +85,18 @@ def load():
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+def pvector(e13):
+    """LAMMPS's 14-slot pair energy vector and (eng_vdwl, eng_coul) of one system's 13 energies (rx_pvector)."""
+    lib = load()
+    e = np.ascontiguousarray(e13, dtype=np.float64)
+    pv = np.zeros(14)
+    vdwl, coul = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    rc = lib.rx_pvector(_p(e), _p(pv), ctypes.addressof(vdwl), ctypes.addressof(coul))
+    if rc != 0:
+        raise RxError(rc, "rx_pvector")
+    return pv, vdwl.value, coul.value
 
 
 class Engine:

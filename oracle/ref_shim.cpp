@@ -14,6 +14,7 @@
 
 #include "reaxmetal/acks2.hpp"
 #include "reaxmetal/bonded.hpp"
+#include "reaxmetal/energy_terms.hpp"
 #include "reaxmetal/forcefield.hpp"
 #include "reaxmetal/neighbor.hpp"
 #include "reaxmetal/nonbonded.hpp"
@@ -144,6 +145,14 @@ int ref_single_point(const char* ffield_text, const double* origin3, const doubl
     set_err(err, errlen, e.what());
     return 1;
   }
+}
+
+// to_lammps_pvector (src/core/energy_terms.cpp:64-72) of 13 energies in EnergyTerm order.
+void ref_pvector(const double* e13, double* out14) {
+  EnergyBreakdown b;
+  for (std::size_t t = 0; t < kEnergyTermCount; ++t) b.e[t] = e13[t];
+  const auto pv = to_lammps_pvector(b);
+  for (std::size_t k = 0; k < kPvectorSize; ++k) out14[k] = pv[k];
 }
 
 }  // extern "C"

@@ -432,3 +432,16 @@ def test_acks2_pair_terms_match_oracle():
         off = eng.compute()
         assert abs(off["e"][0][12] - plain["e"][12]) <= 1e-9 * max(1.0, abs(plain["e"][12]))
     eng.close()
+
+
+@pytest.mark.parametrize("periodic", [(1, 1, 0), (0, 0, 0)], ids=["slab", "cluster"])
+def test_nonperiodic_directions_match_oracle(engine, oracle, periodic):
+    """Box::periodic (include/reaxmetal/system.hpp:29): a water slab periodic in x and y only, and a water cluster with
+    no periodic direction - no image along a non-periodic direction, atoms never wrapped along it. Same bars as the
+    single-point test, virial included."""
+    import systems
+    s = systems.water_box(4)
+    s = dict(s, periodic=np.array(periodic, dtype=np.int32), name="water192_" + "".join(map(str, periodic)))
+    _check_against_oracle(engine, oracle, s, fixed_charges(s))
+    ref = oracle.single_point(s, fixed_charges(s))
+    assert np.abs(engine.virial()[0] - ref["virial"]).max() / len(s["type"]) <= C3_ENERGY_PER_ATOM

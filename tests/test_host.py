@@ -144,3 +144,21 @@ def test_sharded_batch_over_two_ranks_gloo():
     assert sorted(merged) == list(range(6))
     for k, s in enumerate(ss):
         assert merged[k] == float(orc.single_point(s, fixed_charges(s))["e"].sum())
+
+
+def test_pvector_matches_reference_layout():
+    """rx_pvector against the reference's own to_lammps_pvector (where the reference oracle is built), and the slot
+    rules of the pair style's energy tally."""
+    import rxcuda
+    if not rxcuda.LIB_PATH.exists():
+        pytest.skip("librxcuda.so not built")
+    e = np.arange(1, 14, dtype=np.float64) * 1.5
+    pv, vdwl, coul = rxcuda.pvector(e)
+    assert pv[3] == 0.0 and pv[12] == 0.0 and pv[1] == e[1] + e[2] and pv[13] == e[12]
+    assert vdwl == pytest.approx(e[:11].sum()) and coul == pytest.approx(e[11] + e[12])
+    from oracle.oracle import RefOracle
+    if RefOracle.available():
+        lib = ctypes.CDLL(str(RefOracle.PATH))
+        out = np.zeros(14)
+        lib.ref_pvector(e.ctypes.data_as(ctypes.c_void_p), out.ctypes.data_as(ctypes.c_void_p))
+        assert np.array_equal(out, pv)
