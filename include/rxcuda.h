@@ -39,6 +39,7 @@ extern "C" {
 #define RX_COMPUTE_CENSUS 2     /* fill the decision census (include/reaxmetal/census.hpp:12-20) */
 #define RX_COMPUTE_QEQ_COLD 4     /* with RX_COMPUTE_QEQ: start the CG from s = t = 0 instead of the history extrapolation
                                      (a fresh single point; the history is then restarted from this solve) */
+#define RX_COMPUTE_PERATOM 8      /* tally per-atom energies and virials (compute pe/atom, stress/atom): rx_get_peratom */
 
 typedef struct rx_context rx_context;
 
@@ -129,6 +130,21 @@ int rx_compute(rx_context* ctx, int flags, double* energies, double* grad, int32
  * within (bcut_acks2_i + bcut_acks2_j)/2 (softness = general parameter 34) to the Coulomb and polarization energies,
  * the forces and the virial. rx_set_systems switches them off. */
 int rx_set_acks2(rx_context* ctx, const double* s_kin);
+
+/* Per-atom tallies of the last rx_compute with RX_COMPUTE_PERATOM (the step the reference's pair style falls back to
+ * cpu64 for, pair_reaxff_metal.cpp:430-433,506-510): eatom[NA] per-atom energies by the reference's rules (bond, C2,
+ * torsion and pair energies half to each end, H-bonds a third to each of donor, hydrogen and acceptor, the rest to
+ * the centre atom; images folded onto their owners), vatom[6*NA] per-atom virials (LAMMPS order), each interaction's
+ * virial kept by the atom it is centred on (pairs and BO-chain bonds half to each end) - the atoms' sum is exactly
+ * rx_get_virial, the split among atoms is not LAMMPS's v_tally fractions. Either output may be NULL. */
+int rx_get_peratom(rx_context* ctx, double* eatom, double* vatom);
+/* The bond table of the last force evaluation (publish_bonds, pair_reaxff_metal.cpp:330-368; BondTable,
+ * include/reaxmetal/bonded.hpp:32-37), for fix reaxff/bonds and reaxff/species: start[NA+1], and per bond the
+ * partner's atom index, its lattice shift shift[3*nb] (the image the bond reaches), the corrected bond order;
+ * total_bo[NA] and nlp[NA] per atom. Any output but start may be NULL. Returns the number of bonds nb; with start ==
+ * NULL or cap < nb nothing is written (call again with cap >= nb); -1 on error. */
+long long rx_get_bonds(rx_context* ctx, int* start, int* partner, int* shift, double* bo, double* total_bo, double* nlp,
+                       long long cap);
 
 /* Gradient dE/dx[3*NA] of the most recent force evaluation (rx_compute or the last step of rx_md_run). */
 int rx_get_gradient(rx_context* ctx, double* grad);

@@ -154,6 +154,8 @@ struct Dev {
   double4* fnb;          // non-bonded gradient
   double4* grad;         // result
   double* eatom;         // kTerms per atom
+  unsigned long long* pe_fix;   // per-atom energy tallies (fixed point, 2^32 units), written when pe_on
+  int pe_on;
   double* vir;           // kVir per atom: virial of the bonded interactions this atom centres (LAMMPS order xx yy zz xy xz yz)
   double* vir_h;         // kVir per atom: H-bond triples centred on this hydrogen
   double* vir_t;         // kVir per atom: torsions centred on this atom
@@ -209,6 +211,18 @@ template <class T, class U>
 __device__ inline void vir_add(double* v, const T* P, const U* g, double scale = 1.0) {
   const double p0 = P[0], p1 = P[1], p2 = P[2], g0 = g[0] * scale, g1 = g[1] * scale, g2 = g[2] * scale;
   v[0] -= p0 * g0; v[1] -= p1 * g1; v[2] -= p2 * g2; v[3] -= p0 * g1; v[4] -= p0 * g2; v[5] -= p1 * g2;
+}
+
+// Fixed-point accumulation (2^32 units): integer additions commute, so contributions added with atomics in any order
+// give the same bits every run (deterministic scatters to other atoms).
+constexpr double kFixScale = 4294967296.0;
+__device__ inline void fix_add(unsigned long long* acc, double v) {
+  atomicAdd(acc, static_cast<unsigned long long>(__double2ll_rn(v * kFixScale)));
+}
+__device__ inline double fix_value(unsigned long long v) { return static_cast<double>(static_cast<long long>(v)) * (1.0 / kFixScale); }
+// per-atom energy tally (the reference's eatom rules), when requested
+__device__ inline void pe_add(const Dev& d, int a, double e) {
+  if (d.pe_on && e != 0.0) fix_add(d.pe_fix + a, e);
 }
 
 __device__ inline double safe_exp(double v) { return exp(v > 700.0 ? 700.0 : v); }

@@ -137,7 +137,8 @@ struct Context {
   // atoms
   DBuf<double> Deltap, Deltap_boc, cdtot, W, eatom;
   DBuf<double4> dDp_self, fown, fdb, fnb, grad, fown_h, fown_t;
-  DBuf<unsigned long long> fix_h;
+  DBuf<unsigned long long> fix_h, pe_fix;
+  int pe_on = 0;
   DBuf<AtomQ> aq;
   DBuf<int> census, status;
   DBuf<long long> counters;
@@ -554,7 +555,7 @@ struct Context {
     virial.ensure(static_cast<size_t>(nsys) * kVir);
     vir.ensure(n * kVir);
     vir_nb.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
-    fown_h.ensure(n); fown_t.ensure(n); fix_h.ensure(3 * n);
+    fown_h.ensure(n); fown_t.ensure(n); fix_h.ensure(3 * n); pe_fix.ensure(n);
     cg_x.ensure(n); cg_w.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
     cg_sys.ensure(nsys); cg_rb0.ensure(n); cg_rb1.ensure(n); cg_nlive.ensure(2);
@@ -595,7 +596,7 @@ struct Context {
     d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p;
     d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
     d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.vir_nb = vir_nb.p; d.vir_h = vir_h.p; d.vir_t = vir_t.p;
-    d.fown_h = fown_h.p; d.fown_t = fown_t.p; d.fix_h = fix_h.p; d.bcdbo_h = bcdbo_h.p; d.bfn_h = bfn_h.p; d.bacc_t = bacc_t.p; d.bfn_t = bfn_t.p; d.census = census.p; d.status = status.p;
+    d.fown_h = fown_h.p; d.fown_t = fown_t.p; d.fix_h = fix_h.p; d.pe_fix = pe_fix.p; d.pe_on = pe_on; d.bcdbo_h = bcdbo_h.p; d.bfn_h = bfn_h.p; d.bacc_t = bacc_t.p; d.bfn_t = bfn_t.p; d.census = census.p; d.status = status.p;
     d.counters = counters.p;
     return d;
   }
@@ -988,7 +989,13 @@ struct Context {
       RXCU(cudaMemsetAsync(s_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
       RXCU(cudaMemsetAsync(t_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
     }
+    const int want_pe = (flags & RX_COMPUTE_PERATOM) ? 1 : 0;
+    if (want_pe != pe_on) {   // the tallies are a kernel argument: a captured evaluation holds the old value
+      pe_on = want_pe;
+      drop_graph();
+    }
     evaluate((flags & RX_COMPUTE_QEQ) != 0);
+    have_peratom = pe_on != 0;
     energy_sums();
     if (e_out) RXCU(cudaMemcpyAsync(e_out, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
     double4* g = nullptr;
@@ -1038,6 +1045,69 @@ struct Context {
     RXCU(cudaMemsetAsync(s_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
     RXCU(cudaMemsetAsync(t_hist.p, 0, sizeof(double) * 4 * static_cast<size_t>(na), stream));
     RXCU(cudaStreamSynchronize(stream));
+  }
+
+  // per-atom energies (the reference's tally rules, src/cpu/bonded.cpp:210-710, nonbonded.cpp:50-76) and per-atom
+  // virials (the virial of every interaction kept by the atom it is centred on: pairs and bonds half each) of the last
+  // rx_compute with RX_COMPUTE_PERATOM
+  bool have_peratom = false;
+  void get_peratom(double* eatom_out, double* vatom_out) {
+    require_sys();
+    if (!have_peratom) throw Error(RX_ERR_STATE, "no evaluation with RX_COMPUTE_PERATOM yet");
+    if (eatom_out) {
+      std::vector<unsigned long long> h(static_cast<size_t>(na));
+      RXCU(cudaMemcpy(h.data(), pe_fix.p, sizeof(unsigned long long) * na, cudaMemcpyDeviceToHost));
+      for (int a = 0; a < na; ++a) eatom_out[a] = static_cast<double>(static_cast<long long>(h[static_cast<size_t>(a)])) / 4294967296.0;
+    }
+    if (vatom_out) {
+      const size_t m = static_cast<size_t>(na) * kVir;
+      std::vector<double> v1(m), v2(m), v3(m), v4(m);
+      RXCU(cudaMemcpy(v1.data(), vir.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
+      RXCU(cudaMemcpy(v2.data(), vir_h.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
+      RXCU(cudaMemcpy(v3.data(), vir_t.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
+      RXCU(cudaMemcpy(v4.data(), vir_nb.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < m; ++k) vatom_out[k] = ((v1[k] + v2[k]) + v3[k]) + v4[k];
+    }
+  }
+
+  // the bond table of the last evaluation (BondTable, include/reaxmetal/bonded.hpp:32-37): bonds of atom a at
+  // [start[a], start[a+1]), partner owner index and lattice shift, corrected bond order; total bond order and lone pairs
+  // per atom. Returns the number of bonds (the capacity needed when `cap` is too small).
+  long long get_bonds(int* start, int* partner, int* shift3, double* bo, double* total_bo, double* nlp, long long cap) {
+    require_sys();
+    if (!forces_valid) throw Error(RX_ERR_STATE, "no force evaluation of the current positions");
+    const size_t n = static_cast<size_t>(na), nb = n * bcap;
+    std::vector<int> cnt(n);
+    RXCU(cudaMemcpy(cnt.data(), bcnt.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    long long total = 0;
+    for (size_t a = 0; a < n; ++a) total += std::min(cnt[a], bcap);
+    if (!start || total > cap) return total;
+    std::vector<unsigned> code(nb);
+    std::vector<double4> bov(nb);
+    std::vector<AtomQ> aqh(n);
+    RXCU(cudaMemcpy(code.data(), bcode.p, sizeof(unsigned) * nb, cudaMemcpyDeviceToHost));
+    RXCU(cudaMemcpy(bov.data(), bBO.p, sizeof(double4) * nb, cudaMemcpyDeviceToHost));
+    RXCU(cudaMemcpy(aqh.data(), aq.p, sizeof(AtomQ) * n, cudaMemcpyDeviceToHost));
+    const unsigned amask = (abits >= 32) ? 0xffffffffu : ((1u << abits) - 1u);
+    long long k = 0;
+    for (size_t a = 0; a < n; ++a) {
+      start[a] = static_cast<int>(k);
+      for (int s2 = 0; s2 < std::min(cnt[a], bcap); ++s2, ++k) {
+        const unsigned c = code[a * bcap + s2];
+        if (partner) partner[k] = static_cast<int>(c & amask);
+        if (shift3) {
+          const int sidx = static_cast<int>(c >> abits);
+          shift3[3 * k] = sidx / (S * S) - smax;
+          shift3[3 * k + 1] = (sidx / S) % S - smax;
+          shift3[3 * k + 2] = sidx % S - smax;
+        }
+        if (bo) bo[k] = bov[a * bcap + s2].x;
+      }
+      if (total_bo) total_bo[a] = aqh[a].total_bo;
+      if (nlp) nlp[a] = aqh[a].nlp;
+    }
+    start[n] = static_cast<int>(k);
+    return total;
   }
 
   void get_gradient(double* g_out) {
@@ -1703,6 +1773,17 @@ int rx_set_acks2(rx_context* ctx, const double* s_kin) {
 
 int rx_set_neighbor(rx_context* ctx, double skin) {
   return guarded(ctx, [&](rx::Context& c) { c.set_neighbor(skin); });
+}
+
+int rx_get_peratom(rx_context* ctx, double* eatom, double* vatom) {
+  return guarded(ctx, [&](rx::Context& c) { c.get_peratom(eatom, vatom); });
+}
+
+long long rx_get_bonds(rx_context* ctx, int* start, int* partner, int* shift, double* bo, double* total_bo, double* nlp,
+                       long long cap) {
+  long long out = -1;
+  const int rc = guarded(ctx, [&](rx::Context& c) { out = c.get_bonds(start, partner, shift, bo, total_bo, nlp, cap); });
+  return rc == RX_OK ? out : -1;
 }
 
 int rx_get_gradient(rx_context* ctx, double* grad) {

@@ -294,6 +294,7 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
   double fj[3] = {0, 0, 0}, cdd = 0.0;
   double e_bond = 0, e_lp = 0, e_ov = 0, e_un = 0, e_ang = 0, e_pen = 0, e_coa = 0;
   double vir[kVir] = {0, 0, 0, 0, 0, 0};
+  double pe_own = 0.0;   // per-atom tally of this atom (bond-energy and C2 halves of its partners go to them)
 
   // ---- bond energy (owned end chosen by tag order)
   {
@@ -307,7 +308,8 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
       const double pow_BOs_be2 = bo.y == 0.0 ? 0.0 : pow(bo.y, tb[TB_P_BE2]);
       const double exp_be12 = exp(tb[TB_P_BE1] * (1.0 - pow_BOs_be2));
       const double CEbo = -tb[TB_DE_S] * exp_be12 * (1.0 - tb[TB_P_BE1] * tb[TB_P_BE2] * pow_BOs_be2);
-      e_bond += -tb[TB_DE_S] * bo.y * exp_be12 - tb[TB_DE_P] * bo.z - tb[TB_DE_PP] * bo.w;
+      double eb = -tb[TB_DE_S] * bo.y * exp_be12 - tb[TB_DE_P] * bo.z - tb[TB_DE_PP] * bo.w;
+      e_bond += eb;
       double4 acc = d.bacc[b];
       acc.x += CEbo;
       acc.y -= (CEbo + tb[TB_DE_P]);
@@ -321,11 +323,16 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
         const double exphuov = exp(gp4 * (aqj.Delta + aqp.Delta));
         const double hulpov = 1.0 / (1.0 + 25.0 * exphuov);
         e_bond += gp10 * exphu * hulpov * (exphua1 + exphub1);
+        eb += gp10 * exphu * hulpov * (exphua1 + exphub1);
         acc.x += gp10 * exphu * hulpov * (exphua1 + exphub1) * (gp3 - 2.0 * gp7 * (BO - 2.50));
         cdd += -gp10 * exphu * hulpov * (gp3 * exphua1 + 25.0 * gp4 * exphuov * hulpov * (exphua1 + exphub1));
         acc.w += -gp10 * exphu * hulpov * (gp3 * exphub1 + 25.0 * gp4 * exphuov * hulpov * (exphua1 + exphub1));
       }
       d.bacc[b] = acc;
+      if (d.pe_on) {   // etally_half (src/cpu/bonded.cpp:239,246)
+        pe_own += 0.5 * eb;
+        pe_add(d, p, 0.5 * eb);
+      }
     }
   }
   // ---- lone pair + C2 correction
@@ -335,6 +342,7 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
       const double expvd2 = safe_exp(-75 * Delta_lp);
       const double inv = 1.0 / (1.0 + expvd2);
       e_lp += p_lp2 * Delta_lp * inv;
+      pe_own += p_lp2 * Delta_lp * inv;
       const double dElp = p_lp2 * inv + 75 * p_lp2 * Delta_lp * expvd2 * (inv * inv);
       cdd += dElp * aqj.dDelta_lp;
     }
@@ -349,6 +357,10 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
         if (vov3 > 3.) {
           const double dd = vov3 - 3.0;
           e_lp += p_lp3 * (dd * dd);
+          if (d.pe_on) {   // etally_half(i, nbr, c2.e) (src/cpu/bonded.cpp:275)
+            pe_own += 0.5 * p_lp3 * (dd * dd);
+            pe_add(d, p, 0.5 * p_lp3 * (dd * dd));
+          }
           d.bacc[b].x += 2. * p_lp3 * (vov3 - 3.);
           cdd += 2. * p_lp3 * (vov3 - 3.) * (-1. - 0.16 * pow(Di, 3.));
         }
@@ -556,6 +568,7 @@ __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
   for (int c = 0; c < kVir; ++c) d.vir[static_cast<size_t>(j) * kVir + c] = vir[c];   // first writer of the step
   double* ea = d.eatom + static_cast<size_t>(j) * kTerms;
   ea[E_BOND] = e_bond; ea[E_OV] = e_ov; ea[E_UN] = e_un; ea[E_LP] = e_lp;
+  pe_add(d, j, pe_own + e_ov + e_un + e_ang + e_pen + e_coa);   // over/under and the angle sets stay with j
   ea[E_ANG] = e_ang; ea[E_PEN] = e_pen; ea[E_COA] = e_coa;
 }
 
@@ -599,13 +612,6 @@ __device__ inline bool hbond_triple(const DevFF& ff, const HbDonor& dn, int tj, 
   o.CEhb2 = -p1 / 2.0f * (1.0f - exp_hb2) * exp_hb3 * cos_xhz1;
   o.CEhb3 = -p3 * (-r0 / (r_jk * r_jk) + 1.0f / r0) * o.e;
   return true;
-}
-
-// Fixed-point accumulation (2^32 units): integer additions commute, so contributions added with atomics in any order
-// give the same bits every run - the deterministic scatter of the acceptor gradients.
-constexpr double kFixScale = 4294967296.0;
-__device__ inline void fix_add(unsigned long long* acc, double v) {
-  atomicAdd(acc, static_cast<unsigned long long>(__double2ll_rn(v * kFixScale)));
 }
 
 // One warp per hydrogen j (p_hbond = 1): for every donor bond of j, the lanes walk j's near row for acceptors
@@ -680,6 +686,10 @@ __global__ void __launch_bounds__(256) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
       if (!hbond_triple(ff, dn, tj, type_k, d.tag[ka], vk, r_jk, o)) continue;
       ++ntrip;
       e += o.e;
+      if (d.pe_on) {   // a third to each of donor, hydrogen, acceptor (src/cpu/bonded.cpp:704)
+        pe_add(d, static_cast<int>(d.bcode[bi] & d.amask), o.e / 3.0);
+        pe_add(d, ka, o.e / 3.0);
+      }
       c1 += o.CEhb1;
       fi0 += o.CEhb2 * o.dti[0]; fi1 += o.CEhb2 * o.dti[1]; fi2 += o.CEhb2 * o.dti[2];
       const float c3 = -o.CEhb3 / r_jk;
@@ -708,6 +718,7 @@ __global__ void __launch_bounds__(256) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
     for (int c = 0; c < kVir; ++c) d.vir_h[static_cast<size_t>(j) * kVir + c] = vir[c];
     d.eatom[static_cast<size_t>(j) * kTerms + E_HB] = e;
     d.census[3 * d.na + j] = ntrip;
+    pe_add(d, j, e / 3.0);
   }
 }
 
@@ -733,7 +744,7 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
     d.bacc_t[base + c] = make_double4(0, 0, 0, 0);
     d.bfn_t[base + c] = make_double4(0, 0, 0, 0);
   }
-  double fj[3] = {0, 0, 0}, cdd = 0.0, e_tor = 0.0, e_con = 0.0;
+  double fj[3] = {0, 0, 0}, cdd = 0.0, e_tor = 0.0, e_con = 0.0, pe_tor_own = 0.0;
   double vir[kVir] = {0, 0, 0, 0, 0, 0};
   int ntor = 0;
   const double Delta_j = d.aq[j].Delta_boc;
@@ -882,6 +893,11 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
         const double CEtors9 = fn10 * sin_ijk * sin_jkl * (0.5 * V1 - 2.0 * V2 * exp_tor1 * cos_omega + 1.5 * V3 * (cos2omega + 2.0 * (cos_omega * cos_omega)));
         const double fn12 = exp_cot2_ij * exp_cot2_jk * exp_cot2_kl;
         e_con += p_cot1 * fn12 * (1.0 + ((cos_omega * cos_omega) - 1.0) * sin_ijk * sin_jkl);
+        if (d.pe_on) {   // etally_half(j, k, e_tor + e_con) (src/cpu/bonded.cpp:637)
+          const double et = fn10 * sin_ijk * sin_jkl * CV + p_cot1 * fn12 * (1.0 + ((cos_omega * cos_omega) - 1.0) * sin_ijk * sin_jkl);
+          pe_tor_own += 0.5 * et;
+          pe_add(d, ka, 0.5 * et);
+        }
         const double Cconj = -2.0 * fn12 * p_cot1 * p_cot2 * (1.0 + ((cos_omega * cos_omega) - 1.0) * sin_ijk * sin_jkl);
         const double CEconj1 = Cconj * (BOA_ij - 1.5e0), CEconj2 = Cconj * (BOA_jk - 1.5e0), CEconj3 = Cconj * (BOA_kl - 1.5e0);
         const double CEconj4 = -p_cot1 * fn12 * ((cos_omega * cos_omega) - 1.0) * sin_jkl * tan_ijk_i;
@@ -922,6 +938,7 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
   }
   d.fown_t[j] = make_double4(fj[0], fj[1], fj[2], cdd);
   for (int c = 0; c < kVir; ++c) d.vir_t[static_cast<size_t>(j) * kVir + c] = vir[c];
+  pe_add(d, j, pe_tor_own);
   d.eatom[static_cast<size_t>(j) * kTerms + E_TOR] = e_tor;
   d.eatom[static_cast<size_t>(j) * kTerms + E_CON] = e_con;
   d.census[2 * d.na + j] = ntor;
@@ -1012,8 +1029,7 @@ __global__ void k_force_final(Dev d) {
   const size_t base = static_cast<size_t>(a) * d.bcap;
   const double4 f1 = d.fown[a], fh = d.fown_h[a], ft = d.fown_t[a], f2 = d.fdb[a], f3 = d.fnb[a];
   double g[3] = {f1.x + fh.x + ft.x + f2.x + f3.x, f1.y + fh.y + ft.y + f2.y + f3.y, f1.z + fh.z + ft.z + f2.z + f3.z};
-  for (int c = 0; c < 3; ++c)   // H-bond acceptor gradient, fixed point
-    g[c] += static_cast<double>(static_cast<long long>(d.fix_h[3 * static_cast<size_t>(a) + c])) * (1.0 / kFixScale);
+  for (int c = 0; c < 3; ++c) g[c] += fix_value(d.fix_h[3 * static_cast<size_t>(a) + c]);   // H-bond acceptor gradient
   for (int k = 0; k < nb; ++k) {
     const size_t b = base + k;
     const int p = static_cast<int>(d.bcode[b] & d.amask);

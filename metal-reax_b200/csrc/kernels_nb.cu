@@ -201,6 +201,7 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
   if (lane < 3) d.fix_h[3 * static_cast<size_t>(warp) + lane] = 0ull;   // the H-bond acceptor accumulators of this step
+  if (lane == 3 && d.pe_on) d.pe_fix[warp] = 0ull;
   if (lists_failed(d)) return;
   const int i = warp;
   const SysInfo s = d.sys[d.sys_of[i]];
@@ -298,7 +299,7 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
   const float qi = static_cast<float>(d.q[i]);
   const long long tag_i = d.tag[i];
   const int center = (d.S * d.S * d.S - 1) / 2;
-  double gx = 0, gy = 0, gz = 0, ev = 0, ee = 0;
+  double gx = 0, gy = 0, gz = 0, ev = 0, ee = 0, ehalf = 0;
   double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;   // pair virial, half per directed entry
   int counted = 0;
   for (int e = lane; e < cnt; e += 32) {
@@ -381,9 +382,11 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
       ee += static_cast<double>(e_ele);
       ++counted;
     }
+    ehalf += 0.5 * (static_cast<double>(e_vdW) + static_cast<double>(e_ele));   // per-atom tally: half of every pair
   }
   gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); ev = warp_sum(ev); ee = warp_sum(ee);
   v0 = warp_sum(v0); v1 = warp_sum(v1); v2 = warp_sum(v2); v3 = warp_sum(v3); v4 = warp_sum(v4); v5 = warp_sum(v5);
+  if (d.pe_on) ehalf = warp_sum(ehalf);
   for (int o = 16; o > 0; o >>= 1) counted += __shfl_xor_sync(0xffffffffu, counted, o);
   if (lane == 0) {
     d.fnb[i] = make_double4(gx, gy, gz, 0.0);
@@ -393,6 +396,7 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] = ee;
     const double chi = ff.sb[ti * SB_N + SB_CHI], eta = ff.sb[ti * SB_N + SB_ETA], qd = d.q[i];
     d.eatom[static_cast<size_t>(i) * kTerms + E_POL] = 23.02 * (chi * qd + (eta / 2.) * (qd * qd));
+    if (d.pe_on) pe_add(d, i, ehalf + 23.02 * (chi * qd + (eta / 2.) * (qd * qd)));
     d.census[4 * d.na + i] = counted;
   }
 }
@@ -417,7 +421,7 @@ __global__ void k_acks2(Dev d, DevFF ff, const double* s_kin) {
   const double bcut_i = ff.sb[ti * SB_N + SB_BCUT_ACKS2], s_i = s_kin[i];
   const long long tag_i = d.tag[i];
   const int center = (d.S * d.S * d.S - 1) / 2;
-  double gx = 0, gy = 0, gz = 0, ee = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
+  double gx = 0, gy = 0, gz = 0, ee = 0, eh2 = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
   for (int e = lane; e < cnt; e += 32) {
     const unsigned code = d.nbr[static_cast<size_t>(i) * d.ncap + e];
     const int j = static_cast<int>(code & d.amask);
@@ -452,8 +456,10 @@ __global__ void k_acks2(Dev d, DevFF ff, const double* s_kin) {
       }
     }
     if (count) ee += -0.5 * 23.02 * bs * effpot * effpot;
+    eh2 += 0.5 * (-0.5 * 23.02 * bs * effpot * effpot);
   }
   gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); ee = warp_sum(ee);
+  if (d.pe_on) eh2 = warp_sum(eh2);
   v0 = warp_sum(v0); v1 = warp_sum(v1); v2 = warp_sum(v2); v3 = warp_sum(v3); v4 = warp_sum(v4); v5 = warp_sum(v5);
   if (lane == 0) {
     double4 f = d.fnb[i];
@@ -461,6 +467,7 @@ __global__ void k_acks2(Dev d, DevFF ff, const double* s_kin) {
     d.fnb[i] = f;
     d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] += ee;
     d.eatom[static_cast<size_t>(i) * kTerms + E_POL] += 23.02 * d.q[i] * s_i;
+    if (d.pe_on) pe_add(d, i, eh2 + 23.02 * d.q[i] * s_i);
     double* vi = d.vir_nb + static_cast<size_t>(i) * kVir;
     vi[0] += v0; vi[1] += v1; vi[2] += v2; vi[3] += v3; vi[4] += v4; vi[5] += v5;
   }

@@ -26,13 +26,15 @@ CENSUS = ["bonds", "angle_sets", "torsions", "hbonds", "nonbonded", "sbo_region"
 RX_COMPUTE_QEQ = 1
 RX_COMPUTE_CENSUS = 2
 RX_COMPUTE_QEQ_COLD = 4
+RX_COMPUTE_PERATOM = 8
 TUNE = {"pairs_tpb": 1, "bonds_tpb": 2, "nonbonded_tpb": 3, "hbond_tpb": 4, "atom_tpb": 5, "lone_grid_min": 6}
 STATUS = {0: "ok", 1: "invalid", 2: "ffield", 3: "capacity", 4: "cuda", 5: "not_converged", 6: "state", 7: "timeout"}
 EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_forcefield_dump", "rx_forcefield_params",
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
-           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset", "rx_update_systems", "rx_md_targets", "rx_get_gradient", "rx_md_charges", "rx_autotune", "rx_set_tuning", "rx_qeq_refinements", "rx_pvector"]
+           "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset", "rx_update_systems", "rx_md_targets", "rx_get_gradient", "rx_md_charges", "rx_autotune", "rx_set_tuning", "rx_qeq_refinements", "rx_pvector", "rx_get_peratom",
+           "rx_get_bonds"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -72,7 +74,8 @@ def load():
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
         "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
         "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]), "rx_set_acks2": (_I, [_V, _V]), "rx_qeq_reset": (_I, [_V]), "rx_md_targets": (_I, [_V, _V, _V]), "rx_get_gradient": (_I, [_V, _V]), "rx_md_charges": (_I, [_V, _I]), "rx_autotune": (_I, [_V, _I, _V]),
-        "rx_set_tuning": (_I, [_V, _I, _I]), "rx_qeq_refinements": (_I, [_V]), "rx_pvector": (_I, [_V, _V, _V, _V]),
+        "rx_set_tuning": (_I, [_V, _I, _I]), "rx_qeq_refinements": (_I, [_V]), "rx_pvector": (_I, [_V, _V, _V, _V]), "rx_get_peratom": (_I, [_V, _V, _V]),
+        "rx_get_bonds": (ctypes.c_longlong, [_V, _V, _V, _V, _V, _V, _V, ctypes.c_longlong]),
         "rx_update_systems": (_I, [_V, _I, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V]),
     }
     for name, (res, args) in sig.items():
@@ -236,12 +239,13 @@ class Engine:
         return q
 
     # ---- evaluation
-    def compute(self, qeq=False, census=False, counts=False, cold=False):
+    def compute(self, qeq=False, census=False, counts=False, cold=False, peratom=False):
         e = np.zeros(13 * self.nsys)
         g = np.zeros(3 * self.na)
         cen = np.zeros(7 * self.na, dtype=np.int32) if census else None
         cnt = np.zeros(4, dtype=np.int64) if counts else None
-        flags = (RX_COMPUTE_QEQ if qeq else 0) | (RX_COMPUTE_CENSUS if census else 0) | (RX_COMPUTE_QEQ_COLD if cold else 0)
+        flags = (RX_COMPUTE_QEQ if qeq else 0) | (RX_COMPUTE_CENSUS if census else 0) | (RX_COMPUTE_QEQ_COLD if cold else 0) | \
+            (RX_COMPUTE_PERATOM if peratom else 0)
         self._check(self.lib.rx_compute(self.h, flags, _p(e), _p(g), _p(cen), _p(cnt)))
         out = {"e": e.reshape(self.nsys, 13), "grad": g.reshape(-1, 3)}
         if census:
@@ -255,6 +259,29 @@ class Engine:
         sk = None if s_kin is None else np.ascontiguousarray(s_kin, dtype=np.float64)
         self._check(self.lib.rx_set_acks2(self.h, _p(sk)))
         self._s_kin = sk
+
+    def peratom(self):
+        """Per-atom energies (n,) and virials (n, 6) of the last compute(peratom=True)."""
+        e = np.zeros(self.na)
+        v = np.zeros(6 * self.na)
+        self._check(self.lib.rx_get_peratom(self.h, _p(e), _p(v)))
+        return e, v.reshape(-1, 6)
+
+    def bonds(self):
+        """The bond table of the last evaluation: start (n+1,), partner, shift (nb, 3), bo, total_bo, nlp."""
+        nb = self.lib.rx_get_bonds(self.h, None, None, None, None, None, None, 0)
+        if nb < 0:
+            raise RxError(6, self.lib.rx_last_error(self.h).decode())
+        start = np.zeros(self.na + 1, dtype=np.int32)
+        partner = np.zeros(max(nb, 1), dtype=np.int32)
+        shift = np.zeros(3 * max(nb, 1), dtype=np.int32)
+        bo = np.zeros(max(nb, 1))
+        tbo, nlp = np.zeros(self.na), np.zeros(self.na)
+        got = self.lib.rx_get_bonds(self.h, _p(start), _p(partner), _p(shift), _p(bo), _p(tbo), _p(nlp), nb)
+        if got != nb:
+            raise RxError(6, self.lib.rx_last_error(self.h).decode())
+        return {"start": start, "partner": partner[:nb], "shift": shift[:3 * nb].reshape(-1, 3), "bo": bo[:nb],
+                "total_bo": tbo, "nlp": nlp}
 
     def gradient(self):
         """dE/dx of the last force evaluation (rx_compute or the last MD step)."""

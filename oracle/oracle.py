@@ -170,6 +170,30 @@ class RefOracle:
         self.lib.ref_table_dump.argtypes = [ctypes.c_char_p, _I, ctypes.c_char_p, ctypes.c_long]
         self.lib.ref_table_dump.restype = ctypes.c_long
 
+    def peratom(self, system, q, cap=1 << 22):
+        """Per-atom energies and virials (folded onto owners) and the bond table (partners as owner indices)."""
+        n = len(system["type"])
+        arrs = [np.ascontiguousarray(system[k], dtype=dt) for k, dt in
+                (("origin", np.float64), ("box", np.float64), ("periodic", np.int32), ("x", np.float64), ("type", np.int32),
+                 ("tag", np.int64))]
+        qq = np.ascontiguousarray(q, dtype=np.float64)
+        e, v = np.zeros(n), np.zeros(6 * n)
+        start = np.zeros(n + 1, dtype=np.int32)
+        partner = np.zeros(cap, dtype=np.int32)
+        bo = np.zeros(cap)
+        tbo, nlp = np.zeros(n), np.zeros(n)
+        err = ctypes.create_string_buffer(512)
+        f = self.lib.ref_peratom
+        f.restype = ctypes.c_longlong
+        f.argtypes = [ctypes.c_char_p] + [_V] * 3 + [_I] + [_V] * 4 + [_D] + [_V] * 5 + [ctypes.c_longlong] + [_V] * 2 + \
+                     [ctypes.c_char_p, _I]
+        nb = f(self.text, _ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), n, _ptr(arrs[3]), _ptr(arrs[4]), _ptr(arrs[5]),
+               _ptr(qq), self.shell, _ptr(e), _ptr(v), _ptr(start), _ptr(partner), _ptr(bo), cap, _ptr(tbo), _ptr(nlp), err, 512)
+        if nb < 0:
+            raise RuntimeError("reference: " + err.value.decode())
+        return {"eatom": e, "vatom": v.reshape(n, 6), "start": start, "partner": partner[:nb], "bo": bo[:nb],
+                "total_bo": tbo, "nlp": nlp}
+
     def table_dump(self, portable=False):
         buf = ctypes.create_string_buffer(1 << 22)
         m = self.lib.ref_table_dump(self.text, 1 if portable else 0, buf, len(buf))

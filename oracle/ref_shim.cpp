@@ -147,6 +147,66 @@ int ref_single_point(const char* ffield_text, const double* origin3, const doubl
   }
 }
 
+// The per-atom tallies and the bond table of the cpu64 engine (BondedOptions::per_atom / bond_table,
+// NonbondedOptions::per_atom): eatom[n] and vatom[6n] folded from owned + ghost atoms onto the owners (the reverse
+// communication of LAMMPS); the bond table of the owned atoms with the partners mapped to their owners
+// (bond_start[n+1], bond_partner / bond_bo of at most bond_cap bonds, total_bo[n], nlp[n]). Returns the number of bonds,
+// or -1 with a message in err.
+long long ref_peratom(const char* ffield_text, const double* origin3, const double* box9, const int* periodic3, int n,
+                      const double* x, const int* type, const long long* tag, const double* q, double shell, double* eatom,
+                      double* vatom, int* bond_start, int* bond_partner, double* bond_bo, long long bond_cap, double* total_bo,
+                      double* nlp, char* err, int errlen) {
+  try {
+    const ForceField ff = parse_force_field(ffield_text, "ffield");
+    ControlParams ctl;
+    NeighborCutoffs cut;
+    cut.nonb = ff.file_control().nonb_cut;
+    cut.bond = ctl.bond_cut;
+    cut.hbond = ctl.hbond_cut;
+    Box box;
+    for (int c = 0; c < 3; ++c) box.origin[static_cast<std::size_t>(c)] = origin3[c];
+    for (int v = 0; v < 3; ++v)
+      for (int c = 0; c < 3; ++c) box.vectors[static_cast<std::size_t>(v)][static_cast<std::size_t>(c)] = box9[3 * v + c];
+    for (int d = 0; d < 3; ++d) box.periodic[static_cast<std::size_t>(d)] = periodic3[d] != 0;
+    std::vector<double> xs(x, x + 3 * static_cast<std::size_t>(n));
+    std::vector<int> ty(type, type + n);
+    std::vector<std::int64_t> tg(tag, tag + n);
+    ExpandOptions eo;
+    eo.shell = shell > 0 ? shell : cut.required_shell();
+    const AtomSet a = expand_images(box, xs, ty, tg, eo);
+    const FarList f = build_far_list(a, cut);
+    BondedOptions bo;
+    bo.per_atom = true;
+    bo.bond_table = true;
+    const BondedResult r = compute_bonded_core(ff, ctl, a, f, bo);
+    NonbondedOptions no;
+    no.per_atom = true;
+    std::vector<double> qv(q, q + n);
+    const NonbondedResult nb = compute_nonbonded_core(ff, cut, a, f, qv, no);
+    for (int i = 0; i < n; ++i) eatom[i] = 0.0;
+    for (int i = 0; i < 6 * n; ++i) vatom[i] = 0.0;
+    for (std::size_t i = 0; i < a.nall(); ++i) {
+      const std::size_t o = static_cast<std::size_t>(a.owner[i]);
+      eatom[o] += r.eatom[i] + nb.eatom[i];
+      for (std::size_t c = 0; c < 6; ++c) vatom[6 * o + c] += r.vatom[i][c] + nb.vatom[i][c];
+    }
+    const BondTable& t = r.table;
+    const long long nbonds = t.start.empty() ? 0 : t.start.back();
+    if (bond_start && nbonds <= bond_cap) {
+      for (int i = 0; i <= n; ++i) bond_start[i] = t.start[static_cast<std::size_t>(i)];
+      for (long long k = 0; k < nbonds; ++k) {
+        bond_partner[k] = a.owner[static_cast<std::size_t>(t.nbr[static_cast<std::size_t>(k)])];
+        bond_bo[k] = t.bo[static_cast<std::size_t>(k)];
+      }
+      for (int i = 0; i < n; ++i) { total_bo[i] = t.total_bo[static_cast<std::size_t>(i)]; nlp[i] = t.nlp[static_cast<std::size_t>(i)]; }
+    }
+    return nbonds;
+  } catch (const std::exception& e) {
+    set_err(err, errlen, e.what());
+    return -1;
+  }
+}
+
 // to_lammps_pvector (src/core/energy_terms.cpp:64-72) of 13 energies in EnergyTerm order.
 void ref_pvector(const double* e13, double* out14) {
   EnergyBreakdown b;

@@ -445,3 +445,31 @@ def test_nonperiodic_directions_match_oracle(engine, oracle, periodic):
     _check_against_oracle(engine, oracle, s, fixed_charges(s))
     ref = oracle.single_point(s, fixed_charges(s))
     assert np.abs(engine.virial()[0] - ref["virial"]).max() / len(s["type"]) <= C3_ENERGY_PER_ATOM
+
+
+def test_peratom_energies_and_bond_table_match_reference(engine):
+    """RX_COMPUTE_PERATOM and rx_get_bonds against the reference's own per-atom tallies and bond table (cpu64 with
+    BondedOptions::per_atom / bond_table, ghosts folded onto owners): per-atom energies within 1e-4 kcal/mol of each
+    atom (FP32 pair and H-bond terms), summing to the total; per-atom virials summing to the global virial; every
+    atom's bonds (partner, corrected bond order to 1e-9), total bond order and lone pairs the same."""
+    from oracle.oracle import RefOracle
+    if not RefOracle.available():
+        pytest.skip("reference oracle not built here")
+    for s in small_systems()[:3]:
+        q = fixed_charges(s)
+        ref = RefOracle(ffield_text(), shell=15.0).peratom(s, q)
+        engine.set_systems([s])
+        engine.set_charges(q)
+        out = engine.compute(peratom=True)
+        ea, va = engine.peratom()
+        assert np.abs(ea - ref["eatom"]).max() <= 1e-4, (s["name"], np.abs(ea - ref["eatom"]).max())
+        assert abs(ea.sum() - out["e"][0].sum()) <= 1e-6 * max(1.0, abs(out["e"][0].sum()))
+        assert np.abs(va.sum(0) - engine.virial()[0]).max() <= 1e-6 * max(1.0, np.abs(engine.virial()[0]).max())
+        b = engine.bonds()
+        n = len(s["type"])
+        assert np.abs(b["total_bo"] - ref["total_bo"]).max() <= 1e-9 and np.abs(b["nlp"] - ref["nlp"]).max() <= 1e-9
+        for a in range(n):
+            mine = sorted(zip(b["partner"][b["start"][a]:b["start"][a + 1]], b["bo"][b["start"][a]:b["start"][a + 1]]))
+            theirs = sorted(zip(ref["partner"][ref["start"][a]:ref["start"][a + 1]], ref["bo"][ref["start"][a]:ref["start"][a + 1]]))
+            assert [p for p, _ in mine] == [p for p, _ in theirs], (s["name"], a)
+            assert np.allclose([v for _, v in mine], [v for _, v in theirs], rtol=0, atol=1e-9), (s["name"], a)
