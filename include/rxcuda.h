@@ -59,6 +59,10 @@ long rx_forcefield_dump(rx_context* ctx, int portable, char* out, long outlen);
  * file value. Arrays of ntypes entries (0-based type index). */
 int rx_forcefield_params(rx_context* ctx, int* ntypes, double* chi, double* eta, double* gamma, double* mass);
 
+/* ForceField::match_element as pair_coeff uses it (pair_reaxff_metal.cpp:121-134): the force-field type index of an
+ * element symbol (case-insensitive, first three characters), or -1 when the file has no such element. */
+int rx_forcefield_element(rx_context* ctx, const char* symbol);
+
 /* ControlParams (include/reaxmetal/forcefield.hpp:73-78) and the `enobonds` pair_style keyword (bonded.hpp:25). */
 int rx_set_control(rx_context* ctx, double bond_cut, double hbond_cut, double thb_cut, double thb_cutsq, int enobonds);
 

@@ -39,16 +39,33 @@ def _compile(src, verbose):
     return obj
 
 
+LAMMPS_SRC = [PKG / "lammps" / "rx_lammps.cpp", PKG / "lammps" / "rx_lammps_capi.cpp"]
+LAMMPS_OUT = PKG / "librxlammps.so"
+
+
+def build_lammps_bridge():
+    """librxlammps.so: the LAMMPS-side bridge of the CUDA backend (plain C++ over librxcuda.so's C ABI)."""
+    deps = LAMMPS_SRC + [PKG / "lammps" / "rx_lammps.hpp", REPO / "include" / "rxcuda.h", OUT]
+    if LAMMPS_OUT.exists() and all(LAMMPS_OUT.stat().st_mtime >= p.stat().st_mtime for p in deps):
+        return LAMMPS_OUT
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", str(LAMMPS_OUT)] + [str(p) for p in LAMMPS_SRC] + \
+          ["-L" + str(PKG), "-lrxcuda", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("bridge build failed:\n%s%s" % (r.stdout, r.stderr))
+    return LAMMPS_OUT
+
+
 def build(verbose=False):
     BUILD.mkdir(exist_ok=True)
     with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
-    if OUT.exists() and all(OUT.stat().st_mtime >= o.stat().st_mtime for o in objs):
-        return OUT
-    cmd = [NVCC] + ARCH + ["-shared", "-o", str(OUT)] + [str(o) for o in objs] + ["-lcudart"]
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if r.returncode != 0:
-        raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))
+    if not (OUT.exists() and all(OUT.stat().st_mtime >= o.stat().st_mtime for o in objs)):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", str(OUT)] + [str(o) for o in objs] + ["-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))
+    build_lammps_bridge()
     return OUT
 
 

@@ -1647,6 +1647,19 @@ int rx_forcefield_params(rx_context* ctx, int* ntypes, double* chi, double* eta,
   });
 }
 
+int rx_forcefield_element(rx_context* ctx, const char* symbol) {
+  int out = -1;
+  const int rc = guarded(ctx, [&](rx::Context& c) {
+    c.require_ff();
+    if (!symbol) throw rx::Error(RX_ERR_INVALID, "null element symbol");
+    std::string key;
+    for (const char* p = symbol; *p && key.size() < 3; ++p) key.push_back(static_cast<char>(toupper(static_cast<unsigned char>(*p))));
+    for (size_t k = 0; k < c.ff.names.size(); ++k)
+      if (c.ff.names[k] == key) { out = static_cast<int>(k); break; }
+  });
+  return rc == RX_OK ? out : -1;
+}
+
 int rx_set_control(rx_context* ctx, double bond_cut, double hbond_cut, double thb_cut, double thb_cutsq, int enobonds) {
   return guarded(ctx, [&](rx::Context& c) { c.set_control(bond_cut, hbond_cut, thb_cut, thb_cutsq, enobonds); });
 }

@@ -34,7 +34,7 @@ EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
            "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset", "rx_update_systems", "rx_md_targets", "rx_get_gradient", "rx_md_charges", "rx_autotune", "rx_set_tuning", "rx_qeq_refinements", "rx_pvector", "rx_get_peratom",
-           "rx_get_bonds"]
+           "rx_get_bonds", "rx_forcefield_element"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -74,7 +74,7 @@ def load():
         "rx_qeq_solve_static": (_I, [_I, _V, _V, _V, _V, _V, _V, _V, _V, _D, _I, _V, _V, _V, ctypes.c_char_p, _I]),
         "rx_set_capacities": (_I, [_V, _I, _I, _I]), "rx_get_capacities": (_I, [_V, _V]),
         "rx_qeq_last": (_I, [_V, _V, _V]), "rx_get_virial": (_I, [_V, _V]), "rx_set_neighbor": (_I, [_V, _D]), "rx_qeq_cg": (_I, [_V, _V, _V, _V, _V, _V, _V]), "rx_set_acks2": (_I, [_V, _V]), "rx_qeq_reset": (_I, [_V]), "rx_md_targets": (_I, [_V, _V, _V]), "rx_get_gradient": (_I, [_V, _V]), "rx_md_charges": (_I, [_V, _I]), "rx_autotune": (_I, [_V, _I, _V]),
-        "rx_set_tuning": (_I, [_V, _I, _I]), "rx_qeq_refinements": (_I, [_V]), "rx_pvector": (_I, [_V, _V, _V, _V]), "rx_get_peratom": (_I, [_V, _V, _V]),
+        "rx_set_tuning": (_I, [_V, _I, _I]), "rx_qeq_refinements": (_I, [_V]), "rx_pvector": (_I, [_V, _V, _V, _V]), "rx_get_peratom": (_I, [_V, _V, _V]), "rx_forcefield_element": (_I, [_V, ctypes.c_char_p]),
         "rx_get_bonds": (ctypes.c_longlong, [_V, _V, _V, _V, _V, _V, _V, ctypes.c_longlong]),
         "rx_update_systems": (_I, [_V, _I, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V]),
     }
