@@ -139,6 +139,9 @@ struct Dev {
   double4* bacc_t;       // torsion: Cdbo, Cdbopi, -, CdDelta to the partner
   double4* bfn_t;        // torsion: gradient on the partner (xyz)
   double4* Tl;           // torsion: per (central slot, position in the far atom's slots): gradient xyz, Cdbo (w)
+  double4* Ti;           // torsion: per (central slot, position in the central atom's slots): gradient on i, Cdbo of i-j
+  double4* Tsum;         // torsion: per central slot, 2 entries: central gradient + CdDelta; e_tor, e_con, count
+  double* Tvir;          // torsion: per central slot, kVir virial components
   // atoms
   double* Deltap;
   double* Deltap_boc;

@@ -132,7 +132,8 @@ struct Context {
   DBuf<int> nbr_cnt, bsym, bcnt, near_cnt, vcnt;
   DBuf<double4> shifts, xref;
   DBuf<float> hhi, hlo;
-  DBuf<double4> bdv, bBO, bdBOp, bdlnpi, bdlnpi2, bC0, bC1, bC2, bacc, bfn, Tl, bfn_h, bacc_t, bfn_t;
+  DBuf<double4> bdv, bBO, bdBOp, bdlnpi, bdlnpi2, bC0, bC1, bC2, bacc, bfn, Tl, Ti, Tsum, bfn_h, bacc_t, bfn_t;
+  DBuf<double> Tvir;
   DBuf<double> bcdbo_h;
   // atoms
   DBuf<double> Deltap, Deltap_boc, cdtot, W, eatom;
@@ -576,6 +577,9 @@ struct Context {
     bC0.ensure(nb); bC1.ensure(nb); bC2.ensure(nb); bacc.ensure(nb); bfn.ensure(nb);
     bcdbo_h.ensure(nb); bfn_h.ensure(nb); bacc_t.ensure(nb); bfn_t.ensure(nb);
     Tl.ensure(nb * bcap);
+    Ti.ensure(nb * bcap);
+    Tsum.ensure(2 * nb);
+    Tvir.ensure(nb * kVir);
   }
 
   Dev dev() {
@@ -593,7 +597,7 @@ struct Context {
       d.rnear2 = rn * rn;
     }
     d.bcap = bcap; d.bcode = bcode.p; d.bsym = bsym.p; d.bcnt = bcnt.p; d.bdv = bdv.p; d.bBO = bBO.p; d.bdBOp = bdBOp.p;
-    d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p;
+    d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p; d.Ti = Ti.p; d.Tsum = Tsum.p; d.Tvir = Tvir.p;
     d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
     d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.vir_nb = vir_nb.p; d.vir_h = vir_h.p; d.vir_t = vir_t.p;
     d.fown_h = fown_h.p; d.fown_t = fown_t.p; d.fix_h = fix_h.p; d.pe_fix = pe_fix.p; d.pe_on = pe_on; d.bcdbo_h = bcdbo_h.p; d.bfn_h = bfn_h.p; d.bacc_t = bacc_t.p; d.bfn_t = bfn_t.p; d.census = census.p; d.status = status.p;
@@ -739,7 +743,7 @@ struct Context {
     toc(3);
     tic(4, "torsion");
     ++launches;
-    k_torsion<<<blocks(na, tune.tpb_atom), tune.tpb_atom, 0, ts>>>(d, dff, ctl);
+    k_torsion<<<blocks(static_cast<long long>(na) * bcap, tune.tpb_atom), tune.tpb_atom, 0, ts>>>(d, dff, ctl);
     toc(4);
     if (conc) {
       RXCU(cudaEventRecord(ev_join_h, side_h));
@@ -888,7 +892,7 @@ struct Context {
     pick(&tune.tpb_hb, {64, 128, 256}, [&](int t) { k_hbond<<<blocks(nw, t), t, 0, stream>>>(d, dff, ctl); });
     pick(&tune.tpb_atom, {32, 64, 128}, [&](int t) {
       k_bonded_atom<<<blocks(na, t), t, 0, stream>>>(d, dff, ctl);
-      k_torsion<<<blocks(na, t), t, 0, stream>>>(d, dff, ctl);
+      k_torsion<<<blocks(static_cast<long long>(na) * bcap, t), t, 0, stream>>>(d, dff, ctl);
     });
     RXCU(cudaEventDestroy(a));
     RXCU(cudaEventDestroy(b));

@@ -723,39 +723,43 @@ __global__ void __launch_bounds__(256) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
 }
 
 // ------------------------------------------------------------------------------------------------ torsion
-// One thread per atom j, every bond j -> k that j evaluates (tag order, src/cpu/bonded.cpp:480-506): all bonds
-// i of j (i != k) and l of k (l != j) with the gates of :510 and :530 (i != l as images, a torsion entry for
-// (ti, tj, tk, tl), BO_kl > thb_cut, BO_ij BO_jk BO_kl > thb_cut). Contributions to the bond k-l and to the atom l
-// are written to Tl[(slot j->k) * bcap + (position of l in k's slots)], gathered by k in k_fold.
+// One thread per central bond j -> k (slot t of atom j) that j evaluates (tag order, src/cpu/bonded.cpp:480-506): all
+// bonds i of j (i != k) and l of k (l != j) with the gates of :510 and :530 (i != l as images, a torsion entry for
+// (ti, tj, tk, tl), BO_kl > thb_cut, BO_ij BO_jk BO_kl > thb_cut). Every write goes to slot t's own rows: its
+// coefficients and the gradient of k (bacc_t/bfn_t[t]), the contributions to the bond k-l and the atom l
+// (Tl[t * bcap + position of l in k's slots]) and to the bond j-i and the atom i (Ti[t * bcap + position of i in j's
+// slots]), and j's own gradient, CdDelta, energies, count and virial (Tsum[t], Tvir[t]); k_fold gathers them.
 __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
   if (lists_failed(d)) return;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= d.na) return;
-  const int type_j = d.type[j];
+  const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (tid >= static_cast<long long>(d.na) * d.bcap) return;
+  const int j = static_cast<int>(tid / d.bcap), pk = static_cast<int>(tid % d.bcap);
   const int nbj = min(d.bcnt[j], d.bcap);
+  if (pk >= nbj) return;
+  const int type_j = d.type[j];
   const size_t base = static_cast<size_t>(j) * d.bcap;
+  const size_t bjk = base + pk;
   const double thb_cut = ctl.thb_cut;
   const double* gp = ff.gp;
   const double p_tor2 = gp[23], p_tor3 = gp[24], p_tor4 = gp[25], p_cot2 = gp[27];
-  for (int c = 0; c < nbj; ++c) {
-    const int ka = static_cast<int>(d.bcode[base + c] & d.amask);
-    const int nbk = min(d.bcnt[ka], d.bcap);
-    for (int q = 0; q < nbk; ++q) d.Tl[(base + c) * d.bcap + q] = make_double4(0, 0, 0, 0);
-    d.bacc_t[base + c] = make_double4(0, 0, 0, 0);
-    d.bfn_t[base + c] = make_double4(0, 0, 0, 0);
+  {   // this slot's rows start at zero
+    const int ka0 = static_cast<int>(d.bcode[bjk] & d.amask);
+    const int nbk0 = min(d.bcnt[ka0], d.bcap);
+    for (int q = 0; q < nbk0; ++q) d.Tl[bjk * d.bcap + q] = make_double4(0, 0, 0, 0);
+    for (int q = 0; q < nbj; ++q) d.Ti[bjk * d.bcap + q] = make_double4(0, 0, 0, 0);
   }
   double fj[3] = {0, 0, 0}, cdd = 0.0, e_tor = 0.0, e_con = 0.0, pe_tor_own = 0.0;
   double vir[kVir] = {0, 0, 0, 0, 0, 0};
+  double4 acc_jk = make_double4(0, 0, 0, 0), fk_own = make_double4(0, 0, 0, 0);
   int ntor = 0;
   const double Delta_j = d.aq[j].Delta_boc;
-  for (int pk = 0; pk < nbj; ++pk) {
-    const size_t bjk = base + pk;
+  do {
     const double4 dvk4 = d.bdv[bjk];
     const unsigned code_k = d.bcode[bjk];
     const int ka = static_cast<int>(code_k & d.amask);
-    if (skip_by_tag(d, j, ka, dvk4)) continue;
+    if (skip_by_tag(d, j, ka, dvk4)) break;
     const double4 bo_jk = d.bBO[bjk];
-    if (!(bo_jk.x > thb_cut)) continue;
+    if (!(bo_jk.x > thb_cut)) break;
     const int sym_jk = d.bsym[bjk];
     const int nbk = min(d.bcnt[ka], d.bcap);
     const size_t base_k = static_cast<size_t>(ka) * d.bcap;
@@ -904,29 +908,26 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
         const double CEconj5 = -p_cot1 * fn12 * ((cos_omega * cos_omega) - 1.0) * sin_ijk * tan_jkl_i;
         const double CEconj6 = 2.0 * p_cot1 * fn12 * cos_omega * sin_ijk * sin_jkl;
         // coefficients
-        d.bacc_t[bjk].y += CEtors2;
+        acc_jk.y += CEtors2;
         cdd += CEtors3;
-        d.bacc_t[bjk].w += CEtors3;
-        d.bacc_t[bij].x += (CEtors4 + CEconj1);
-        d.bacc_t[bjk].x += (CEtors5 + CEconj2);
+        acc_jk.w += CEtors3;
+        double4& ti = d.Ti[bjk * d.bcap + pi];
+        ti.w += (CEtors4 + CEconj1);
+        acc_jk.x += (CEtors5 + CEconj2);
         double4& tl = d.Tl[bjk * d.bcap + pl];
         tl.w += (CEtors6 + CEconj3);
         // gradient
         const double c78 = CEtors7 + CEconj4, c85 = CEtors8 + CEconj5, c96 = CEtors9 + CEconj6;
-        double4 fi = d.bfn_t[bij];
-        double4 fk = d.bfn_t[bjk];
         double gi[3], gk[3], gl[3];
         for (int c = 0; c < 3; ++c) {
           gi[c] = c78 * pijk_dk[c] + c96 * dco_i[c];
           gk[c] = c78 * pijk_di[c] + c85 * pjkl_dj[c] + c96 * dco_k[c];
           gl[c] = c85 * pjkl_dk[c] + c96 * dco_l[c];
-          (&fi.x)[c] += gi[c];
+          (&ti.x)[c] += gi[c];
           fj[c] += c78 * pijk_dj[c] + c85 * pjkl_di[c] + c96 * dco_j[c];
-          (&fk.x)[c] += gk[c];
+          (&fk_own.x)[c] += gk[c];
           (&tl.x)[c] += gl[c];
         }
-        d.bfn_t[bij] = fi;
-        d.bfn_t[bjk] = fk;
         {   // virial about j: i at dij, k at djk, l at djk + dkl
           const double pl[3] = {djk[0] + dkl[0], djk[1] + dkl[1], djk[2] + dkl[2]};
           vir_add(vir, dij, gi);
@@ -935,13 +936,13 @@ __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
         }
       }
     }
-  }
-  d.fown_t[j] = make_double4(fj[0], fj[1], fj[2], cdd);
-  for (int c = 0; c < kVir; ++c) d.vir_t[static_cast<size_t>(j) * kVir + c] = vir[c];
+  } while (false);
   pe_add(d, j, pe_tor_own);
-  d.eatom[static_cast<size_t>(j) * kTerms + E_TOR] = e_tor;
-  d.eatom[static_cast<size_t>(j) * kTerms + E_CON] = e_con;
-  d.census[2 * d.na + j] = ntor;
+  d.bacc_t[bjk] = acc_jk;
+  d.bfn_t[bjk] = fk_own;
+  d.Tsum[2 * bjk] = make_double4(fj[0], fj[1], fj[2], cdd);
+  d.Tsum[2 * bjk + 1] = make_double4(e_tor, e_con, static_cast<double>(ntor), 0.0);
+  for (int c = 0; c < kVir; ++c) d.Tvir[bjk * kVir + c] = vir[c];
 }
 
 // ------------------------------------------------------------------------------------------------ gathers
@@ -953,11 +954,30 @@ __global__ void k_fold(Dev d) {
   if (a >= d.na) return;
   const int nb = min(d.bcnt[a], d.bcap);
   const size_t base = static_cast<size_t>(a) * d.bcap;
+  {   // a's torsions as the central atom j: per-slot partials of its central bonds, in slot order
+    double4 own = make_double4(0, 0, 0, 0), en = make_double4(0, 0, 0, 0);
+    double vr[kVir] = {0, 0, 0, 0, 0, 0};
+    for (int c = 0; c < nb; ++c) {
+      const double4 t0 = d.Tsum[2 * (base + c)], t1 = d.Tsum[2 * (base + c) + 1];
+      own.x += t0.x; own.y += t0.y; own.z += t0.z; own.w += t0.w;
+      en.x += t1.x; en.y += t1.y; en.z += t1.z;
+      for (int k = 0; k < kVir; ++k) vr[k] += d.Tvir[(base + c) * kVir + k];
+    }
+    d.fown_t[a] = own;
+    for (int k = 0; k < kVir; ++k) d.vir_t[static_cast<size_t>(a) * kVir + k] = vr[k];
+    d.eatom[static_cast<size_t>(a) * kTerms + E_TOR] = en.x;
+    d.eatom[static_cast<size_t>(a) * kTerms + E_CON] = en.y;
+    d.census[2 * d.na + a] = static_cast<int>(en.z);
+  }
   for (int p = 0; p < nb; ++p) {
     double4 acc = make_double4(0, 0, 0, 0);
     for (int b = 0; b < nb; ++b) {
       const int c = d.bsym[base + b];
       const double4 t = d.Tl[static_cast<size_t>(c) * d.bcap + p];
+      acc.x += t.x; acc.y += t.y; acc.z += t.z; acc.w += t.w;
+    }
+    for (int c = 0; c < nb; ++c) {   // torsions in which the bond a-p is the first bond i-j of a central bond of a
+      const double4 t = d.Ti[(base + c) * d.bcap + p];
       acc.x += t.x; acc.y += t.y; acc.z += t.z; acc.w += t.w;
     }
     double4 at = d.bacc_t[base + p];

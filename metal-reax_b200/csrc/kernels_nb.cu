@@ -300,16 +300,18 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
   const long long tag_i = d.tag[i];
   const int center = (d.S * d.S * d.S - 1) / 2;
   double gx = 0, gy = 0, gz = 0, ev = 0, ee = 0, ehalf = 0;
-  double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;   // pair virial, half per directed entry
+  float v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;   // pair virial, half per directed entry (lane partials)
   int counted = 0;
+  const double4 xi4 = d.x[i];
   for (int e = lane; e < cnt; e += 32) {
     const unsigned code = d.nbr[static_cast<size_t>(i) * d.ncap + e];
     const int j = static_cast<int>(code & d.amask);
     const int sidx = static_cast<int>(code >> d.abits);
     double dvd[3];
-    pair_dvec(d, s, i, j, sidx, dvd);
+    pair_dvec_x(d, s, i, j, sidx, xi4, d.x[j], dvd);
     const float dx = static_cast<float>(dvd[0]), dy = static_cast<float>(dvd[1]), dz = static_cast<float>(dvd[2]);
-    const float r = static_cast<float>(sqrt(dvd[0] * dvd[0] + dvd[1] * dvd[1] + dvd[2] * dvd[2]));
+    // the exact cut-off test was taken in FP64 when the row was filtered; the pair terms run in FP32
+    const float r = sqrtf(static_cast<float>(dvd[0] * dvd[0] + dvd[1] * dvd[1] + dvd[2] * dvd[2]));
     const int tj = d.type[j];
     const float* pp = ff.nbf + (static_cast<size_t>(ti) * ff.nt + tj) * 12;
     float Tap, dTap;
@@ -317,9 +319,9 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     const float alpha = pp[0], D = pp[1], r_vdW = pp[2];
     float e_vdW = 0.f, CEvd;
     if (ff.vdw_type == 1 || ff.vdw_type == 3) {
-      const float powr_vdW1 = powf(r, p_vdW1);
+      const float powr_vdW1 = exp2f(p_vdW1 * __log2f(r));   // r^p and (..)^(1/p) through the fast base-2 pair
       const float sum = powr_vdW1 + pp[3];
-      const float fn13 = powf(sum, p_vdW1i);
+      const float fn13 = exp2f(p_vdW1i * __log2f(sum));
       const float exp1 = __expf(alpha * (1.f - fn13 / r_vdW));
       const float exp2 = __expf(0.5f * alpha * (1.f - fn13 / r_vdW));
       const float evd = D * (exp1 - 2.f * exp2);
@@ -358,9 +360,9 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     gy -= static_cast<double>(CE * dy);
     gz -= static_cast<double>(CE * dz);
     {   // the gradient -CE dv on i and +CE dv on the partner: virial -CE dv (x) dv, half of it from each direction
-      const double c = -0.5 * static_cast<double>(CE);
-      v0 += c * dvd[0] * dvd[0]; v1 += c * dvd[1] * dvd[1]; v2 += c * dvd[2] * dvd[2];
-      v3 += c * dvd[0] * dvd[1]; v4 += c * dvd[0] * dvd[2]; v5 += c * dvd[1] * dvd[2];
+      const float c = -0.5f * CE;
+      v0 += c * dx * dx; v1 += c * dy * dy; v2 += c * dz * dz;
+      v3 += c * dx * dy; v4 += c * dx * dz; v5 += c * dy * dz;
     }
     // owner-computes counting of the energy
     bool count = false;
@@ -385,13 +387,14 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     ehalf += 0.5 * (static_cast<double>(e_vdW) + static_cast<double>(e_ele));   // per-atom tally: half of every pair
   }
   gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); ev = warp_sum(ev); ee = warp_sum(ee);
-  v0 = warp_sum(v0); v1 = warp_sum(v1); v2 = warp_sum(v2); v3 = warp_sum(v3); v4 = warp_sum(v4); v5 = warp_sum(v5);
+  const double w0 = warp_sum(static_cast<double>(v0)), w1 = warp_sum(static_cast<double>(v1)), w2 = warp_sum(static_cast<double>(v2));
+  const double w3 = warp_sum(static_cast<double>(v3)), w4 = warp_sum(static_cast<double>(v4)), w5 = warp_sum(static_cast<double>(v5));
   if (d.pe_on) ehalf = warp_sum(ehalf);
   for (int o = 16; o > 0; o >>= 1) counted += __shfl_xor_sync(0xffffffffu, counted, o);
   if (lane == 0) {
     d.fnb[i] = make_double4(gx, gy, gz, 0.0);
     double* vi = d.vir_nb + static_cast<size_t>(i) * kVir;
-    vi[0] = v0; vi[1] = v1; vi[2] = v2; vi[3] = v3; vi[4] = v4; vi[5] = v5;
+    vi[0] = w0; vi[1] = w1; vi[2] = w2; vi[3] = w3; vi[4] = w4; vi[5] = w5;
     d.eatom[static_cast<size_t>(i) * kTerms + E_VDW] = ev;
     d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] = ee;
     const double chi = ff.sb[ti * SB_N + SB_CHI], eta = ff.sb[ti * SB_N + SB_ETA], qd = d.q[i];
