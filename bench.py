@@ -370,7 +370,10 @@ def run_engine(args, rank, world, local_rank):
         if not args.no_batch:
             line["batch"] = batch_run(local_rank)
         if args.serve_requests > 0:
-            line["serve"] = serve_run(local_rank, args.serve_requests)
+            try:
+                line["serve"] = serve_run(local_rank, args.serve_requests)
+            except Exception as exc:   # the serving sample is reported beside the headline; its failure is recorded
+                line["serve"] = {"error": "%s: %s" % (type(exc).__name__, exc)}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(args.cpu_seconds)
     elif rank == 0:

@@ -226,7 +226,8 @@ int rx_md_targets(rx_context* ctx, const double* t_target, const int* active);
  * these changes a result bit. RX_TUNE_*_TPB: threads per block of a warp-per-atom kernel (64, 128, 256: atoms per
  * block x 32) or of the thread-per-atom bonded kernels (32, 64, 128); RX_TUNE_LONE_GRID_MIN: a context holding one
  * system of more atoms takes the single-system CG (all SMs on its rows, default 4096; a batch always takes the
- * segmented CG, so a system alone and in a batch give the same bits only below this size). rx_autotune times every
+ * segmented CG, so a system alone and in a batch give the same bits only below this size); RX_TUNE_OVERLAP: 1 (the
+ * default) runs the bonded terms, which need no charge, concurrently with the charge solve, 0 after it. rx_autotune times every
  * candidate shape on the current systems (reps launches each, CUDA events) and keeps the fastest; chosen[5] (may be
  * NULL) receives pairs, bonds, non-bonded, H-bond and per-atom shapes. */
 #define RX_TUNE_PAIRS_TPB 1
@@ -235,6 +236,7 @@ int rx_md_targets(rx_context* ctx, const double* t_target, const int* active);
 #define RX_TUNE_HBOND_TPB 4
 #define RX_TUNE_ATOM_TPB 5
 #define RX_TUNE_LONE_GRID_MIN 6
+#define RX_TUNE_OVERLAP 7
 int rx_set_tuning(rx_context* ctx, int key, int value);
 int rx_autotune(rx_context* ctx, int reps, int* chosen);
 

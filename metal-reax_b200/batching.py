@@ -1,8 +1,8 @@
-"""Host side of the batching form: which systems a GPU takes, and the batched versus one-context-per-system runs.
+"""Host side of the batching form across GPUs: which systems each GPU takes.
 
 Independent periodic systems shard across GPUs with no exchange on the data path: each rank (one process per GPU) takes
-a disjoint subset of the systems, balanced by atom count, and evaluates its subset as one batch. Results are gathered
-on the host only when the caller wants them in one place (the serving loop and the tests).
+a disjoint subset of the systems, balanced by atom count, and evaluates its subset as one batch in its own engine
+context. Results are gathered on the host only when the caller wants them in one place (bench.py and the tests).
 """
 import numpy as np
 

@@ -76,8 +76,8 @@ struct Context {
   int device = 0;
   int nsm = 0;
   cudaStream_t stream = nullptr;
-  // concurrent branches of an evaluation: non-bonded pairs (side), H-bonds (side_h) and torsions (side_t) next to
-  // the bonded chain on `stream`
+  // concurrent branches of an evaluation: the bonded chain (side), H-bonds (side_h) and torsions (side_t) next to
+  // the charge solve and the non-bonded pairs on `stream`
   cudaStream_t side = nullptr, side_h = nullptr, side_t = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join_h = nullptr, ev_join_t = nullptr;
   // one captured MD step (replayed for every step of rx_md_run); dropped whenever a buffer or a parameter it holds
@@ -145,7 +145,8 @@ struct Context {
   DBuf<long long> counters;
   DBuf<double> energies, virial, vir, vir_nb, vir_h, vir_t;
   // QEq
-  DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q, cg_w;
+  DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
+  DBuf<float2> cg_df;
   DBuf<double> cg_eta, cg_part, s_hist, t_hist, cg_rel;
   DBuf<int> cg_iters, cg_nlive, cg_nref, cg_brk;
   DBuf<SysCg> cg_sys;
@@ -557,7 +558,7 @@ struct Context {
     vir.ensure(n * kVir);
     vir_nb.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
     fown_h.ensure(n); fown_t.ensure(n); fix_h.ensure(3 * n); pe_fix.ensure(n);
-    cg_x.ensure(n); cg_w.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
+    cg_x.ensure(n); cg_df.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
     cg_sys.ensure(nsys); cg_rb0.ensure(n); cg_rb1.ensure(n); cg_nlive.ensure(2);
     cg_part.ensure(16 * static_cast<size_t>(std::max(nsm, 1)) * 32);
@@ -655,7 +656,7 @@ struct Context {
   CgArgs cg_args() {
     CgArgs a{};
     a.imax = qeq_imax; a.tol = qeq_tol;
-    a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.w = cg_w.p; a.eta = cg_eta.p; a.part = cg_part.p;
+    a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.df = cg_df.p; a.eta = cg_eta.p; a.part = cg_part.p;
     a.out_iters = cg_iters.p; a.out_rel = cg_rel.p; a.out_nref = cg_nref.p; a.out_brk = cg_brk.p; a.write_q = 1;
     return a;
   }
@@ -665,6 +666,7 @@ struct Context {
   struct Tune {
     int tpb_pairs = 128, tpb_nb = 128, tpb_hb = 128, tpb_bonds = 128, tpb_atom = 64;
     int lone_grid_min = 4096;
+    int overlap = 1;   // bonded chain beside the charge solve
   } tune;
   int grid_per_sm = 0, seg_per_sm = 0;
   void launch_cg(const Dev& d, CgArgs a) {
@@ -704,41 +706,33 @@ struct Context {
     toc(1);
   }
 
-  // After the rows (and the charges): the non-bonded pairs on `side` run next to the bonded chain; after the bond
-  // orders, the H-bonds (`side_h`) and the torsions (`side_t`) run next to k_bonded_atom. Each branch writes its own
-  // arrays (fnb, vir_nb; *_h; *_t, Tl), and all join before the gathers, which add them in fixed order. With timing on,
-  // every branch runs on `stream`, one after the other, so each phase is timed alone.
-  void launch_forces(const Dev& d) {
+  // After the rows, the bonded chain (bond orders, then k_bonded_atom, with the H-bonds on `side_h` and the torsions
+  // on `side_t`) needs no charge, so with tune.overlap it runs on `side` next to the charge solve; the non-bonded pairs
+  // follow the charges on `stream`. Each branch writes its own arrays (fnb, vir_nb; bacc/bfn/fown; *_h; *_t, Tl), and
+  // all join before the gathers, which add them in fixed order, so the schedule changes no result bit. With timing
+  // on, every branch runs on `stream`, one after the other, so each phase is timed alone.
+  void launch_bonded(const Dev& d) {
     const bool conc = !timing;
-    cudaStream_t nbs = conc ? side : stream, hs = conc ? side_h : stream, ts = conc ? side_t : stream;
+    cudaStream_t bs = conc ? side : stream, hs = conc ? side_h : stream, ts = conc ? side_t : stream;
     if (conc) {
       RXCU(cudaEventRecord(ev_fork, stream));
       RXCU(cudaStreamWaitEvent(side, ev_fork, 0));
     }
-    tic(5, "nonbonded");
-    ++launches;
-    k_nonbonded<<<blocks(static_cast<long long>(na) * 32, tune.tpb_nb), tune.tpb_nb, 0, nbs>>>(d, dff);
-    if (acks2_on) {
-      ++launches;
-      k_acks2<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, nbs>>>(d, dff, s_kin.p);
-    }
-    toc(5);
-    if (conc) RXCU(cudaEventRecord(ev_join, side));
     tic(2, "bond_orders");
     launches += 4;
-    k_bonds<<<blocks(static_cast<long long>(na) * 32, tune.tpb_bonds), tune.tpb_bonds, 0, stream>>>(d, dff, ctl);
-    k_bond_sym<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d);
-    k_bo_correct<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, stream>>>(d, dff);
-    k_atom_quantities<<<blocks(na, 128), 128, 0, stream>>>(d, dff);
+    k_bonds<<<blocks(static_cast<long long>(na) * 32, tune.tpb_bonds), tune.tpb_bonds, 0, bs>>>(d, dff, ctl);
+    k_bond_sym<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, bs>>>(d);
+    k_bo_correct<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, bs>>>(d, dff);
+    k_atom_quantities<<<blocks(na, 128), 128, 0, bs>>>(d, dff);
     toc(2);
     if (conc) {
-      RXCU(cudaEventRecord(ev_fork2, stream));
+      RXCU(cudaEventRecord(ev_fork2, bs));
       RXCU(cudaStreamWaitEvent(side_h, ev_fork2, 0));
       RXCU(cudaStreamWaitEvent(side_t, ev_fork2, 0));
     }
     tic(3, "bonded_terms");
     launches += 2;
-    k_bonded_atom<<<blocks(na, tune.tpb_atom), tune.tpb_atom, 0, stream>>>(d, dff, ctl);
+    k_bonded_atom<<<blocks(na, tune.tpb_atom), tune.tpb_atom, 0, bs>>>(d, dff, ctl);
     k_hbond<<<blocks(static_cast<long long>(na) * 32, tune.tpb_hb), tune.tpb_hb, 0, hs>>>(d, dff, ctl);
     toc(3);
     tic(4, "torsion");
@@ -746,8 +740,26 @@ struct Context {
     k_torsion<<<blocks(static_cast<long long>(na) * bcap, tune.tpb_atom), tune.tpb_atom, 0, ts>>>(d, dff, ctl);
     toc(4);
     if (conc) {
+      RXCU(cudaEventRecord(ev_join, bs));
       RXCU(cudaEventRecord(ev_join_h, side_h));
       RXCU(cudaEventRecord(ev_join_t, side_t));
+    }
+  }
+
+  void launch_nonbonded(const Dev& d) {
+    tic(5, "nonbonded");
+    ++launches;
+    k_nonbonded<<<blocks(static_cast<long long>(na) * 32, tune.tpb_nb), tune.tpb_nb, 0, stream>>>(d, dff);
+    if (acks2_on) {
+      ++launches;
+      k_acks2<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, s_kin.p);
+    }
+    toc(5);
+  }
+
+  void launch_gathers(const Dev& d) {
+    if (!timing) {
+      RXCU(cudaStreamWaitEvent(stream, ev_join, 0));
       RXCU(cudaStreamWaitEvent(stream, ev_join_h, 0));
       RXCU(cudaStreamWaitEvent(stream, ev_join_t, 0));
     }
@@ -755,18 +767,25 @@ struct Context {
     launches += 3;
     k_fold<<<blocks(na, 128), 128, 0, stream>>>(d);
     k_dbond<<<blocks(na, 128), 128, 0, stream>>>(d);
-    if (conc) RXCU(cudaStreamWaitEvent(stream, ev_join, 0));
     k_force_final<<<blocks(na, 128), 128, 0, stream>>>(d);
     toc(6);
   }
 
   // One evaluation of every system, enqueued without any host synchronisation: kernels after a failure (a list
-  // overflow) return at once; the host reads the status word when it next synchronises.
+  // overflow) return at once; the host reads the status word when it next synchronises. Without tune.overlap the
+  // bonded chain is forked after the charges instead (the non-bonded pairs then run beside it).
   void enqueue_eval(bool do_qeq) {
     const Dev d = dev();
     build_lists(d);
-    if (do_qeq) launch_qeq(d);
-    launch_forces(d);
+    if (tune.overlap) {
+      launch_bonded(d);
+      if (do_qeq) launch_qeq(d);
+    } else {
+      if (do_qeq) launch_qeq(d);
+      launch_bonded(d);
+    }
+    launch_nonbonded(d);
+    launch_gathers(d);
   }
 
   // grow the capacities from a status word with overflow bits; false if nothing overflowed
@@ -912,6 +931,7 @@ struct Context {
       case RX_TUNE_HBOND_TPB: check(value == 64 || value == 128 || value == 256); tune.tpb_hb = value; break;
       case RX_TUNE_ATOM_TPB: check(value == 32 || value == 64 || value == 128); tune.tpb_atom = value; break;
       case RX_TUNE_LONE_GRID_MIN: check(value >= 0); tune.lone_grid_min = value; break;
+      case RX_TUNE_OVERLAP: check(value == 0 || value == 1); tune.overlap = value; break;
       default: throw Error(RX_ERR_INVALID, "unknown tuning key");
     }
     drop_graph();

@@ -478,9 +478,8 @@ __global__ void k_acks2(Dev d, DevFF ff, const double* s_kin) {
 
 // ------------------------------------------------------------------------------------------------ QEq CG
 // y = (diag(eta) + H) v for one row, both right-hand sides (s, t) at once; warp per row, each lane taking four
-// consecutive entries per pass with 16-byte loads (rows start 128-byte aligned: ncap is a multiple of 32). FULL: H as
-// hi + lo (the FP64 matrix to ~1e-15); otherwise hi alone (the single-precision matrix of the inner CG iterations).
-template <bool FULL>
+// consecutive entries per pass with 16-byte loads (rows start 128-byte aligned: ncap is a multiple of 32); H as
+// hi + lo (the FP64 matrix to ~1e-15).
 __device__ inline double2 row_mv(const Dev& d, int i, double eta, const double2* v) {
   const int cnt = min(d.nbr_cnt[i], d.ncap);
   const int lane = threadIdx.x & 31;
@@ -490,17 +489,44 @@ __device__ inline double2 row_mv(const Dev& d, int i, double eta, const double2*
   for (int e0 = lane * 4; e0 < cnt; e0 += 128) {
     const uint4 c4 = *reinterpret_cast<const uint4*>(d.nbr + base + e0);
     const float4 h4 = *reinterpret_cast<const float4*>(d.hhi + base + e0);
-    float4 l4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (FULL) l4 = *reinterpret_cast<const float4*>(d.hlo + base + e0);
+    const float4 l4 = *reinterpret_cast<const float4*>(d.hlo + base + e0);
     const unsigned cc[4] = {c4.x, c4.y, c4.z, c4.w};
     const float hh[4] = {h4.x, h4.y, h4.z, h4.w}, ll[4] = {l4.x, l4.y, l4.z, l4.w};
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       if (e0 + k < cnt) {
-        const double h = FULL ? static_cast<double>(hh[k]) + static_cast<double>(ll[k]) : static_cast<double>(hh[k]);
+        const double h = static_cast<double>(hh[k]) + static_cast<double>(ll[k]);
         const double2 vj = v[cc[k] & d.amask];
         ys += h * vj.x;
         yt += h * vj.y;
+      }
+    }
+  }
+  ys = warp_sum(ys);
+  yt = warp_sum(yt);
+  return make_double2(eta * vi.x + __shfl_sync(0xffffffffu, ys, 0), eta * vi.y + __shfl_sync(0xffffffffu, yt, 0));
+}
+
+// (A v)_i of the single-precision-matrix iterations: FP32 values of the matrix (hhi) times the FP32 copy vf of v,
+// products and sums in FP64; the diagonal term takes v_i itself. Gathering 8-byte float2 halves the bytes of the
+// gathers (the vector of a 24k-atom system then fits in an SM's L1).
+__device__ inline double2 row_mv_f32(const Dev& d, int i, double eta, const double2* v, const float2* vf) {
+  const int cnt = min(d.nbr_cnt[i], d.ncap);
+  const int lane = threadIdx.x & 31;
+  const double2 vi = v[i];
+  double ys = 0.0, yt = 0.0;
+  const size_t base = static_cast<size_t>(i) * d.ncap;
+  for (int e0 = lane * 4; e0 < cnt; e0 += 128) {
+    const uint4 c4 = *reinterpret_cast<const uint4*>(d.nbr + base + e0);
+    const float4 h4 = *reinterpret_cast<const float4*>(d.hhi + base + e0);
+    const unsigned cc[4] = {c4.x, c4.y, c4.z, c4.w};
+    const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (e0 + k < cnt) {
+        const float2 vj = vf[cc[k] & d.amask];
+        ys += static_cast<double>(hh[k]) * static_cast<double>(vj.x);
+        yt += static_cast<double>(hh[k]) * static_cast<double>(vj.y);
       }
     }
   }
@@ -551,8 +577,8 @@ __device__ inline void grid_totals(const double* part, int nblocks, double* tot,
 // reproduced in plugin/adapter/fix_qeq_reaxff_metal.cpp:89-123, each right-hand side stopping on its own test
 // sqrt(r.M^-1 r)/|b| <= tol with at most imax-1 iterations; then calculate_Q: q = s - (sum s / sum t) t.
 // Precision (the resident refinement of src/metal/metal_backend.mm:435-530, in FP64 instead of double-single): the
-// iterations multiply by the single-precision matrix (hi: 8 bytes per entry with its index), the vectors and every dot
-// product are FP64, and the residual is recomputed with the FP64 matrix (hi + lo) whenever the iterations have
+// iterations multiply the single-precision matrix (hi: 8 bytes per entry with its index) by an FP32 copy of the search
+// direction (products and sums in FP64), the vectors and every dot product are FP64, and the residual is recomputed with the FP64 matrix (hi + lo) whenever the iterations have
 // converged - or have reduced the residual by kRefineDrop, below which the single-precision matrix stops helping. The
 // solve ends only on that FP64 residual, so the tolerance and the reported residuals are those of the FP64 system.
 // Rows are distributed over all warps of the grid; reductions are fixed-order (per-block partials summed in block
@@ -580,7 +606,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
     for (int r = gw; r < n; r += nwarps) {
       const int i = i0 + r;
       const double eta = a.eta[i];
-      const double2 y = row_mv<true>(d, i, eta, a.x);
+      const double2 y = row_mv(d, i, eta, a.x);
       if (lane == 0) {
         const double2 b = a.b[i];
         const double2 rr = make_double2(b.x - y.x, b.y - y.y);
@@ -604,7 +630,11 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
     const double stop_s = fmax(a.tol * bnorm_s, kRefineDrop * sqrt(sig_s));
     const double stop_t = fmax(a.tol * bnorm_t, kRefineDrop * sqrt(sig_t));
     // ---- single-precision-matrix iterations from this residual (d = p on entry)
-    for (int r = gw * 32 + lane; r < n; r += nwarps * 32) a.d[i0 + r] = a.p[i0 + r];
+    for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+      const double2 pp = a.p[i0 + r];
+      a.d[i0 + r] = pp;
+      a.df[i0 + r] = make_float2(static_cast<float>(pp.x), static_cast<float>(pp.y));
+    }
     g.sync();
     for (;;) {
       const bool in_s = act_s && it_s < a.imax && sqrt(sig_s) > stop_s;
@@ -614,7 +644,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
       loc[0] = loc[1] = 0.0;
       for (int r = gw; r < n; r += nwarps) {
         const int i = i0 + r;
-        const double2 y = row_mv<false>(d, i, a.eta[i], a.d);
+        const double2 y = row_mv_f32(d, i, a.eta[i], a.d, a.df);
         if (lane == 0) {
           a.q[i] = y;
           const double2 dd = a.d[i];
@@ -659,6 +689,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
         if (in_s) dd.x = pp.x + beta_s * dd.x;
         if (in_t) dd.y = pp.y + beta_t * dd.y;
         a.d[i] = dd;
+        a.df[i] = make_float2(static_cast<float>(dd.x), static_cast<float>(dd.y));
       }
       g.sync();
     }
@@ -768,7 +799,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_seg(Dev d, CgArgs a) {
         cnt = 0;
       }
       const double eta = a.eta[i];
-      const double2 y = row_mv<true>(d, i, eta, a.x);
+      const double2 y = row_mv(d, i, eta, a.x);
       if (lane == 0) {
         const double2 b = a.b[i];
         const double2 rr = make_double2(b.x - y.x, b.y - y.y);
@@ -814,7 +845,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_seg(Dev d, CgArgs a) {
           live = __ldcg(&a.sc[s].live) != 0;
         }
         if (!live) continue;
-        const double2 y = row_mv<true>(d, i, a.eta[i], a.d);
+        const double2 y = row_mv(d, i, a.eta[i], a.d);
         if (lane == 0) {
           a.q[i] = y;
           const double2 dd = a.d[i];
@@ -963,7 +994,7 @@ __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (warp >= d.na) return;
   const double eta = ff.sb[d.type[warp] * SB_N + SB_ETA];
-  const double2 r = row_mv<true>(d, warp, eta, v);
+  const double2 r = row_mv(d, warp, eta, v);
   if ((threadIdx.x & 31) == 0) y[warp] = r;
 }
 
