@@ -460,6 +460,77 @@ def serve_run(device, nreq=400, rate=200.0, chunk=10):
     return st
 
 
+def precision_run(device, nvt_steps=10000, nve_ps=20.0, sample=100):
+    """The precision form: 30,000 carbon atoms uniformly random at 1.0 g/cm3 (84.265 A box, pairs closer than 1.2 A
+    rejected) with the 2013 C force field and zero charges (one element: no charge solve), Maxwell velocities at 4000 K,
+    `nvt_steps` Nose-Hoover steps at 4000 K (Tdamp 25 fs), then `nve_ps` of NVE, dt 0.25 fs. Returns the step times of
+    both phases (CUDA events on the engine stream) and the NVE total-energy drift (slope of a linear fit of E_tot/N
+    against time) and the RMS of E_tot/N about that line, sampled every `sample` steps. None when the force field has
+    not been extracted (metal-reax_b200/data/decode_c2013.py)."""
+    import torch
+    import rxcuda
+    path = PKG / "data" / "_c2013" / "ffield.reax.C2013"
+    if not path.exists():
+        return None
+    s = systems.random_carbon(30000, density=1.0, seed=4000, amu=12.011)
+    n = len(s["type"])
+    mass = 12.011
+    eng = rxcuda.Engine(device)
+    eng.set_forcefield(path.read_text())
+    eng.set_control()
+    eng.set_systems([s])
+    eng.set_charges(np.zeros(n))
+    eng.md_setup([mass], dt=0.25, t_start=4000.0, t_damp=25.0, chain=3)
+    eng.md_charges(False)
+    eng.set_velocities(systems.maxwell_velocities(dict(s, mass=np.full(n, mass)), 4000.0, seed=4001))
+    st = torch.cuda.ExternalStream(eng.stream(), device=torch.device("cuda", device))
+
+    def timed(nsteps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        out = eng.md_run(nsteps)
+        b.record(st)
+        b.synchronize()
+        return out, a.elapsed_time(b)
+
+    ms_nvt = 0.0
+    done = 0
+    while done < nvt_steps:
+        k = min(1000, nvt_steps - done)
+        out, ms = timed(k)
+        ms_nvt += ms
+        done += k
+    t_nvt = float(out["T"][0])
+    v = eng.get_velocities()
+    eng.md_setup([mass], dt=0.25, t_start=4000.0, t_damp=25.0, chain=0)   # chain 0: plain velocity Verlet (NVE)
+    eng.set_velocities(v)
+    nve_steps = int(round(nve_ps * 1000.0 / 0.25))
+    kcal = 1.0 / 4.184e-4    # g/mol A^2/fs^2 -> kcal/mol
+    times, etot, temps = [], [], []
+    ms_nve = 0.0
+    for k in range(0, nve_steps, sample):
+        out, ms = timed(sample)
+        ms_nve += ms
+        vv = eng.get_velocities()
+        ke = 0.5 * mass * float((vv * vv).sum()) * kcal
+        etot.append((float(out["e"][0].sum()) + ke) / n)
+        times.append((k + sample) * 0.25e-3)
+        temps.append(float(out["T"][0]))
+    eng.close()
+    t_ps = np.asarray(times)
+    e = np.asarray(etot)
+    slope, icpt = np.polyfit(t_ps, e, 1)
+    rms = float(np.sqrt(np.mean((e - (slope * t_ps + icpt)) ** 2)))
+    return {"workload": "carbon30k_c2013_precision", "atoms": n, "dt_fs": 0.25, "nvt_steps": nvt_steps,
+            "nvt_T_end_K": t_nvt, "nve_ps": nve_ps, "nve_steps": nve_steps, "sample_every": sample,
+            "ms_per_step_nvt": ms_nvt / nvt_steps, "ms_per_step_nve": ms_nve / nve_steps,
+            "atom_steps_per_s_nvt": n * nvt_steps / (ms_nvt * 1e-3),
+            "nve_drift_kcal_per_atom_ps": float(slope), "nve_rms_kcal_per_atom": rms,
+            "nve_T_mean_K": float(np.mean(temps)), "nve_etot_first_last": [float(e[0]), float(e[-1])],
+            "reference_published": "VO oxide, 512 atoms, 20 ps NVE (docs/make_figures.py): drift stock 3.7e-6, "
+                                   "all-FP32 GPU 4.0e-4, mixed 3.4e-6 kcal/mol/atom/ps; RMS 1.1e-4 / 1.24e-3 / 1.07e-4"}
+
+
 # ---------------------------------------------------------------------------------------------------- reference arm
 def run_reference(args, rank):
     if rank != 0:
@@ -527,8 +598,18 @@ def main():
     ap.add_argument("--qeq-passes", type=int, default=0,
                     help="profiling case: after the warm-up steps, one charge solve of exactly this many matrix passes "
                          "(tolerance 0), then print the counts and exit")
+    ap.add_argument("--precision-form", action="store_true",
+                    help="run only the precision form (30k carbon, 2013 C force field: NVT at 4000 K, then NVE drift) "
+                         "and print its JSON line")
+    ap.add_argument("--nvt-steps", type=int, default=10000)
+    ap.add_argument("--nve-ps", type=float, default=20.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.precision_form:
+        out = precision_run(int(os.environ.get("LOCAL_RANK", "0")), args.nvt_steps, args.nve_ps)
+        print(json.dumps(out if out is not None else {"workload": "carbon30k_c2013_precision",
+                                                      "unavailable": "2013 C force field not extracted"}), flush=True)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -146,7 +146,7 @@ struct Context {
   DBuf<double> energies, virial, vir, vir_nb, vir_h, vir_t;
   // QEq
   DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
-  DBuf<float2> cg_df;
+  DBuf<float2> cg_pf;
   DBuf<double> cg_eta, cg_part, s_hist, t_hist, cg_rel;
   DBuf<int> cg_iters, cg_nlive, cg_nref, cg_brk;
   DBuf<SysCg> cg_sys;
@@ -558,7 +558,7 @@ struct Context {
     vir.ensure(n * kVir);
     vir_nb.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
     fown_h.ensure(n); fown_t.ensure(n); fix_h.ensure(3 * n); pe_fix.ensure(n);
-    cg_x.ensure(n); cg_df.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
+    cg_x.ensure(n); cg_pf.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
     cg_sys.ensure(nsys); cg_rb0.ensure(n); cg_rb1.ensure(n); cg_nlive.ensure(2);
     cg_part.ensure(16 * static_cast<size_t>(std::max(nsm, 1)) * 32);
@@ -656,7 +656,7 @@ struct Context {
   CgArgs cg_args() {
     CgArgs a{};
     a.imax = qeq_imax; a.tol = qeq_tol;
-    a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.df = cg_df.p; a.eta = cg_eta.p; a.part = cg_part.p;
+    a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.pf = cg_pf.p; a.eta = cg_eta.p; a.part = cg_part.p;
     a.out_iters = cg_iters.p; a.out_rel = cg_rel.p; a.out_nref = cg_nref.p; a.out_brk = cg_brk.p; a.write_q = 1;
     return a;
   }

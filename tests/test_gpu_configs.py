@@ -1,5 +1,5 @@
 """GPU parity on the benchmark workloads themselves: the 648-atom water box (216 H2O) and the 24,000-atom water box
-(8000 H2O) of the throughput measurement, at step 0 and at the frame the GPU's own NVT trajectory reaches after 100
+(8000 H2O) of the throughput measurement, at step 0 and at the frame the GPU's own NVT trajectory reaches after 1000
 steps (dt 0.25 fs, 300 K, charges equilibrated every step at tol 1e-6), each frame re-evaluated on the CPU.
 
 The CPU side is the reference's own cpu64 engine compiled from its sources (RefOracle) where it was built, else the C
@@ -88,10 +88,10 @@ def test_water_step0_and_trajectory_frame(n_side):
     # may stop one iteration apart
     assert np.abs(np.asarray(it) - np.asarray(ref_q["iters"])).max() <= 1, (it, ref_q["iters"])
     _compare("step0", s, out, eng.virial()[0], q, report)
-    # ---- 100 NVT steps on the GPU, then the frame they reach, re-evaluated on the CPU
+    # ---- 1000 NVT steps on the GPU, then the frame they reach, re-evaluated on the CPU
     eng.md_setup(MASS, dt=0.25, t_start=300.0, t_damp=25.0, chain=3)
     eng.set_velocities(systems.maxwell_velocities(s, 300.0, seed=11))
-    md = eng.md_run(100)
+    md = eng.md_run(1000)
     # the synthetic force field's water is not at equilibrium in this lattice start: it heats well above 300 K in the
     # first 25 fs while the chain (Tdamp 25 fs) catches up, so only a sane range is checked here
     assert np.all(np.isfinite(md["e"])) and 100.0 < md["T"][0] < 5000.0
@@ -99,13 +99,13 @@ def test_water_step0_and_trajectory_frame(n_side):
     frame["x"] = eng.get_positions()
     qf = eng.get_charges()
     out = eng.compute(census=True)           # the frame with the trajectory's own charges
-    _compare("step100", frame, out, eng.virial()[0], qf, report)
+    _compare("step1000", frame, out, eng.virial()[0], qf, report)
     # ---- a tight charge solve at that frame. The relative tolerance is on |b| of the whole system, so the per-atom
     # error it allows grows with the system: tol 1e-13 keeps both solutions within a few 1e-11 e at 24,000 atoms
     eng.set_qeq(0.0, 10.0, 1e-13, 600)
     got = eng.qeq_solve()
     ref = orc.qeq(frame, tol=1e-13, imax=600)
-    report.append({"frame": "step100", "charge_max_error_tol1e-13": float(np.abs(got["q"] - ref["q"]).max())})
+    report.append({"frame": "step1000", "charge_max_error_tol1e-13": float(np.abs(got["q"] - ref["q"]).max())})
     assert np.abs(got["q"] - ref["q"]).max() <= 1e-10
     eng.close()
     _write("water%d" % (3 * n_side ** 3), report)

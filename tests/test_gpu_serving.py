@@ -61,18 +61,29 @@ def _requests(specs):
     return out
 
 
+def _late_clock():
+    """A clock that reads 0 when the loop starts and 10 s ever after: every request (arrivals <= 0.003 s) has arrived
+    at the first round, and no round waits for an arrival."""
+    calls = []
+
+    def clock():
+        calls.append(None)
+        return 0.0 if len(calls) == 1 else 10.0
+    return clock
+
+
 def test_served_results_same_alone_and_in_mix():
     from serving import Server
     specs = [(3, 0.0, "md", 40, 600.0), (11, 0.0, "sp", 0, 300.0), (21, 0.001, "md", 25, 1500.0),
              (7, 0.002, "sp", 0, 300.0), (40, 0.003, "md", 40, 900.0)]
     srv = Server(ffield_text(), budget_bytes=1 << 34, bytes_per_atom=20000.0, chunk=10)
-    # the mix: all requests at once (the clock is frozen at 1 s, so every request has arrived at the first round)
+    # the mix: all requests at once (every request has arrived at the first round)
     mix = _requests(specs)
-    st = srv.run(mix, clock=lambda: 1.0)
+    st = srv.run(mix, clock=_late_clock())
     assert st["requests"] == len(specs)
     for k, spec in enumerate(specs):
         alone = _requests([spec])
-        srv.run(alone, clock=lambda: 1.0)
+        srv.run(alone, clock=_late_clock())
         r_mix, r_alone = mix[k], alone[0]
         n = r_alone.natoms
         if spec[2] == "sp":
@@ -95,6 +106,6 @@ def test_admission_respects_the_memory_budget():
     budget = bpa * (sum(r.natoms for r in reqs[:2]) + 1)
     peak = []
     srv = Server(ffield_text(), budget_bytes=budget, bytes_per_atom=bpa, chunk=5)
-    st = srv.run(reqs, clock=lambda: 1.0, on_round=lambda s, act: peak.append(sum(r.natoms for r in act) * bpa))
+    st = srv.run(reqs, clock=_late_clock(), on_round=lambda s, act: peak.append(sum(r.natoms for r in act) * bpa))
     assert st["requests"] == len(specs)
     assert max(peak) <= budget
