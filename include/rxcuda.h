@@ -222,12 +222,15 @@ int rx_update_systems(rx_context* ctx, int nkeep, const int* keep, int nnew, con
  * forces are still evaluated). */
 int rx_md_targets(rx_context* ctx, const double* t_target, const int* active);
 
-/* Launch-shape tuning (no counterpart in the reference, whose Metal kernels use a fixed threadgroup of 64). None of
- * these changes a result bit. RX_TUNE_*_TPB: threads per block of a warp-per-atom kernel (64, 128, 256: atoms per
+/* Launch-shape tuning (no counterpart in the reference, whose Metal kernels use a fixed threadgroup of 64). All but
+ * RX_TUNE_CG_BLOCKS_PER_SM leave every result bit unchanged. RX_TUNE_*_TPB: threads per block of a warp-per-atom kernel (64, 128, 256: atoms per
  * block x 32) or of the thread-per-atom bonded kernels (32, 64, 128); RX_TUNE_LONE_GRID_MIN: a context holding one
  * system of more atoms takes the single-system CG (all SMs on its rows, default 4096; a batch always takes the
  * segmented CG, so a system alone and in a batch give the same bits only below this size); RX_TUNE_OVERLAP: 1 (the
- * default) runs the bonded terms, which need no charge, concurrently with the charge solve, 0 after it. rx_autotune times every
+ * default) runs the bonded terms, which need no charge, concurrently with the charge solve, 0 after it;
+ * RX_TUNE_CG_BLOCKS_PER_SM: blocks per SM of the single-system CG (0, the default: as many as fit), fewer leaving room
+ * for the concurrent bonded terms - unlike the other keys this changes the order of the CG's sums, so the charges'
+ * last bits (a fixed setting stays bitwise reproducible), and rx_autotune does not touch it. rx_autotune times every
  * candidate shape on the current systems (reps launches each, CUDA events) and keeps the fastest; chosen[5] (may be
  * NULL) receives pairs, bonds, non-bonded, H-bond and per-atom shapes. */
 #define RX_TUNE_PAIRS_TPB 1
@@ -237,6 +240,7 @@ int rx_md_targets(rx_context* ctx, const double* t_target, const int* active);
 #define RX_TUNE_ATOM_TPB 5
 #define RX_TUNE_LONE_GRID_MIN 6
 #define RX_TUNE_OVERLAP 7
+#define RX_TUNE_CG_BLOCKS_PER_SM 8
 int rx_set_tuning(rx_context* ctx, int key, int value);
 int rx_autotune(rx_context* ctx, int reps, int* chosen);
 

@@ -146,7 +146,7 @@ struct Context {
   DBuf<double> energies, virial, vir, vir_nb, vir_h, vir_t;
   // QEq
   DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
-  DBuf<float2> cg_pf;
+  DBuf<float2> cg_df;
   DBuf<double> cg_eta, cg_part, s_hist, t_hist, cg_rel;
   DBuf<int> cg_iters, cg_nlive, cg_nref, cg_brk;
   DBuf<SysCg> cg_sys;
@@ -558,7 +558,7 @@ struct Context {
     vir.ensure(n * kVir);
     vir_nb.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
     fown_h.ensure(n); fown_t.ensure(n); fix_h.ensure(3 * n); pe_fix.ensure(n);
-    cg_x.ensure(n); cg_pf.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
+    cg_x.ensure(n); cg_df.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
     cg_sys.ensure(nsys); cg_rb0.ensure(n); cg_rb1.ensure(n); cg_nlive.ensure(2);
     cg_part.ensure(16 * static_cast<size_t>(std::max(nsm, 1)) * 32);
@@ -656,7 +656,7 @@ struct Context {
   CgArgs cg_args() {
     CgArgs a{};
     a.imax = qeq_imax; a.tol = qeq_tol;
-    a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.pf = cg_pf.p; a.eta = cg_eta.p; a.part = cg_part.p;
+    a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.df = cg_df.p; a.eta = cg_eta.p; a.part = cg_part.p;
     a.out_iters = cg_iters.p; a.out_rel = cg_rel.p; a.out_nref = cg_nref.p; a.out_brk = cg_brk.p; a.write_q = 1;
     return a;
   }
@@ -667,13 +667,15 @@ struct Context {
     int tpb_pairs = 128, tpb_nb = 128, tpb_hb = 128, tpb_bonds = 128, tpb_atom = 64;
     int lone_grid_min = 4096;
     int overlap = 1;   // bonded chain beside the charge solve
+    int cg_per_sm = 0;   // blocks of the single-system CG per SM (0: as many as fit); changes its summation order
   } tune;
   int grid_per_sm = 0, seg_per_sm = 0;
   void launch_cg(const Dev& d, CgArgs a) {
     if (nsys == 1 && na > tune.lone_grid_min) {   // one large system: all SMs on its rows, block partials in block order
       const int threads = 256;
       if (!grid_per_sm) RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k_cg_grid, threads, 0));
-      int grid = std::max(1, std::min(grid_per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
+      const int per_sm = tune.cg_per_sm > 0 ? std::min(tune.cg_per_sm, grid_per_sm) : grid_per_sm;
+      int grid = std::max(1, std::min(per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
       grid = std::min(grid, nsm * 32);
       a.begin = 0;
       a.n = na;
@@ -932,6 +934,7 @@ struct Context {
       case RX_TUNE_ATOM_TPB: check(value == 32 || value == 64 || value == 128); tune.tpb_atom = value; break;
       case RX_TUNE_LONE_GRID_MIN: check(value >= 0); tune.lone_grid_min = value; break;
       case RX_TUNE_OVERLAP: check(value == 0 || value == 1); tune.overlap = value; break;
+      case RX_TUNE_CG_BLOCKS_PER_SM: check(value >= 0 && value <= 32); tune.cg_per_sm = value; break;
       default: throw Error(RX_ERR_INVALID, "unknown tuning key");
     }
     drop_graph();

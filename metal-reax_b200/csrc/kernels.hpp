@@ -29,7 +29,7 @@ struct CgArgs {
   double2* d;
   double2* p;
   double2* q;
-  float2* pf;     // FP32 copy of p, gathered by the single-precision-matrix iterations (single-system CG)
+  float2* df;     // FP32 copy of d, gathered by the single-precision-matrix iterations (single-system CG)
   double* eta;
   double* part;    // 2 * 8 * gridDim.x partial sums (double-buffered)
   int* out_iters;

@@ -577,8 +577,8 @@ __device__ inline void grid_totals(const double* part, int nblocks, double* tot,
 // reproduced in plugin/adapter/fix_qeq_reaxff_metal.cpp:89-123, each right-hand side stopping on its own test
 // sqrt(r.M^-1 r)/|b| <= tol with at most imax-1 iterations; then calculate_Q: q = s - (sum s / sum t) t.
 // Precision (the resident refinement of src/metal/metal_backend.mm:435-530, in FP64 instead of double-single): the
-// iterations multiply the single-precision matrix (hi: 8 bytes per entry with its index) by an FP32 copy of the
-// preconditioned residual (products and sums in FP64), the vectors and every dot product are FP64, and the residual is recomputed with the FP64 matrix (hi + lo) whenever the iterations have
+// iterations multiply the single-precision matrix (hi: 8 bytes per entry with its index) by an FP32 copy of the search
+// direction (products and sums in FP64), the vectors and every dot product are FP64, and the residual is recomputed with the FP64 matrix (hi + lo) whenever the iterations have
 // converged - or have reduced the residual by kRefineDrop, below which the single-precision matrix stops helping. The
 // solve ends only on that FP64 residual, so the tolerance and the reported residuals are those of the FP64 system.
 // Rows are distributed over all warps of the grid; reductions are fixed-order (per-block partials summed in block
@@ -613,7 +613,6 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
         a.r[i] = rr;
         const double2 pp = make_double2(rr.x / eta, rr.y / eta);
         a.p[i] = pp;
-        a.pf[i] = make_float2(static_cast<float>(pp.x), static_cast<float>(pp.y));
         loc[0] += b.x * b.x; loc[1] += b.y * b.y; loc[2] += rr.x * pp.x; loc[3] += rr.y * pp.y;
       }
     }
@@ -630,32 +629,26 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
     if ((!act_s || it_s >= a.imax) && (!act_t || it_t >= a.imax)) break;
     const double stop_s = fmax(a.tol * bnorm_s, kRefineDrop * sqrt(sig_s));
     const double stop_t = fmax(a.tol * bnorm_t, kRefineDrop * sqrt(sig_t));
-    // ---- single-precision-matrix iterations from this residual. Two barriers per iteration: A d is carried by the
-    // recurrence q <- A p + beta q (the product of the new p, gathered once p is complete), so the direction update
-    // d <- p + beta d happens row by row inside the product pass instead of in a pass of its own.
-    bool first = true, upd_s = false, upd_t = false;
-    double beta_s = 0.0, beta_t = 0.0;
+    // ---- single-precision-matrix iterations from this residual (d = p on entry)
+    for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+      const double2 pp = a.p[i0 + r];
+      a.d[i0 + r] = pp;
+      a.df[i0 + r] = make_float2(static_cast<float>(pp.x), static_cast<float>(pp.y));
+    }
+    g.sync();
     for (;;) {
       const bool in_s = act_s && it_s < a.imax && sqrt(sig_s) > stop_s;
       const bool in_t = act_t && it_t < a.imax && sqrt(sig_t) > stop_t;
       if (!in_s && !in_t) break;
-      // w = A p ; d = p + beta d ; q = w + beta q (q = A d) ; partial d.q
+      // q = A d ; partial d.q
       loc[0] = loc[1] = 0.0;
       for (int r = gw; r < n; r += nwarps) {
         const int i = i0 + r;
-        const double2 w = row_mv_f32(d, i, a.eta[i], a.p, a.pf);
+        const double2 y = row_mv_f32(d, i, a.eta[i], a.d, a.df);
         if (lane == 0) {
-          const double2 pp = a.p[i];
-          double2 dd = pp, qq = w;
-          if (!first) {
-            dd = a.d[i];
-            qq = a.q[i];
-            if (upd_s) { dd.x = pp.x + beta_s * dd.x; qq.x = w.x + beta_s * qq.x; }
-            if (upd_t) { dd.y = pp.y + beta_t * dd.y; qq.y = w.y + beta_t * qq.y; }
-          }
-          a.d[i] = dd;
-          a.q[i] = qq;
-          loc[0] += dd.x * qq.x; loc[1] += dd.y * qq.y;
+          a.q[i] = y;
+          const double2 dd = a.d[i];
+          loc[0] += dd.x * y.x; loc[1] += dd.y * y.y;
         }
       }
       block_partials<2>(loc, partbuf(), sh);
@@ -678,20 +671,27 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
         const double eta = a.eta[i];
         const double2 pp = make_double2(rr.x / eta, rr.y / eta);
         a.p[i] = pp;
-        a.pf[i] = make_float2(static_cast<float>(pp.x), static_cast<float>(pp.y));
         loc[0] += rr.x * pp.x; loc[1] += rr.y * pp.y;
       }
       block_partials<2>(loc, partbuf(), sh);
       g.sync();
       grid_totals<2>(partbuf(), gridDim.x, tot, tot_sh);
       ++phase;
-      beta_s = in_s ? tot[0] / sig_s : 0.0;
-      beta_t = in_t ? tot[1] / sig_t : 0.0;
+      const double beta_s = in_s ? tot[0] / sig_s : 0.0;
+      const double beta_t = in_t ? tot[1] / sig_t : 0.0;
       if (in_s) { sig_s = tot[0]; ++it_s; }
       if (in_t) { sig_t = tot[1]; ++it_t; }
-      upd_s = in_s;
-      upd_t = in_t;
-      first = false;
+      // d = p + beta d (only for the right-hand sides still iterating)
+      for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
+        const int i = i0 + r;
+        const double2 pp = a.p[i];
+        double2 dd = a.d[i];
+        if (in_s) dd.x = pp.x + beta_s * dd.x;
+        if (in_t) dd.y = pp.y + beta_t * dd.y;
+        a.d[i] = dd;
+        a.df[i] = make_float2(static_cast<float>(dd.x), static_cast<float>(dd.y));
+      }
+      g.sync();
     }
     if (breakdown) break;
   }

@@ -27,7 +27,7 @@ RX_COMPUTE_QEQ = 1
 RX_COMPUTE_CENSUS = 2
 RX_COMPUTE_QEQ_COLD = 4
 RX_COMPUTE_PERATOM = 8
-TUNE = {"pairs_tpb": 1, "bonds_tpb": 2, "nonbonded_tpb": 3, "hbond_tpb": 4, "atom_tpb": 5, "lone_grid_min": 6, "overlap": 7}
+TUNE = {"pairs_tpb": 1, "bonds_tpb": 2, "nonbonded_tpb": 3, "hbond_tpb": 4, "atom_tpb": 5, "lone_grid_min": 6, "overlap": 7, "cg_blocks_per_sm": 8}
 STATUS = {0: "ok", 1: "invalid", 2: "ffield", 3: "capacity", 4: "cuda", 5: "not_converged", 6: "state", 7: "timeout"}
 EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_forcefield_dump", "rx_forcefield_params",
            "rx_set_control", "rx_set_systems", "rx_num_atoms", "rx_set_positions", "rx_get_positions", "rx_set_charges",
