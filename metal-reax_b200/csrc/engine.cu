@@ -709,8 +709,8 @@ struct Context {
   }
 
   // After the rows, the bonded chain (bond orders, then k_bonded_atom, with the H-bonds on `side_h` and the torsions
-  // on `side_t`) needs no charge, so with tune.overlap it runs on `side` next to the charge solve; the non-bonded pairs
-  // follow the charges on `stream`. Each branch writes its own arrays (fnb, vir_nb; bacc/bfn/fown; *_h; *_t, Tl), and
+  // on `side_t`, then the bonded gathers k_fold and k_dbond) needs no charge, so with tune.overlap it runs on `side`
+  // next to the charge solve; the non-bonded pairs follow the charges on `stream`, and k_force_final joins both. Each branch writes its own arrays (fnb, vir_nb; bacc/bfn/fown; *_h; *_t, Tl), and
   // all join before the gathers, which add them in fixed order, so the schedule changes no result bit. With timing
   // on, every branch runs on `stream`, one after the other, so each phase is timed alone.
   void launch_bonded(const Dev& d) {
@@ -741,11 +741,20 @@ struct Context {
     ++launches;
     k_torsion<<<blocks(static_cast<long long>(na) * bcap, tune.tpb_atom), tune.tpb_atom, 0, ts>>>(d, dff, ctl);
     toc(4);
+    // the bonded gathers need the H-bond and torsion branches but no charge or non-bonded result: they stay on the
+    // bonded branch, so only k_force_final follows the non-bonded pairs
     if (conc) {
-      RXCU(cudaEventRecord(ev_join, bs));
       RXCU(cudaEventRecord(ev_join_h, side_h));
       RXCU(cudaEventRecord(ev_join_t, side_t));
+      RXCU(cudaStreamWaitEvent(bs, ev_join_h, 0));
+      RXCU(cudaStreamWaitEvent(bs, ev_join_t, 0));
     }
+    tic(6, "gather");
+    launches += 2;
+    k_fold<<<blocks(na, 128), 128, 0, bs>>>(d);
+    k_dbond<<<blocks(na, 128), 128, 0, bs>>>(d);
+    toc(6);
+    if (conc) RXCU(cudaEventRecord(ev_join, bs));
   }
 
   void launch_nonbonded(const Dev& d) {
@@ -760,17 +769,11 @@ struct Context {
   }
 
   void launch_gathers(const Dev& d) {
-    if (!timing) {
-      RXCU(cudaStreamWaitEvent(stream, ev_join, 0));
-      RXCU(cudaStreamWaitEvent(stream, ev_join_h, 0));
-      RXCU(cudaStreamWaitEvent(stream, ev_join_t, 0));
-    }
-    tic(6, "gather");
-    launches += 3;
-    k_fold<<<blocks(na, 128), 128, 0, stream>>>(d);
-    k_dbond<<<blocks(na, 128), 128, 0, stream>>>(d);
+    if (!timing) RXCU(cudaStreamWaitEvent(stream, ev_join, 0));
+    tic(7, "force_final");
+    ++launches;
     k_force_final<<<blocks(na, 128), 128, 0, stream>>>(d);
-    toc(6);
+    toc(7);
   }
 
   // One evaluation of every system, enqueued without any host synchronisation: kernels after a failure (a list
