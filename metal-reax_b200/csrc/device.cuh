@@ -140,6 +140,9 @@ struct Dev {
   double4* bfn_t;        // torsion: gradient on the partner (xyz)
   double4* Tl;           // torsion: per (central slot, position in the far atom's slots): gradient xyz, Cdbo (w)
   double4* Ti;           // torsion: per (central slot, position in the central atom's slots): gradient on i, Cdbo of i-j
+  unsigned char* tflag;  // per slot: 1 if it is a listed central bond of the torsions (its torsion rows are written)
+  int* tor_list;         // the listed central-bond slots, in arrival order, and their count
+  int* tor_n;
   double4* Tsum;         // torsion: per central slot, 2 entries: central gradient + CdDelta; e_tor, e_con, count
   double* Tvir;          // torsion: per central slot, kVir virial components
   // atoms

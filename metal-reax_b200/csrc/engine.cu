@@ -134,6 +134,8 @@ struct Context {
   DBuf<float> hhi, hlo;
   DBuf<double4> bdv, bBO, bdBOp, bdlnpi, bdlnpi2, bC0, bC1, bC2, bacc, bfn, Tl, Ti, Tsum, bfn_h, bacc_t, bfn_t;
   DBuf<double> Tvir;
+  DBuf<unsigned char> tflag;
+  DBuf<int> tor_list, tor_n;
   DBuf<double> bcdbo_h;
   // atoms
   DBuf<double> Deltap, Deltap_boc, cdtot, W, eatom;
@@ -227,7 +229,7 @@ struct Context {
     for (int a = 0; a < ff.nt; ++a)
       for (int b = 0; b < ff.nt; ++b) shld[static_cast<size_t>(a) * ff.nt + b] = std::pow(ff.s(a, SB_GAMMA) * ff.s(b, SB_GAMMA), -1.5);
     // single-precision pair table of the non-bonded kernel: alpha, D, r_vdW, (1/gamma_w)^p_vdW1, ecore, acore, rcore,
-    // gamma (Coulomb shielding), lgcij, lgre^6 (12 floats per type pair)
+    // gamma (Coulomb shielding), lgcij, lgre^6, 1/r_vdW, 1/rcore (12 floats per type pair)
     std::vector<float> nbf(static_cast<size_t>(ff.nt) * ff.nt * 12, 0.0f);
     for (int a = 0; a < ff.nt; ++a)
       for (int b = 0; b < ff.nt; ++b) {
@@ -242,6 +244,8 @@ struct Context {
         o[7] = static_cast<float>(ff.p(a, b, TB_GAMMA));
         o[8] = static_cast<float>(ff.p(a, b, TB_LGCIJ));
         o[9] = static_cast<float>(std::pow(ff.p(a, b, TB_LGRE), 6.0));
+        o[10] = static_cast<float>(1.0 / ff.p(a, b, TB_R_VDW));
+        o[11] = static_cast<float>(1.0 / ff.p(a, b, TB_RCORE));
       }
     const size_t nbf_d = nbf.size() / 2;
     // Bond-order reach per type pair: beyond r_bo every uncorrected component BO'_s, BO'_pi, BO'_pipi is below bo_cut/3
@@ -581,6 +585,9 @@ struct Context {
     Ti.ensure(nb * bcap);
     Tsum.ensure(2 * nb);
     Tvir.ensure(nb * kVir);
+    tflag.ensure(nb);
+    tor_list.ensure(nb);
+    tor_n.ensure(1);
   }
 
   Dev dev() {
@@ -599,6 +606,7 @@ struct Context {
     }
     d.bcap = bcap; d.bcode = bcode.p; d.bsym = bsym.p; d.bcnt = bcnt.p; d.bdv = bdv.p; d.bBO = bBO.p; d.bdBOp = bdBOp.p;
     d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p; d.Ti = Ti.p; d.Tsum = Tsum.p; d.Tvir = Tvir.p;
+    d.tflag = tflag.p; d.tor_list = tor_list.p; d.tor_n = tor_n.p;
     d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
     d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.vir_nb = vir_nb.p; d.vir_h = vir_h.p; d.vir_t = vir_t.p;
     d.fown_h = fown_h.p; d.fown_t = fown_t.p; d.fix_h = fix_h.p; d.pe_fix = pe_fix.p; d.pe_on = pe_on; d.bcdbo_h = bcdbo_h.p; d.bfn_h = bfn_h.p; d.bacc_t = bacc_t.p; d.bfn_t = bfn_t.p; d.census = census.p; d.status = status.p;
@@ -667,7 +675,10 @@ struct Context {
     int tpb_pairs = 128, tpb_nb = 128, tpb_hb = 128, tpb_bonds = 128, tpb_atom = 64;
     int lone_grid_min = 4096;
     int overlap = 1;   // bonded chain beside the charge solve
-    int cg_per_sm = 0;   // blocks of the single-system CG per SM (0: as many as fit); changes its summation order
+    // blocks of the single-system CG per SM (0: as many as fit). Two leave half of every SM to the bonded terms that
+    // run beside the solve: on the 24,000-atom water step the solve alone is slower, the step faster. The setting
+    // changes the CG's summation order, so it is one value for every solve of the context.
+    int cg_per_sm = 2;
   } tune;
   int grid_per_sm = 0, seg_per_sm = 0;
   void launch_cg(const Dev& d, CgArgs a) {
@@ -724,7 +735,7 @@ struct Context {
     launches += 4;
     k_bonds<<<blocks(static_cast<long long>(na) * 32, tune.tpb_bonds), tune.tpb_bonds, 0, bs>>>(d, dff, ctl);
     k_bond_sym<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, bs>>>(d);
-    k_bo_correct<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, bs>>>(d, dff);
+    k_bo_correct<<<blocks(static_cast<long long>(na) * bcap, 256), 256, 0, bs>>>(d, dff, ctl);
     k_atom_quantities<<<blocks(na, 128), 128, 0, bs>>>(d, dff);
     toc(2);
     if (conc) {
@@ -739,7 +750,8 @@ struct Context {
     toc(3);
     tic(4, "torsion");
     ++launches;
-    k_torsion<<<blocks(static_cast<long long>(na) * bcap, tune.tpb_atom), tune.tpb_atom, 0, ts>>>(d, dff, ctl);
+    // at most one listed slot per bond (the tag-order end): half the slots bound the list
+    k_torsion<<<blocks((static_cast<long long>(na) * bcap + 1) / 2, tune.tpb_atom), tune.tpb_atom, 0, ts>>>(d, dff, ctl);
     toc(4);
     // the bonded gathers need the H-bond and torsion branches but no charge or non-bonded result: they stay on the
     // bonded branch, so only k_force_final follows the non-bonded pairs
@@ -916,7 +928,7 @@ struct Context {
     pick(&tune.tpb_hb, {64, 128, 256}, [&](int t) { k_hbond<<<blocks(nw, t), t, 0, stream>>>(d, dff, ctl); });
     pick(&tune.tpb_atom, {32, 64, 128}, [&](int t) {
       k_bonded_atom<<<blocks(na, t), t, 0, stream>>>(d, dff, ctl);
-      k_torsion<<<blocks(static_cast<long long>(na) * bcap, t), t, 0, stream>>>(d, dff, ctl);
+      k_torsion<<<blocks((static_cast<long long>(na) * bcap + 1) / 2, t), t, 0, stream>>>(d, dff, ctl);
     });
     RXCU(cudaEventDestroy(a));
     RXCU(cudaEventDestroy(b));

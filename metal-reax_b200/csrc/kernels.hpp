@@ -61,7 +61,7 @@ __global__ void k_energy_sum(Dev d, double* out, double* out_vir);
 
 __global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl);
 __global__ void k_bond_sym(Dev d);
-__global__ void k_bo_correct(Dev d, DevFF ff);
+__global__ void k_bo_correct(Dev d, DevFF ff, DevCtl ctl);
 __global__ void k_atom_quantities(Dev d, DevFF ff);
 __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl);
 __global__ void k_hbond(Dev d, DevFF ff, DevCtl ctl);

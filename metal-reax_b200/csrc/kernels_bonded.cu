@@ -139,6 +139,7 @@ __global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl) {
 }
 
 __global__ void k_bond_sym(Dev d) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d.tor_n = 0;   // the central bonds of this evaluation's torsions (k_bo_correct)
   if (lists_failed(d)) return;
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= static_cast<long long>(d.na) * d.bcap) return;
@@ -161,7 +162,7 @@ __global__ void k_bond_sym(Dev d) {
 
 // terms::bo_correct (include/reaxmetal/terms.hpp:66-132) for every slot, the slot's atom as "i". The corrected bond
 // orders are symmetric in (i, j) bit for bit, so both slots of a bond hold the same values.
-__global__ void k_bo_correct(Dev d, DevFF ff) {
+__global__ void k_bo_correct(Dev d, DevFF ff, DevCtl ctl) {
   if (lists_failed(d)) return;
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= static_cast<long long>(d.na) * d.bcap) return;
@@ -238,6 +239,12 @@ __global__ void k_bo_correct(Dev d, DevFF ff) {
   if (oBO_pi < 1e-10) oBO_pi = 0;
   if (oBO_pi2 < 1e-10) oBO_pi2 = 0;
   d.bBO[t] = make_double4(oBO, oBO_s, oBO_pi, oBO_pi2);
+  {   // a central bond of the torsions (src/cpu/bonded.cpp:487-506): evaluated by the tag-order end, BO above thb_cut.
+      // The slots are listed in any order (each writes only its own rows), so k_torsion runs dense warps.
+    const bool central = oBO > ctl.thb_cut && !skip_by_tag(d, a, j, d.bdv[t]);
+    d.tflag[t] = central ? 1 : 0;
+    if (central) d.tor_list[atomicAdd(d.tor_n, 1)] = static_cast<int>(t);
+  }
   d.bC0[t] = make_double4(C1dbo, C2dbo, C3dbo, C1dbopi);
   d.bC1[t] = make_double4(C2dbopi, C3dbopi, C4dbopi, C1dbopi2);
   d.bC2[t] = make_double4(C2dbopi2, C3dbopi2, C4dbopi2, 0.0);
@@ -723,19 +730,20 @@ __global__ void __launch_bounds__(256) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
 }
 
 // ------------------------------------------------------------------------------------------------ torsion
-// One thread per central bond j -> k (slot t of atom j) that j evaluates (tag order, src/cpu/bonded.cpp:480-506): all
-// bonds i of j (i != k) and l of k (l != j) with the gates of :510 and :530 (i != l as images, a torsion entry for
-// (ti, tj, tk, tl), BO_kl > thb_cut, BO_ij BO_jk BO_kl > thb_cut). Every write goes to slot t's own rows: its
-// coefficients and the gradient of k (bacc_t/bfn_t[t]), the contributions to the bond k-l and the atom l
-// (Tl[t * bcap + position of l in k's slots]) and to the bond j-i and the atom i (Ti[t * bcap + position of i in j's
-// slots]), and j's own gradient, CdDelta, energies, count and virial (Tsum[t], Tvir[t]); k_fold gathers them.
+// One thread per central bond j -> k (slot t of atom j, listed by k_bo_correct: the end that evaluates it in tag order,
+// src/cpu/bonded.cpp:480-506, with BO_jk > thb_cut): all bonds i of j (i != k) and l of k (l != j) with the gates of
+// :510 and :530 (i != l as images, a torsion entry for (ti, tj, tk, tl), BO_kl > thb_cut, BO_ij BO_jk BO_kl > thb_cut).
+// Every write goes to slot t's own rows: its coefficients and the gradient of k (bacc_t/bfn_t[t]), the contributions
+// to the bond k-l and the atom l (Tl[t * bcap + position of l in k's slots]) and to the bond j-i and the atom i
+// (Ti[t * bcap + position of i in j's slots]), and j's own gradient, CdDelta, energies, count and virial (Tsum[t],
+// Tvir[t]); k_fold gathers the rows of the listed slots (tflag) only.
 __global__ void k_torsion(Dev d, DevFF ff, DevCtl ctl) {
   if (lists_failed(d)) return;
   const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (tid >= static_cast<long long>(d.na) * d.bcap) return;
-  const int j = static_cast<int>(tid / d.bcap), pk = static_cast<int>(tid % d.bcap);
+  if (tid >= static_cast<long long>(*d.tor_n)) return;
+  const long long slot = d.tor_list[tid];
+  const int j = static_cast<int>(slot / d.bcap), pk = static_cast<int>(slot % d.bcap);
   const int nbj = min(d.bcnt[j], d.bcap);
-  if (pk >= nbj) return;
   const int type_j = d.type[j];
   const size_t base = static_cast<size_t>(j) * d.bcap;
   const size_t bjk = base + pk;
@@ -958,6 +966,7 @@ __global__ void k_fold(Dev d) {
     double4 own = make_double4(0, 0, 0, 0), en = make_double4(0, 0, 0, 0);
     double vr[kVir] = {0, 0, 0, 0, 0, 0};
     for (int c = 0; c < nb; ++c) {
+      if (!d.tflag[base + c]) continue;
       const double4 t0 = d.Tsum[2 * (base + c)], t1 = d.Tsum[2 * (base + c) + 1];
       own.x += t0.x; own.y += t0.y; own.z += t0.z; own.w += t0.w;
       en.x += t1.x; en.y += t1.y; en.z += t1.z;
@@ -973,24 +982,27 @@ __global__ void k_fold(Dev d) {
     double4 acc = make_double4(0, 0, 0, 0);
     for (int b = 0; b < nb; ++b) {
       const int c = d.bsym[base + b];
+      if (!d.tflag[c]) continue;
       const double4 t = d.Tl[static_cast<size_t>(c) * d.bcap + p];
       acc.x += t.x; acc.y += t.y; acc.z += t.z; acc.w += t.w;
     }
     for (int c = 0; c < nb; ++c) {   // torsions in which the bond a-p is the first bond i-j of a central bond of a
+      if (!d.tflag[base + c]) continue;
       const double4 t = d.Ti[(base + c) * d.bcap + p];
       acc.x += t.x; acc.y += t.y; acc.z += t.z; acc.w += t.w;
     }
-    double4 at = d.bacc_t[base + p];
+    const bool own = d.tflag[base + p] != 0;
+    double4 at = own ? d.bacc_t[base + p] : make_double4(0, 0, 0, 0);
     at.x += acc.w;
     d.bacc_t[base + p] = at;
-    double4 fn = d.bfn_t[base + p];
+    double4 fn = own ? d.bfn_t[base + p] : make_double4(0, 0, 0, 0);
     fn.x += acc.x; fn.y += acc.y; fn.z += acc.z;
     d.bfn_t[base + p] = fn;
   }
   double cd = d.fown[a].w + d.fown_t[a].w;
   for (int b = 0; b < nb; ++b) {
     const int c = d.bsym[base + b];
-    cd += d.bacc[c].w + d.bacc_t[c].w;
+    cd += d.bacc[c].w + (d.tflag[c] ? d.bacc_t[c].w : 0.0);   // .w of a listed slot: k_torsion's, unchanged here
   }
   d.cdtot[a] = cd;
 }

@@ -273,13 +273,6 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
 }
 
 // ------------------------------------------------------------------------------------------------ non-bonded
-// taper_stable (include/reaxmetal/terms.hpp:268-272): the FP32-safe form in t = (r - swa)/(swb - swa)
-__device__ inline void taper_stable_f(float swa, float swb, float r, float& Tap, float& dTap) {
-  const float dd = swb - swa, t = (r - swa) / dd, t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
-  Tap = 1.f - t4 * (35.f - 84.f * t + 70.f * t2 - 20.f * t3);
-  dTap = (t3 * (-140.f + 420.f * t - 420.f * t2 + 140.f * t3)) / (dd * r);
-}
-
 // One warp per atom over its full row (FP32 pair arithmetic, FP64 accumulation). The gradient of atom i collects
 // -CE * dvec from every entry of its own row, so no write ever touches another atom. Energies use the reference's
 // counted pairs (owner-computes rule, classify_nonbonded_entry, src/neighbor/neighbor.cpp:295-310): an entry counts
@@ -295,7 +288,7 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
   const int ti = d.type[i];
   const int cnt = min(d.nbr_cnt[i], d.ncap);
   const float p_vdW1 = static_cast<float>(ff.gp[28]), p_vdW1i = 1.f / p_vdW1;
-  const float swa = static_cast<float>(ff.nonb_low), swb = static_cast<float>(ff.nonb_cut);
+  const float swa = static_cast<float>(ff.nonb_low), inv_dd = static_cast<float>(1.0 / (ff.nonb_cut - ff.nonb_low));
   const float qi = static_cast<float>(d.q[i]);
   const long long tag_i = d.tag[i];
   const int center = (d.S * d.S * d.S - 1) / 2;
@@ -309,53 +302,63 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     const int sidx = static_cast<int>(code >> d.abits);
     double dvd[3];
     pair_dvec_x(d, s, i, j, sidx, xi4, d.x[j], dvd);
-    const float dx = static_cast<float>(dvd[0]), dy = static_cast<float>(dvd[1]), dz = static_cast<float>(dvd[2]);
-    // the exact cut-off test was taken in FP64 when the row was filtered; the pair terms run in FP32
-    const float r = sqrtf(static_cast<float>(dvd[0] * dvd[0] + dvd[1] * dvd[1] + dvd[2] * dvd[2]));
+    // the exact cut-off test was taken in FP64 when the row was filtered; the pair terms run in FP32, division-free:
+    // 1/r from the reciprocal square root, reciprocals of the type-pair constants from the table, exp(a) as the square
+    // of exp(a/2), and the Coulomb shielding through the reciprocal cube root z = (r^3 + gamma^-3)^(-1/3), whose cube
+    // is 1/(r^3 + gamma^-3)
+    const float r2f = static_cast<float>(dvd[0] * dvd[0] + dvd[1] * dvd[1] + dvd[2] * dvd[2]);
+    const float inv_r = rsqrtf(r2f);
+    const float r = r2f * inv_r;
     const int tj = d.type[j];
     const float* pp = ff.nbf + (static_cast<size_t>(ti) * ff.nt + tj) * 12;
     float Tap, dTap;
-    taper_stable_f(swa, swb, r, Tap, dTap);
-    const float alpha = pp[0], D = pp[1], r_vdW = pp[2];
+    {   // taper_stable (include/reaxmetal/terms.hpp:268-272) in t = (r - swa)/(swb - swa)
+      const float t = (r - swa) * inv_dd, t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
+      Tap = 1.f - t4 * (35.f - 84.f * t + 70.f * t2 - 20.f * t3);
+      dTap = (t3 * (-140.f + 420.f * t - 420.f * t2 + 140.f * t3)) * (inv_dd * inv_r);
+    }
+    const float alpha = pp[0], D = pp[1], inv_rvdw = pp[10];
     float e_vdW = 0.f, CEvd;
     if (ff.vdw_type == 1 || ff.vdw_type == 3) {
       const float powr_vdW1 = exp2f(p_vdW1 * __log2f(r));   // r^p and (..)^(1/p) through the fast base-2 pair
       const float sum = powr_vdW1 + pp[3];
       const float fn13 = exp2f(p_vdW1i * __log2f(sum));
-      const float exp1 = __expf(alpha * (1.f - fn13 / r_vdW));
-      const float exp2 = __expf(0.5f * alpha * (1.f - fn13 / r_vdW));
+      const float exp2 = __expf(0.5f * alpha * (1.f - fn13 * inv_rvdw));
+      const float exp1 = exp2 * exp2;
       const float evd = D * (exp1 - 2.f * exp2);
       e_vdW += Tap * evd;
       // (sum)^(1/p - 1) r^(p - 2) = fn13 / sum * powr / r^2
-      const float dfn13 = (fn13 / sum) * (powr_vdW1 / (r * r));
-      CEvd = dTap * evd - Tap * D * (alpha / r_vdW) * (exp1 - exp2) * dfn13;
+      const float dfn13 = __fdividef(fn13, sum) * (powr_vdW1 * inv_r * inv_r);
+      CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * dfn13;
     } else {
-      const float exp1 = __expf(alpha * (1.f - r / r_vdW));
-      const float exp2 = __expf(0.5f * alpha * (1.f - r / r_vdW));
+      const float exp2 = __expf(0.5f * alpha * (1.f - r * inv_rvdw));
+      const float exp1 = exp2 * exp2;
       const float evd = D * (exp1 - 2.f * exp2);
       e_vdW += Tap * evd;
-      CEvd = dTap * evd - Tap * D * (alpha / r_vdW) * (exp1 - exp2) / r;
+      CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * inv_r;
     }
     if (ff.vdw_type == 2 || ff.vdw_type == 3) {
-      const float ecore = pp[4], acore = pp[5], rcore = pp[6];
-      const float e_core = ecore * __expf(acore * (1.f - (r / rcore)));
+      const float ecore = pp[4], acore = pp[5], inv_rcore = pp[11];
+      const float e_core = ecore * __expf(acore * (1.f - r * inv_rcore));
       e_vdW += Tap * e_core;
-      const float de_core = -(acore / rcore) * e_core;
-      CEvd += dTap * e_core + Tap * de_core / r;
+      const float de_core = -(acore * inv_rcore) * e_core;
+      CEvd += dTap * e_core + Tap * de_core * inv_r;
       if (ff.lg) {
-        const float r2f = r * r, r4 = r2f * r2f, r5 = r4 * r, r6 = r4 * r2f, re6 = pp[9];
-        const float e_lg = -(pp[8] / (r6 + re6));
+        const float r4 = r2f * r2f, r5 = r4 * r, r6 = r4 * r2f, re6 = pp[9];
+        const float inv6 = __fdividef(1.f, r6 + re6);
+        const float e_lg = -pp[8] * inv6;
         e_vdW += Tap * e_lg;
-        const float de_lg = -6.f * e_lg * r5 / (r6 + re6);
-        CEvd += dTap * e_lg + Tap * de_lg / r;
+        const float de_lg = -6.f * e_lg * r5 * inv6;
+        CEvd += dTap * e_lg + Tap * de_lg * inv_r;
       }
     }
     const float qj = static_cast<float>(d.q[j]);
-    const float dr3gamij_1 = r * r * r + pp[7];
-    const float dr3gamij_3 = cbrtf(dr3gamij_1);
-    const float e_ele = 332.06371f * qi * qj * (Tap / dr3gamij_3);
-    const float CEclmb = 332.06371f * qi * qj * (dTap - Tap * r / dr3gamij_1) / dr3gamij_3;
+    const float z = rcbrtf(r2f * r + pp[7]);
+    const float cq = 332.06371f * qi * qj;
+    const float e_ele = cq * (Tap * z);
+    const float CEclmb = cq * (dTap - Tap * r * (z * z * z)) * z;
     const float CE = CEvd + CEclmb;
+    const float dx = static_cast<float>(dvd[0]), dy = static_cast<float>(dvd[1]), dz = static_cast<float>(dvd[2]);
     gx -= static_cast<double>(CE * dx);
     gy -= static_cast<double>(CE * dy);
     gz -= static_cast<double>(CE * dz);
