@@ -89,8 +89,11 @@ int rx_get_capacities(const rx_context* ctx, int* out3);
  * skin/2 since the last rebuild (neighbor.cpp:362-374 rebuilds every step; the cut-off decisions of every step are the
  * same either way, taken on the current positions). 0 rebuilds every evaluation. */
 int rx_set_neighbor(rx_context* ctx, double skin);
-int rx_set_positions(rx_context* ctx, const double* x);   /* x[3*NA] */
-int rx_get_positions(rx_context* ctx, double* x);         /* positions as held (wrapped into the primary cell) */
+/* x[3*NA], in any periodic image (each atom is moved to the image the engine's lists use; the lists are rebuilt only
+ * for systems whose atoms moved more than skin/2 since their last rebuild) */
+int rx_set_positions(rx_context* ctx, const double* x);
+/* positions as held: wrapped into the primary cell at the last list rebuild of their system, unwrapped since */
+int rx_get_positions(rx_context* ctx, double* x);
 int rx_set_charges(rx_context* ctx, const double* q);     /* q[NA] */
 int rx_get_charges(rx_context* ctx, double* q);
 

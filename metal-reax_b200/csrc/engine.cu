@@ -1013,7 +1013,8 @@ struct Context {
     double4* h = stage(static_cast<size_t>(na));
     for (int a = 0; a < na; ++a) h[a] = make_double4(xin[3 * a], xin[3 * a + 1], xin[3 * a + 2], 0.0);
     RXCU(cudaMemcpyAsync(x.p, h, sizeof(double4) * na, cudaMemcpyHostToDevice, stream));
-    force_rebuild();
+    // no forced rebuild: the next evaluation's Verlet check moves every atom to the periodic image of the engine's
+    // rows and rebuilds the systems whose atoms moved more than skin/2 (or whose layout fit_nonperiodic changed)
     RXCU(cudaStreamSynchronize(stream));
     have_pos = true;
     forces_valid = false;

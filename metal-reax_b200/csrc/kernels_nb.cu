@@ -22,7 +22,25 @@ __global__ void k_nbr_check(Dev d) {
   }
   if (*reinterpret_cast<volatile const int*>(d.sys_flag + s)) return;
   const double4 r = d.xref[a];
-  const double dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
+  double dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
+  {   // positions handed in by a caller may sit in another periodic image than the engine's own (wrapped at the last
+      // rebuild): the atom moves to the image nearest its reference position, so that the rows' lattice shifts hold
+    const SysInfo& sy = d.sys[s];
+    double n[3];
+    bool shift = false;
+    for (int k = 0; k < 3; ++k) {
+      n[k] = sy.per[k] ? rint(sy.R[3 * k] * dx + sy.R[3 * k + 1] * dy + sy.R[3 * k + 2] * dz) : 0.0;
+      shift = shift || n[k] != 0.0;
+    }
+    if (shift) {
+      double4 y = x;
+      y.x -= n[0] * sy.L[0] + n[1] * sy.L[3] + n[2] * sy.L[6];
+      y.y -= n[0] * sy.L[1] + n[1] * sy.L[4] + n[2] * sy.L[7];
+      y.z -= n[0] * sy.L[2] + n[1] * sy.L[5] + n[2] * sy.L[8];
+      d.x[a] = y;
+      dx = y.x - r.x; dy = y.y - r.y; dz = y.z - r.z;
+    }
+  }
   if (dx * dx + dy * dy + dz * dz > d.half_skin2) atomicOr(d.sys_flag + s, 1);
 }
 
