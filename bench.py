@@ -252,15 +252,19 @@ def e2e_run(device, s, v, steps, warmup):
     stream = torch.cuda.ExternalStream(e.stream(), device=torch.device("cuda", device))
     out = e.compute(qeq=True)
     g = out["grad"]
+    kick = 0.5 * DT * ftm2v / m          # per-atom half-kick factor
+    tmp = np.empty_like(x)
 
-    def step():
-        nonlocal x, vel, g
-        vel -= 0.5 * DT * ftm2v * g / m
-        x += DT * vel
+    def step():                         # velocity Verlet on the host, in place
+        nonlocal g
+        np.multiply(g, kick, out=tmp)
+        vel -= tmp
+        np.multiply(vel, DT, out=tmp)
+        x += tmp
         e.set_positions(x)
-        r = e.compute(qeq=True)
-        g = r["grad"]
-        vel -= 0.5 * DT * ftm2v * g / m
+        g = e.compute(qeq=True)["grad"]
+        np.multiply(g, kick, out=tmp)
+        vel -= tmp
 
     for _ in range(warmup):
         step()

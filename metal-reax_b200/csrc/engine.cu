@@ -162,12 +162,39 @@ struct Context {
   DBuf<int> kfirst, ksys;
   MdDev md{};
   long long md_step = 0;
-  // pinned host staging for per-step positions in and gradients out
+  // pinned host staging for per-step positions in and gradients out, and for the small results of an evaluation
+  // (status words, CG counts, energies), so that one synchronisation brings all of them back
   double4* pinned = nullptr;
   size_t pinned_n = 0;
+  char* pin_small = nullptr;
+  size_t pin_small_n = 0;
+  double* pin_e = nullptr;
+  size_t pin_e_n = 0;
+  double* energy_stage(size_t n) {
+    if (pin_e_n < n) {
+      if (pin_e) cudaFreeHost(pin_e);
+      pin_e = nullptr;
+      pin_e_n = 0;
+      RXCU(cudaMallocHost(&pin_e, n * sizeof(double)));
+      pin_e_n = n;
+    }
+    return pin_e;
+  }
+  char* small_stage(size_t bytes) {
+    if (pin_small_n < bytes) {
+      if (pin_small) cudaFreeHost(pin_small);
+    if (pin_e) cudaFreeHost(pin_e);
+      pin_small = nullptr;
+      pin_small_n = 0;
+      RXCU(cudaMallocHost(&pin_small, bytes));
+      pin_small_n = bytes;
+    }
+    return pin_small;
+  }
   double4* stage(size_t n) {
     if (pinned_n < n) {
       if (pinned) cudaFreeHost(pinned);
+    if (pin_small) cudaFreeHost(pin_small);
       pinned = nullptr;
       pinned_n = 0;
       RXCU(cudaMallocHost(&pinned, n * sizeof(double4)));
@@ -858,10 +885,20 @@ struct Context {
 
   // One force evaluation of every system, with grow-and-retry of the list capacities (neighbor.cpp:362-374,
   // bonded_device.cpp:117-190). With `do_qeq` the charges are equilibrated first and the histories advanced on success.
-  void evaluate(bool do_qeq) {
+  void evaluate(bool do_qeq) { evaluate_with(do_qeq, [] {}); }
+
+  // `tail` enqueues work ordered after the evaluation (result sums and copies into pinned memory); it is repeated with
+  // the evaluation when the lists are regrown, and the one synchronisation waits for both
+  template <class Tail>
+  void evaluate_with(bool do_qeq, Tail&& tail) {
     require_ff();
     require_sys();
     if (!have_pos) throw Error(RX_ERR_STATE, "no positions set");
+    const size_t n2 = 2 * static_cast<size_t>(nsys);
+    char* sm = small_stage(sizeof(int) * (kStatusWords + n2) + sizeof(double) * n2);
+    int* st = reinterpret_cast<int*>(sm);
+    int* it = st + kStatusWords;
+    double* rl = reinterpret_cast<double*>(sm + sizeof(int) * (kStatusWords + n2));
     for (int attempt = 0;; ++attempt) {
       RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * kStatusWords, stream));
       const int gi = do_qeq ? 1 : 0;
@@ -872,11 +909,18 @@ struct Context {
       } else {
         enqueue_eval(do_qeq);
       }
-      if (do_qeq) fetch_qeq_counts();
-      int st[kStatusWords];
-      RXCU(cudaMemcpyAsync(st, status.p, sizeof st, cudaMemcpyDeviceToHost, stream));
+      if (do_qeq) {
+        RXCU(cudaMemcpyAsync(it, cg_iters.p, sizeof(int) * n2, cudaMemcpyDeviceToHost, stream));
+        RXCU(cudaMemcpyAsync(rl, cg_rel.p, sizeof(double) * n2, cudaMemcpyDeviceToHost, stream));
+      }
+      tail();
+      RXCU(cudaMemcpyAsync(st, status.p, sizeof(int) * kStatusWords, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaStreamSynchronize(stream));
       RXCU(cudaGetLastError());
+      if (do_qeq) {
+        last_iters.assign(it, it + n2);
+        last_rel.assign(rl, rl + n2);
+      }
       if (grow_from_status(st, attempt)) {
         force_rebuild();
         continue;
@@ -1058,15 +1102,18 @@ struct Context {
       pe_on = want_pe;
       drop_graph();
     }
-    evaluate((flags & RX_COMPUTE_QEQ) != 0);
+    double4* g = g_out ? stage(static_cast<size_t>(na)) : nullptr;
+    double* eh = nullptr;
+    evaluate_with((flags & RX_COMPUTE_QEQ) != 0, [&] {
+      energy_sums();
+      if (e_out) {
+        eh = energy_stage(static_cast<size_t>(kTerms) * nsys);
+        RXCU(cudaMemcpyAsync(eh, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
+      }
+      if (g) RXCU(cudaMemcpyAsync(g, grad.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, stream));
+    });
     have_peratom = pe_on != 0;
-    energy_sums();
-    if (e_out) RXCU(cudaMemcpyAsync(e_out, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
-    double4* g = nullptr;
-    if (g_out) {
-      g = stage(static_cast<size_t>(na));
-      RXCU(cudaMemcpyAsync(g, grad.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, stream));
-    }
+    if (e_out) std::copy(eh, eh + static_cast<size_t>(kTerms) * nsys, e_out);
     if (cen_out) RXCU(cudaMemcpyAsync(cen_out, census.p, sizeof(int) * kCensus * na, cudaMemcpyDeviceToHost, stream));
     std::vector<int> nb, bc;
     if (counts) {
@@ -1075,7 +1122,7 @@ struct Context {
       RXCU(cudaMemcpyAsync(nb.data(), nbr_cnt.p, sizeof(int) * na, cudaMemcpyDeviceToHost, stream));
       RXCU(cudaMemcpyAsync(bc.data(), bcnt.p, sizeof(int) * na, cudaMemcpyDeviceToHost, stream));
     }
-    RXCU(cudaStreamSynchronize(stream));
+    if (cen_out || counts) RXCU(cudaStreamSynchronize(stream));
     if (g_out)
       for (int a = 0; a < na; ++a) { g_out[3 * a] = g[a].x; g_out[3 * a + 1] = g[a].y; g_out[3 * a + 2] = g[a].z; }
     if (counts) {

@@ -240,8 +240,8 @@ class Engine:
 
     # ---- evaluation
     def compute(self, qeq=False, census=False, counts=False, cold=False, peratom=False):
-        e = np.zeros(13 * self.nsys)
-        g = np.zeros(3 * self.na)
+        e = np.empty(13 * self.nsys)   # every entry is written by rx_compute
+        g = np.empty(3 * self.na)
         cen = np.zeros(7 * self.na, dtype=np.int32) if census else None
         cnt = np.zeros(4, dtype=np.int64) if counts else None
         flags = (RX_COMPUTE_QEQ if qeq else 0) | (RX_COMPUTE_CENSUS if census else 0) | (RX_COMPUTE_QEQ_COLD if cold else 0) | \
