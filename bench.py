@@ -256,7 +256,7 @@ def e2e_run(device, s, v, steps, warmup):
     tmp = np.empty_like(x)
 
     def step():                         # velocity Verlet on the host, in place
-        nonlocal g
+        nonlocal g, vel, x
         np.multiply(g, kick, out=tmp)
         vel -= tmp
         np.multiply(vel, DT, out=tmp)
