@@ -137,8 +137,7 @@ def phase_impl_bytes(name, N, E, D, I, R=1, EV=None):
 
 
 PHASE_KERNEL = {"neighbors": "k_neighbors", "qeq": "k_cg_grid", "bond_orders": "k_bonds", "bonded_terms": "k_bonded_atom",
-                "torsion": "k_torsion", "nonbonded": "k_nonbonded<2>", "vdw": "k_nonbonded<1>", "gather": "k_fold",
-                "force_final": "k_force_final"}
+                "torsion": "k_torsion", "nonbonded": "k_nonbonded", "gather": "k_fold", "force_final": "k_force_final"}
 
 
 def profiled_traffic(kernel, passes):

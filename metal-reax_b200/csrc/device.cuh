@@ -157,8 +157,7 @@ struct Dev {
   double* cdtot;
   double* W;
   double4* fdb;
-  double4* fnb;          // non-bonded gradient: Coulomb part (k_nonbonded<2>, k_acks2)
-  double4* fnb_v;        // non-bonded gradient: van der Waals part (k_nonbonded<1>)
+  double4* fnb;          // non-bonded gradient
   double4* grad;         // result
   double* eatom;         // kTerms per atom
   unsigned long long* pe_fix;   // per-atom energy tallies (fixed point, 2^32 units), written when pe_on
@@ -166,8 +165,7 @@ struct Dev {
   double* vir;           // kVir per atom: virial of the bonded interactions this atom centres (LAMMPS order xx yy zz xy xz yz)
   double* vir_h;         // kVir per atom: H-bond triples centred on this hydrogen
   double* vir_t;         // kVir per atom: torsions centred on this atom
-  double* vir_nb;        // kVir per atom: half the virial of the atom's non-bonded pairs, Coulomb part
-  double* vir_v;         // the same, van der Waals part
+  double* vir_nb;        // kVir per atom: half the virial of the atom's non-bonded pairs
   int* census;           // kCensus per atom (atom-major: census[c*na + a])
   int* status;
   long long* counters;   // [0] neighbor entries, [1] counted pairs, [2] bonds (directed), [3] H-bond triples

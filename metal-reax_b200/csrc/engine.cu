@@ -76,10 +76,10 @@ struct Context {
   int device = 0;
   int nsm = 0;
   cudaStream_t stream = nullptr;
-  // concurrent branches of an evaluation: the bonded chain (side), H-bonds (side_h), torsions (side_t) and the van
-  // der Waals pairs (side_v) next to the charge solve and the Coulomb pairs on `stream`
-  cudaStream_t side = nullptr, side_h = nullptr, side_t = nullptr, side_v = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join_h = nullptr, ev_join_t = nullptr, ev_join_v = nullptr;
+  // concurrent branches of an evaluation: the bonded chain (side), H-bonds (side_h) and torsions (side_t) next to
+  // the charge solve and the non-bonded pairs on `stream`
+  cudaStream_t side = nullptr, side_h = nullptr, side_t = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join_h = nullptr, ev_join_t = nullptr;
   // one captured MD step (replayed for every step of rx_md_run); dropped whenever a buffer or a parameter it holds
   // changes
   cudaGraphExec_t md_graph = nullptr;
@@ -139,13 +139,13 @@ struct Context {
   DBuf<double> bcdbo_h;
   // atoms
   DBuf<double> Deltap, Deltap_boc, cdtot, W, eatom;
-  DBuf<double4> dDp_self, fown, fdb, fnb, fnb_v, grad, fown_h, fown_t;
+  DBuf<double4> dDp_self, fown, fdb, fnb, grad, fown_h, fown_t;
   DBuf<unsigned long long> fix_h, pe_fix;
   int pe_on = 0;
   DBuf<AtomQ> aq;
   DBuf<int> census, status;
   DBuf<long long> counters;
-  DBuf<double> energies, virial, vir, vir_nb, vir_v, vir_h, vir_t;
+  DBuf<double> energies, virial, vir, vir_nb, vir_h, vir_t;
   // QEq
   DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
   DBuf<float2> cg_df;
@@ -223,8 +223,8 @@ struct Context {
     RXCU(cudaSetDevice(dev));
     RXCU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     RXCU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    for (cudaStream_t* st : {&side, &side_h, &side_t, &side_v}) RXCU(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
-    for (cudaEvent_t* ev : {&ev_fork, &ev_join, &ev_fork2, &ev_join_h, &ev_join_t, &ev_join_v}) RXCU(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    for (cudaStream_t* st : {&side, &side_h, &side_t}) RXCU(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
+    for (cudaEvent_t* ev : {&ev_fork, &ev_join, &ev_fork2, &ev_join_h, &ev_join_t}) RXCU(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
     status.ensure(kStatusWords);
     counters.ensure(8);
     set_qeq(0.0, 10.0, 1e-6, 200, 0);
@@ -234,9 +234,9 @@ struct Context {
     if (pinned) cudaFreeHost(pinned);
     drop_graph();
     for (auto& p : phases) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
-    for (cudaEvent_t ev : {ev_fork, ev_join, ev_fork2, ev_join_h, ev_join_t, ev_join_v})
+    for (cudaEvent_t ev : {ev_fork, ev_join, ev_fork2, ev_join_h, ev_join_t})
       if (ev) cudaEventDestroy(ev);
-    for (cudaStream_t st : {side, side_h, side_t, side_v})
+    for (cudaStream_t st : {side, side_h, side_t})
       if (st) cudaStreamDestroy(st);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -580,14 +580,14 @@ struct Context {
   void alloc_atoms() {
     const size_t n = static_cast<size_t>(na);
     Deltap.ensure(n); Deltap_boc.ensure(n); cdtot.ensure(n); W.ensure(n); eatom.ensure(n * kTerms);
-    dDp_self.ensure(n); fown.ensure(n); fdb.ensure(n); fnb.ensure(n); fnb_v.ensure(n); grad.ensure(n);
+    dDp_self.ensure(n); fown.ensure(n); fdb.ensure(n); fnb.ensure(n); grad.ensure(n);
     aq.ensure(n); census.ensure(n * kCensus);
     nbr_cnt.ensure(n); bcnt.ensure(n); near_cnt.ensure(n); vcnt.ensure(n); xref.ensure(n);
     sys_flag.ensure(static_cast<size_t>(nsys)); cg_nref.ensure(1); cg_brk.ensure(static_cast<size_t>(nsys));
     energies.ensure(static_cast<size_t>(nsys) * kTerms);
     virial.ensure(static_cast<size_t>(nsys) * kVir);
     vir.ensure(n * kVir);
-    vir_nb.ensure(n * kVir); vir_v.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
+    vir_nb.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
     fown_h.ensure(n); fown_t.ensure(n); fix_h.ensure(3 * n); pe_fix.ensure(n);
     cg_x.ensure(n); cg_df.ensure(n); cg_b.ensure(n); cg_r.ensure(n); cg_d.ensure(n); cg_p.ensure(n); cg_q.ensure(n); cg_eta.ensure(n);
     cg_iters.ensure(2 * static_cast<size_t>(nsys)); cg_rel.ensure(2 * static_cast<size_t>(nsys));
@@ -635,7 +635,7 @@ struct Context {
     d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p; d.Ti = Ti.p; d.Tsum = Tsum.p; d.Tvir = Tvir.p;
     d.tflag = tflag.p; d.tor_list = tor_list.p; d.tor_n = tor_n.p;
     d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
-    d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.fnb_v = fnb_v.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.vir_nb = vir_nb.p; d.vir_v = vir_v.p; d.vir_h = vir_h.p; d.vir_t = vir_t.p;
+    d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.vir_nb = vir_nb.p; d.vir_h = vir_h.p; d.vir_t = vir_t.p;
     d.fown_h = fown_h.p; d.fown_t = fown_t.p; d.fix_h = fix_h.p; d.pe_fix = pe_fix.p; d.pe_on = pe_on; d.bcdbo_h = bcdbo_h.p; d.bfn_h = bfn_h.p; d.bacc_t = bacc_t.p; d.bfn_t = bfn_t.p; d.census = census.p; d.status = status.p;
     d.counters = counters.p;
     return d;
@@ -748,10 +748,9 @@ struct Context {
 
   // After the rows, the bonded chain (bond orders, then k_bonded_atom, with the H-bonds on `side_h` and the torsions
   // on `side_t`, then the bonded gathers k_fold and k_dbond) needs no charge, so with tune.overlap it runs on `side`
-  // next to the charge solve, as do the van der Waals pairs on `side_v`; the Coulomb pairs follow the charges on
-  // `stream`, and k_force_final joins all branches. Each branch writes its own arrays (fnb, vir_nb; fnb_v, vir_v;
-  // bacc/bfn/fown; *_h; *_t, Tl), which k_force_final and the sums add in fixed order, so the schedule changes no
-  // result bit. With timing on, every branch runs on `stream`, one after the other, so each phase is timed alone.
+  // next to the charge solve; the non-bonded pairs follow the charges on `stream`, and k_force_final joins both. Each branch writes its own arrays (fnb, vir_nb; bacc/bfn/fown; *_h; *_t, Tl), and
+  // all join before the gathers, which add them in fixed order, so the schedule changes no result bit. With timing
+  // on, every branch runs on `stream`, one after the other, so each phase is timed alone.
   void launch_bonded(const Dev& d) {
     const bool conc = !timing;
     cudaStream_t bs = conc ? side : stream, hs = conc ? side_h : stream, ts = conc ? side_t : stream;
@@ -797,22 +796,10 @@ struct Context {
     if (conc) RXCU(cudaEventRecord(ev_join, bs));
   }
 
-  // the van der Waals pairs need no charge: on `side_v` from the fork after the rows, beside everything else
-  void launch_vdw(const Dev& d) {
-    const bool conc = !timing;
-    cudaStream_t vs = conc ? side_v : stream;
-    if (conc) RXCU(cudaStreamWaitEvent(side_v, ev_fork, 0));
-    tic(8, "vdw");
-    ++launches;
-    k_nonbonded<1><<<blocks(static_cast<long long>(na) * 32, tune.tpb_nb), tune.tpb_nb, 0, vs>>>(d, dff);
-    toc(8);
-    if (conc) RXCU(cudaEventRecord(ev_join_v, side_v));
-  }
-
   void launch_nonbonded(const Dev& d) {
     tic(5, "nonbonded");
     ++launches;
-    k_nonbonded<2><<<blocks(static_cast<long long>(na) * 32, tune.tpb_nb), tune.tpb_nb, 0, stream>>>(d, dff);
+    k_nonbonded<<<blocks(static_cast<long long>(na) * 32, tune.tpb_nb), tune.tpb_nb, 0, stream>>>(d, dff);
     if (acks2_on) {
       ++launches;
       k_acks2<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, s_kin.p);
@@ -821,10 +808,7 @@ struct Context {
   }
 
   void launch_gathers(const Dev& d) {
-    if (!timing) {
-      RXCU(cudaStreamWaitEvent(stream, ev_join, 0));
-      RXCU(cudaStreamWaitEvent(stream, ev_join_v, 0));
-    }
+    if (!timing) RXCU(cudaStreamWaitEvent(stream, ev_join, 0));
     tic(7, "force_final");
     ++launches;
     k_force_final<<<blocks(na, 128), 128, 0, stream>>>(d);
@@ -839,12 +823,10 @@ struct Context {
     build_lists(d);
     if (tune.overlap) {
       launch_bonded(d);
-      launch_vdw(d);
       if (do_qeq) launch_qeq(d);
     } else {
       if (do_qeq) launch_qeq(d);
       launch_bonded(d);
-      launch_vdw(d);
     }
     launch_nonbonded(d);
     launch_gathers(d);
@@ -986,10 +968,7 @@ struct Context {
     };
     pick(&tune.tpb_pairs, {64, 128, 256}, [&](int t) { k_pairs<<<blocks(nw, t), t, 0, stream>>>(d, dff, qp); });
     pick(&tune.tpb_bonds, {64, 128, 256}, [&](int t) { k_bonds<<<blocks(nw, t), t, 0, stream>>>(d, dff, ctl); });
-    pick(&tune.tpb_nb, {64, 128, 256}, [&](int t) {
-      k_nonbonded<1><<<blocks(nw, t), t, 0, stream>>>(d, dff);
-      k_nonbonded<2><<<blocks(nw, t), t, 0, stream>>>(d, dff);
-    });
+    pick(&tune.tpb_nb, {64, 128, 256}, [&](int t) { k_nonbonded<<<blocks(nw, t), t, 0, stream>>>(d, dff); });
     pick(&tune.tpb_hb, {64, 128, 256}, [&](int t) { k_hbond<<<blocks(nw, t), t, 0, stream>>>(d, dff, ctl); });
     pick(&tune.tpb_atom, {32, 64, 128}, [&](int t) {
       k_bonded_atom<<<blocks(na, t), t, 0, stream>>>(d, dff, ctl);
@@ -1172,13 +1151,12 @@ struct Context {
     }
     if (vatom_out) {
       const size_t m = static_cast<size_t>(na) * kVir;
-      std::vector<double> v1(m), v2(m), v3(m), v4(m), v5(m);
+      std::vector<double> v1(m), v2(m), v3(m), v4(m);
       RXCU(cudaMemcpy(v1.data(), vir.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
       RXCU(cudaMemcpy(v2.data(), vir_h.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
       RXCU(cudaMemcpy(v3.data(), vir_t.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
       RXCU(cudaMemcpy(v4.data(), vir_nb.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
-      RXCU(cudaMemcpy(v5.data(), vir_v.p, sizeof(double) * m, cudaMemcpyDeviceToHost));
-      for (size_t k = 0; k < m; ++k) vatom_out[k] = (((v1[k] + v2[k]) + v3[k]) + v5[k]) + v4[k];
+      for (size_t k = 0; k < m; ++k) vatom_out[k] = ((v1[k] + v2[k]) + v3[k]) + v4[k];
     }
   }
 

@@ -49,8 +49,7 @@ __global__ void k_cell_start(Dev d, const int* sorted_keys);
 __global__ void k_nbr_check(Dev d);
 __global__ void k_neighbors(Dev d);
 __global__ void k_pairs(Dev d, DevFF ff, QeqParams qp);
-template <int PART>
-__global__ void k_nonbonded(Dev d, DevFF ff);   // PART 1: van der Waals, 2: Coulomb + polarization
+__global__ void k_nonbonded(Dev d, DevFF ff);
 __global__ void k_acks2(Dev d, DevFF ff, const double* s_kin);
 __global__ void k_cg_grid(Dev d, CgArgs a);
 __global__ void k_cg_seg(Dev d, CgArgs a);

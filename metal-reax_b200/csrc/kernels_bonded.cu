@@ -1059,9 +1059,8 @@ __global__ void k_force_final(Dev d) {
   if (a >= d.na) return;
   const int nb = min(d.bcnt[a], d.bcap);
   const size_t base = static_cast<size_t>(a) * d.bcap;
-  const double4 f1 = d.fown[a], fh = d.fown_h[a], ft = d.fown_t[a], f2 = d.fdb[a], fv = d.fnb_v[a], f3 = d.fnb[a];
-  double g[3] = {f1.x + fh.x + ft.x + f2.x + fv.x + f3.x, f1.y + fh.y + ft.y + f2.y + fv.y + f3.y,
-                 f1.z + fh.z + ft.z + f2.z + fv.z + f3.z};
+  const double4 f1 = d.fown[a], fh = d.fown_h[a], ft = d.fown_t[a], f2 = d.fdb[a], f3 = d.fnb[a];
+  double g[3] = {f1.x + fh.x + ft.x + f2.x + f3.x, f1.y + fh.y + ft.y + f2.y + f3.y, f1.z + fh.z + ft.z + f2.z + f3.z};
   for (int c = 0; c < 3; ++c) g[c] += fix_value(d.fix_h[3 * static_cast<size_t>(a) + c]);   // H-bond acceptor gradient
   for (int k = 0; k < nb; ++k) {
     const size_t b = base + k;

@@ -291,15 +291,11 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
 }
 
 // ------------------------------------------------------------------------------------------------ non-bonded
-// One warp per atom over its full row (FP32 pair arithmetic, FP64 accumulation), in two parts: PART 1 the van der
-// Waals terms (terms::nonbonded_pair without the Coulomb term, terms.hpp:282-323), which need no charge and run beside
-// the charge solve; PART 2 the shielded Coulomb term (q_i q_j C_ele Tap / cbrt(r^3 + gamma^-3)) and the polarization
-// energy, after it. The gradient of atom i collects -CE * dvec from every entry of its own row, so no write ever
-// touches another atom. Energies use the reference's counted pairs (owner-computes rule, classify_nonbonded_entry,
-// src/neighbor/neighbor.cpp:295-310): an entry counts at i if it is owned-owned with j > i, or a periodic image with
-// tag_i < tag_j or, for an image of i itself, the positive direction; each counted entry contributes its full pair
-// energy.
-template <int PART>
+// One warp per atom over its full row (FP32 pair arithmetic, FP64 accumulation). The gradient of atom i collects
+// -CE * dvec from every entry of its own row, so no write ever touches another atom. Energies use the reference's
+// counted pairs (owner-computes rule, classify_nonbonded_entry, src/neighbor/neighbor.cpp:295-310): an entry counts
+// at i if it is owned-owned with j > i, or a periodic image with tag_i < tag_j or, for an image of i itself, the
+// positive direction; each counted entry contributes its full pair energy (terms::nonbonded_pair, terms.hpp:282-323).
 __global__ void k_nonbonded(Dev d, DevFF ff) {
   if (lists_failed(d)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -311,10 +307,10 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
   const int cnt = min(d.nbr_cnt[i], d.ncap);
   const float p_vdW1 = static_cast<float>(ff.gp[28]), p_vdW1i = 1.f / p_vdW1;
   const float swa = static_cast<float>(ff.nonb_low), inv_dd = static_cast<float>(1.0 / (ff.nonb_cut - ff.nonb_low));
-  const float qi = PART == 2 ? static_cast<float>(d.q[i]) : 0.f;
+  const float qi = static_cast<float>(d.q[i]);
   const long long tag_i = d.tag[i];
   const int center = (d.S * d.S * d.S - 1) / 2;
-  double gx = 0, gy = 0, gz = 0, en = 0, ehalf = 0;
+  double gx = 0, gy = 0, gz = 0, ev = 0, ee = 0, ehalf = 0;
   float v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;   // pair virial, half per directed entry (lane partials)
   int counted = 0;
   const double4 xi4 = d.x[i];
@@ -339,52 +335,47 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
       Tap = 1.f - t4 * (35.f - 84.f * t + 70.f * t2 - 20.f * t3);
       dTap = (t3 * (-140.f + 420.f * t - 420.f * t2 + 140.f * t3)) * (inv_dd * inv_r);
     }
-    float e_pair, CE;
-    if (PART == 1) {
-      const float alpha = pp[0], D = pp[1], inv_rvdw = pp[10];
-      float e_vdW = 0.f, CEvd;
-      if (ff.vdw_type == 1 || ff.vdw_type == 3) {
-        const float powr_vdW1 = exp2f(p_vdW1 * __log2f(r));   // r^p and (..)^(1/p) through the fast base-2 pair
-        const float sum = powr_vdW1 + pp[3];
-        const float fn13 = exp2f(p_vdW1i * __log2f(sum));
-        const float exp2 = __expf(0.5f * alpha * (1.f - fn13 * inv_rvdw));
-        const float exp1 = exp2 * exp2;
-        const float evd = D * (exp1 - 2.f * exp2);
-        e_vdW += Tap * evd;
-        // (sum)^(1/p - 1) r^(p - 2) = fn13 / sum * powr / r^2
-        const float dfn13 = __fdividef(fn13, sum) * (powr_vdW1 * inv_r * inv_r);
-        CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * dfn13;
-      } else {
-        const float exp2 = __expf(0.5f * alpha * (1.f - r * inv_rvdw));
-        const float exp1 = exp2 * exp2;
-        const float evd = D * (exp1 - 2.f * exp2);
-        e_vdW += Tap * evd;
-        CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * inv_r;
-      }
-      if (ff.vdw_type == 2 || ff.vdw_type == 3) {
-        const float ecore = pp[4], acore = pp[5], inv_rcore = pp[11];
-        const float e_core = ecore * __expf(acore * (1.f - r * inv_rcore));
-        e_vdW += Tap * e_core;
-        const float de_core = -(acore * inv_rcore) * e_core;
-        CEvd += dTap * e_core + Tap * de_core * inv_r;
-        if (ff.lg) {
-          const float r4 = r2f * r2f, r5 = r4 * r, r6 = r4 * r2f, re6 = pp[9];
-          const float inv6 = __fdividef(1.f, r6 + re6);
-          const float e_lg = -pp[8] * inv6;
-          e_vdW += Tap * e_lg;
-          const float de_lg = -6.f * e_lg * r5 * inv6;
-          CEvd += dTap * e_lg + Tap * de_lg * inv_r;
-        }
-      }
-      e_pair = e_vdW;
-      CE = CEvd;
+    const float alpha = pp[0], D = pp[1], inv_rvdw = pp[10];
+    float e_vdW = 0.f, CEvd;
+    if (ff.vdw_type == 1 || ff.vdw_type == 3) {
+      const float powr_vdW1 = exp2f(p_vdW1 * __log2f(r));   // r^p and (..)^(1/p) through the fast base-2 pair
+      const float sum = powr_vdW1 + pp[3];
+      const float fn13 = exp2f(p_vdW1i * __log2f(sum));
+      const float exp2 = __expf(0.5f * alpha * (1.f - fn13 * inv_rvdw));
+      const float exp1 = exp2 * exp2;
+      const float evd = D * (exp1 - 2.f * exp2);
+      e_vdW += Tap * evd;
+      // (sum)^(1/p - 1) r^(p - 2) = fn13 / sum * powr / r^2
+      const float dfn13 = __fdividef(fn13, sum) * (powr_vdW1 * inv_r * inv_r);
+      CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * dfn13;
     } else {
-      const float qj = static_cast<float>(d.q[j]);
-      const float z = rcbrtf(r2f * r + pp[7]);
-      const float cq = 332.06371f * qi * qj;
-      e_pair = cq * (Tap * z);
-      CE = cq * (dTap - Tap * r * (z * z * z)) * z;
+      const float exp2 = __expf(0.5f * alpha * (1.f - r * inv_rvdw));
+      const float exp1 = exp2 * exp2;
+      const float evd = D * (exp1 - 2.f * exp2);
+      e_vdW += Tap * evd;
+      CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * inv_r;
     }
+    if (ff.vdw_type == 2 || ff.vdw_type == 3) {
+      const float ecore = pp[4], acore = pp[5], inv_rcore = pp[11];
+      const float e_core = ecore * __expf(acore * (1.f - r * inv_rcore));
+      e_vdW += Tap * e_core;
+      const float de_core = -(acore * inv_rcore) * e_core;
+      CEvd += dTap * e_core + Tap * de_core * inv_r;
+      if (ff.lg) {
+        const float r4 = r2f * r2f, r5 = r4 * r, r6 = r4 * r2f, re6 = pp[9];
+        const float inv6 = __fdividef(1.f, r6 + re6);
+        const float e_lg = -pp[8] * inv6;
+        e_vdW += Tap * e_lg;
+        const float de_lg = -6.f * e_lg * r5 * inv6;
+        CEvd += dTap * e_lg + Tap * de_lg * inv_r;
+      }
+    }
+    const float qj = static_cast<float>(d.q[j]);
+    const float z = rcbrtf(r2f * r + pp[7]);
+    const float cq = 332.06371f * qi * qj;
+    const float e_ele = cq * (Tap * z);
+    const float CEclmb = cq * (dTap - Tap * r * (z * z * z)) * z;
+    const float CE = CEvd + CEclmb;
     const float dx = static_cast<float>(dvd[0]), dy = static_cast<float>(dvd[1]), dz = static_cast<float>(dvd[2]);
     gx -= static_cast<double>(CE * dx);
     gy -= static_cast<double>(CE * dy);
@@ -410,36 +401,29 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
       }
     }
     if (count) {
-      en += static_cast<double>(e_pair);
+      ev += static_cast<double>(e_vdW);
+      ee += static_cast<double>(e_ele);
       ++counted;
     }
-    ehalf += 0.5 * static_cast<double>(e_pair);   // per-atom tally: half of every pair
+    ehalf += 0.5 * (static_cast<double>(e_vdW) + static_cast<double>(e_ele));   // per-atom tally: half of every pair
   }
-  gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); en = warp_sum(en);
+  gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); ev = warp_sum(ev); ee = warp_sum(ee);
   const double w0 = warp_sum(static_cast<double>(v0)), w1 = warp_sum(static_cast<double>(v1)), w2 = warp_sum(static_cast<double>(v2));
   const double w3 = warp_sum(static_cast<double>(v3)), w4 = warp_sum(static_cast<double>(v4)), w5 = warp_sum(static_cast<double>(v5));
   if (d.pe_on) ehalf = warp_sum(ehalf);
-  if (PART == 1)
-    for (int o = 16; o > 0; o >>= 1) counted += __shfl_xor_sync(0xffffffffu, counted, o);
+  for (int o = 16; o > 0; o >>= 1) counted += __shfl_xor_sync(0xffffffffu, counted, o);
   if (lane == 0) {
-    double* vi = (PART == 1 ? d.vir_v : d.vir_nb) + static_cast<size_t>(i) * kVir;
+    d.fnb[i] = make_double4(gx, gy, gz, 0.0);
+    double* vi = d.vir_nb + static_cast<size_t>(i) * kVir;
     vi[0] = w0; vi[1] = w1; vi[2] = w2; vi[3] = w3; vi[4] = w4; vi[5] = w5;
-    if (PART == 1) {
-      d.fnb_v[i] = make_double4(gx, gy, gz, 0.0);
-      d.eatom[static_cast<size_t>(i) * kTerms + E_VDW] = en;
-      if (d.pe_on) pe_add(d, i, ehalf);
-      d.census[4 * d.na + i] = counted;
-    } else {
-      d.fnb[i] = make_double4(gx, gy, gz, 0.0);
-      d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] = en;
-      const double chi = ff.sb[ti * SB_N + SB_CHI], eta = ff.sb[ti * SB_N + SB_ETA], qd = d.q[i];
-      d.eatom[static_cast<size_t>(i) * kTerms + E_POL] = 23.02 * (chi * qd + (eta / 2.) * (qd * qd));
-      if (d.pe_on) pe_add(d, i, ehalf + 23.02 * (chi * qd + (eta / 2.) * (qd * qd)));
-    }
+    d.eatom[static_cast<size_t>(i) * kTerms + E_VDW] = ev;
+    d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] = ee;
+    const double chi = ff.sb[ti * SB_N + SB_CHI], eta = ff.sb[ti * SB_N + SB_ETA], qd = d.q[i];
+    d.eatom[static_cast<size_t>(i) * kTerms + E_POL] = 23.02 * (chi * qd + (eta / 2.) * (qd * qd));
+    if (d.pe_on) pe_add(d, i, ehalf + 23.02 * (chi * qd + (eta / 2.) * (qd * qd)));
+    d.census[4 * d.na + i] = counted;
   }
 }
-template __global__ void k_nonbonded<1>(Dev d, DevFF ff);
-template __global__ void k_nonbonded<2>(Dev d, DevFF ff);
 
 // ------------------------------------------------------------------------------------------------ ACKS2 pair terms
 // The pair side of the ACKS2 charge model (src/cpu/acks2.cpp:11-63), FP64, one warp per atom over its full row, with
@@ -1049,7 +1033,7 @@ __global__ void k_energy_sum(Dev d, double* out, double* out_vir) {
     const int c = t - kTerms;
     for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) {
       const size_t k = static_cast<size_t>(s.begin + r) * kVir + c;
-      v += (((d.vir[k] + d.vir_h[k]) + d.vir_t[k]) + d.vir_v[k]) + d.vir_nb[k];
+      v += ((d.vir[k] + d.vir_h[k]) + d.vir_t[k]) + d.vir_nb[k];
     }
   }
   sh[threadIdx.x] = v;
