@@ -143,7 +143,6 @@ struct Dev {
   unsigned char* tflag;  // per slot: 1 if it is a listed central bond of the torsions (its torsion rows are written)
   int* tor_list;         // the listed central-bond slots, in arrival order, and their count
   int* tor_n;
-  int* by_type;          // atom indices in type order (thread order of k_bonded_atom)
   double4* Tsum;         // torsion: per central slot, 2 entries: central gradient + CdDelta; e_tor, e_con, count
   double* Tvir;          // torsion: per central slot, kVir virial components
   // atoms

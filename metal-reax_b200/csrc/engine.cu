@@ -113,7 +113,6 @@ struct Context {
   std::vector<int> hsys_of;
   std::vector<long long> htag;
   std::vector<int> htype;
-  DBuf<int> by_type;
   std::vector<SysInfo> huser;   // systems as the caller gave them
   DBuf<SysInfo> sys;
   DBuf<int> sys_of, type, cell_key, cell_key_sorted, cell_atoms, atom_iota, cell_start, sys_flag;
@@ -436,14 +435,6 @@ struct Context {
     t_hist.ensure(4 * static_cast<size_t>(na));
     htag.assign(tags, tags + na);
     htype.assign(types, types + na);
-    {   // the atoms in type order (stable): the thread-per-atom bonded kernel runs them so, so that the atoms of a warp
-        // share an element and take the same branches and similar loop counts
-      std::vector<int> order(static_cast<size_t>(na));
-      for (int a = 0; a < na; ++a) order[static_cast<size_t>(a)] = a;
-      std::stable_sort(order.begin(), order.end(), [&](int u, int w) { return types[u] < types[w]; });
-      by_type.ensure(static_cast<size_t>(na));
-      RXCU(cudaMemcpy(by_type.p, order.data(), sizeof(int) * na, cudaMemcpyHostToDevice));
-    }
     {
       std::vector<double> sh(4 * static_cast<size_t>(na), 0.0), th(4 * static_cast<size_t>(na), 0.0);
       if (!old_sh.empty()) {
@@ -642,7 +633,7 @@ struct Context {
     }
     d.bcap = bcap; d.bcode = bcode.p; d.bsym = bsym.p; d.bcnt = bcnt.p; d.bdv = bdv.p; d.bBO = bBO.p; d.bdBOp = bdBOp.p;
     d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p; d.Ti = Ti.p; d.Tsum = Tsum.p; d.Tvir = Tvir.p;
-    d.tflag = tflag.p; d.tor_list = tor_list.p; d.tor_n = tor_n.p; d.by_type = by_type.p;
+    d.tflag = tflag.p; d.tor_list = tor_list.p; d.tor_n = tor_n.p;
     d.Deltap = Deltap.p; d.Deltap_boc = Deltap_boc.p; d.dDp_self = dDp_self.p; d.aq = aq.p; d.fown = fown.p; d.cdtot = cdtot.p;
     d.W = W.p; d.fdb = fdb.p; d.fnb = fnb.p; d.grad = grad.p; d.eatom = eatom.p; d.vir = vir.p; d.vir_nb = vir_nb.p; d.vir_h = vir_h.p; d.vir_t = vir_t.p;
     d.fown_h = fown_h.p; d.fown_t = fown_t.p; d.fix_h = fix_h.p; d.pe_fix = pe_fix.p; d.pe_on = pe_on; d.bcdbo_h = bcdbo_h.p; d.bfn_h = bfn_h.p; d.bacc_t = bacc_t.p; d.bfn_t = bfn_t.p; d.census = census.p; d.status = status.p;

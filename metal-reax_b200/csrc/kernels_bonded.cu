@@ -286,9 +286,8 @@ __global__ void k_atom_quantities(Dev d, DevFF ff) {
 // (its CdDelta, its gradient) go to the slot naming it, for the partner to gather.
 __global__ void k_bonded_atom(Dev d, DevFF ff, DevCtl ctl) {
   if (lists_failed(d)) return;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid >= d.na) return;
-  const int j = d.by_type[tid];   // atoms of one element per warp: same branches, similar bond counts
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.na) return;
   const int tj = d.type[j];
   const double* sj = SBp(ff, tj);
   const int nb = min(d.bcnt[j], d.bcap);
