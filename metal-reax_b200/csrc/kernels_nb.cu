@@ -537,13 +537,15 @@ __device__ inline double2 row_mv_f32(const Dev& d, int i, double eta, const doub
   const double2 vi = v[i];
   double ys = 0.0, yt = 0.0;
   const size_t base = static_cast<size_t>(i) * d.ncap;
-  for (int e0 = lane * 4; e0 < cnt; e0 += 128) {
-    const uint4 c4 = *reinterpret_cast<const uint4*>(d.nbr + base + e0);
-    const float4 h4 = *reinterpret_cast<const float4*>(d.hhi + base + e0);
-    const unsigned cc[4] = {c4.x, c4.y, c4.z, c4.w};
-    const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+  for (int e0 = lane * 8; e0 < cnt; e0 += 256) {   // eight entries per lane in flight (rows hold ncap, a multiple of 32)
+    const uint4 c4a = *reinterpret_cast<const uint4*>(d.nbr + base + e0);
+    const uint4 c4b = *reinterpret_cast<const uint4*>(d.nbr + base + e0 + 4);
+    const float4 h4a = *reinterpret_cast<const float4*>(d.hhi + base + e0);
+    const float4 h4b = *reinterpret_cast<const float4*>(d.hhi + base + e0 + 4);
+    const unsigned cc[8] = {c4a.x, c4a.y, c4a.z, c4a.w, c4b.x, c4b.y, c4b.z, c4b.w};
+    const float hh[8] = {h4a.x, h4a.y, h4a.z, h4a.w, h4b.x, h4b.y, h4b.z, h4b.w};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 8; ++k) {
       if (e0 + k < cnt) {
         const float2 vj = vf[cc[k] & d.amask];
         ys += static_cast<double>(hh[k]) * static_cast<double>(vj.x);
