@@ -34,8 +34,10 @@ enum Status : int {
   ST_CG_NOTCONV = 128,   // a system's charge solve ended above its tolerance (iteration limit)
   ST_VERLET_OVERFLOW = 256,
   ST_NONPERIODIC_ESCAPE = 512,   // an atom left the padded extent of a non-periodic direction
+  ST_ACC_OVERFLOW = 1024,
 };
-// status words: [0] bits, [1] max neighbor-row count, [2] max bond count, [3] max near-row count, [4] max Verlet-row count
+// status words: [0] bits, [1] max neighbor-row count, [2] max bond count, [3] max near-row count, [4] max Verlet-row
+// count, [5] max acceptor-row count
 constexpr int kStatusWords = 8;
 
 struct SysInfo {
@@ -113,10 +115,14 @@ struct Dev {
   int smax, S;
   const double4* shifts; // per system and shift index: L.s (xyz), summed as the reference sums lattice shifts
   // near rows: the entries of the full row within max(bond_cut, hbond_cut), in the same order
-  int ncap_near;
+  int ncap_near;         // bond-candidate rows: entries within bond_cut (k_bonds)
   unsigned* near;
   int* near_cnt;
   double rnear2;
+  int ncap_acc;          // acceptor rows of the H-bond hydrogens (p_hbond = 1): p_hbond = 2 atoms within hbond_cut
+  unsigned* acc;
+  int* acc_cnt;
+  double racc2;
   // bonds
   int bcap;
   unsigned* bcode;
@@ -207,7 +213,7 @@ __device__ inline void pair_dvec(const Dev& d, const SysInfo& s, int i, int j, i
 // A list of this evaluation overflowed (the host grows it and repeats the evaluation): later kernels skip their work.
 __device__ inline bool lists_failed(const Dev& d) {
   return (*reinterpret_cast<volatile const int*>(d.status) &
-          (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW | ST_BOND_OVERFLOW | ST_SHIFT_RANGE | ST_VERLET_OVERFLOW)) != 0;
+          (ST_NBR_OVERFLOW | ST_NEAR_OVERFLOW | ST_BOND_OVERFLOW | ST_SHIFT_RANGE | ST_VERLET_OVERFLOW | ST_ACC_OVERFLOW)) != 0;
 }
 
 // Virial of an interaction cluster, sum over its atoms of x_a f_b = -x_a g_b, taken with positions P relative to the

@@ -126,10 +126,10 @@ struct Context {
   bool have_pos = false;
 
   // lists
-  int ncap = 0, bcap = 0, ncap_near = 0, vcap = 0;
+  int ncap = 0, bcap = 0, ncap_near = 0, ncap_acc = 0, vcap = 0;
   double skin = 1.0;   // Verlet skin [A]: rows hold every image within nonb_cut + skin, rebuilt per system on demand
-  DBuf<unsigned> nbr, bcode, near, vrow;
-  DBuf<int> nbr_cnt, bsym, bcnt, near_cnt, vcnt;
+  DBuf<unsigned> nbr, bcode, near, acc, vrow;
+  DBuf<int> nbr_cnt, bsym, bcnt, near_cnt, acc_cnt, vcnt;
   DBuf<double4> shifts, xref;
   DBuf<float> hhi, hlo;
   DBuf<double4> bdv, bBO, bdBOp, bdlnpi, bdlnpi2, bC0, bC1, bC2, bacc, bfn, Tl, Ti, Tsum, bfn_h, bacc_t, bfn_t;
@@ -568,9 +568,12 @@ struct Context {
     const double expect_v = 4.0 / 3.0 * M_PI * rc * rc * rc * max_density;
     const int want_vcap = static_cast<int>(std::ceil((expect_v * 1.3 + 32) / 32.0)) * 32;
     if (vcap < want_vcap) vcap = want_vcap;
-    const double rn = std::max(ctl.bond_cut, ctl.hbond_cut);
+    const double rn = ctl.bond_cut, ra = ctl.hbond_cut;
     const int want_near = static_cast<int>(std::ceil((4.0 / 3.0 * M_PI * rn * rn * rn * max_density * 1.3 + 32) / 32.0)) * 32;
     if (ncap_near < want_near) ncap_near = want_near;
+    // acceptors are a fraction of the atoms; the estimate takes half of them and grows on overflow
+    const int want_acc = static_cast<int>(std::ceil((4.0 / 3.0 * M_PI * ra * ra * ra * max_density * 0.5 + 32) / 32.0)) * 32;
+    if (ncap_acc < want_acc) ncap_acc = want_acc;
     if (bcap < 16) bcap = 16;
     alloc_atoms();
     alloc_lists();
@@ -582,7 +585,7 @@ struct Context {
     Deltap.ensure(n); Deltap_boc.ensure(n); cdtot.ensure(n); W.ensure(n); eatom.ensure(n * kTerms);
     dDp_self.ensure(n); fown.ensure(n); fdb.ensure(n); fnb.ensure(n); grad.ensure(n);
     aq.ensure(n); census.ensure(n * kCensus);
-    nbr_cnt.ensure(n); bcnt.ensure(n); near_cnt.ensure(n); vcnt.ensure(n); xref.ensure(n);
+    nbr_cnt.ensure(n); bcnt.ensure(n); near_cnt.ensure(n); acc_cnt.ensure(n); vcnt.ensure(n); xref.ensure(n);
     sys_flag.ensure(static_cast<size_t>(nsys)); cg_nref.ensure(1); cg_brk.ensure(static_cast<size_t>(nsys));
     energies.ensure(static_cast<size_t>(nsys) * kTerms);
     virial.ensure(static_cast<size_t>(nsys) * kVir);
@@ -603,6 +606,7 @@ struct Context {
     hhi.ensure(n * ncap);
     hlo.ensure(n * ncap);
     near.ensure(n * ncap_near);
+    acc.ensure(n * ncap_acc);
     const size_t nb = n * bcap;
     bcode.ensure(nb); bsym.ensure(nb);
     bdv.ensure(nb); bBO.ensure(nb); bdBOp.ensure(nb); bdlnpi.ensure(nb); bdlnpi2.ensure(nb);
@@ -627,9 +631,11 @@ struct Context {
     d.half_skin2 = 0.25 * skin * skin;
     d.abits = abits; d.amask = (abits >= 32) ? 0xffffffffu : ((1u << abits) - 1u); d.smax = smax; d.S = S;
     d.shifts = shifts.p; d.ncap_near = ncap_near; d.near = near.p; d.near_cnt = near_cnt.p;
-    {  // a superset of every consumer's sqrt(r2) <= cut test
-      const double rn = std::max(ctl.bond_cut, ctl.hbond_cut) * (1.0 + 1e-9);
+    d.ncap_acc = ncap_acc; d.acc = acc.p; d.acc_cnt = acc_cnt.p;
+    {  // supersets of the consumers' sqrt(r2) <= cut tests
+      const double rn = ctl.bond_cut * (1.0 + 1e-9), ra = ctl.hbond_cut * (1.0 + 1e-9);
       d.rnear2 = rn * rn;
+      d.racc2 = ra * ra;
     }
     d.bcap = bcap; d.bcode = bcode.p; d.bsym = bsym.p; d.bcnt = bcnt.p; d.bdv = bdv.p; d.bBO = bBO.p; d.bdBOp = bdBOp.p;
     d.bdlnpi = bdlnpi.p; d.bdlnpi2 = bdlnpi2.p; d.bC0 = bC0.p; d.bC1 = bC1.p; d.bC2 = bC2.p; d.bacc = bacc.p; d.bfn = bfn.p; d.Tl = Tl.p; d.Ti = Ti.p; d.Tsum = Tsum.p; d.Tvir = Tvir.p;
@@ -834,10 +840,11 @@ struct Context {
 
   // grow the capacities from a status word with overflow bits; false if nothing overflowed
   bool grow_from_status(const int* st, int attempt) {
-    if (!(st[0] & (ST_NBR_OVERFLOW | ST_BOND_OVERFLOW | ST_NEAR_OVERFLOW | ST_VERLET_OVERFLOW))) return false;
+    if (!(st[0] & (ST_NBR_OVERFLOW | ST_BOND_OVERFLOW | ST_NEAR_OVERFLOW | ST_VERLET_OVERFLOW | ST_ACC_OVERFLOW))) return false;
     if (attempt >= 4) throw Error(RX_ERR_CAPACITY, "list capacity still exceeded after 4 grow attempts");
     if (st[0] & ST_NBR_OVERFLOW) ncap = ((st[1] * 5 / 4) + 31) / 32 * 32;
     if (st[0] & ST_NEAR_OVERFLOW) ncap_near = ((st[3] * 5 / 4) + 31) / 32 * 32;
+    if (st[0] & ST_ACC_OVERFLOW) ncap_acc = ((st[5] * 5 / 4) + 31) / 32 * 32;
     if (st[0] & ST_VERLET_OVERFLOW) vcap = ((st[4] * 5 / 4) + 31) / 32 * 32;
     if (st[0] & ST_BOND_OVERFLOW) bcap = std::max(bcap, ((st[2] * 5 / 4) + 3) / 4 * 4);
     alloc_lists();

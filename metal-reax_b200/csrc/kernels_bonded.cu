@@ -621,8 +621,8 @@ __device__ inline bool hbond_triple(const DevFF& ff, const HbDonor& dn, int tj, 
   return true;
 }
 
-// One warp per hydrogen j (p_hbond = 1): for every donor bond of j, the lanes walk j's near row for acceptors
-// (p_hbond = 2, r <= hbond_cut); each triple is evaluated once. Energy, the gradient of j and the coefficient /
+// One warp per hydrogen j (p_hbond = 1): for every donor bond of j, the lanes walk j's acceptor row (p_hbond = 2 atoms,
+// r <= hbond_cut taken again exactly here); each triple is evaluated once. Energy, the gradient of j and the coefficient /
 // gradient of the donor bond are reduced over the warp in fixed order (the donor's share goes to j's slot for the
 // donor to gather); the acceptor's gradient is added to its fixed-point accumulator (zeroed by k_pairs).
 __global__ void __launch_bounds__(256) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
@@ -650,7 +650,7 @@ __global__ void __launch_bounds__(256) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
     return;
   }
   const SysInfo s = d.sys[d.sys_of[j]];
-  const int cnt = min(d.near_cnt[j], d.ncap_near);
+  const int cnt = min(d.acc_cnt[j], d.ncap_acc);
   const int nb = min(d.bcnt[j], d.bcap);
   const double hc2 = ctl.hbond_cut * ctl.hbond_cut;
   const size_t base = static_cast<size_t>(j) * d.bcap;
@@ -677,10 +677,9 @@ __global__ void __launch_bounds__(256) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
     for (int e0 = 0; e0 < cnt; e0 += 32) {
       const int ee = e0 + lane;
       if (ee >= cnt) continue;
-      const unsigned code = d.near[static_cast<size_t>(j) * d.ncap_near + ee];
+      const unsigned code = d.acc[static_cast<size_t>(j) * d.ncap_acc + ee];   // p_hbond = 2 atoms only
       const int ka = static_cast<int>(code & d.amask);
       const int type_k = d.type[ka];
-      if (static_cast<int>(SBp(ff, type_k)[SB_P_HBOND]) != 2) continue;
       double dvjk[3];
       pair_dvec(d, s, j, ka, static_cast<int>(code >> d.abits), dvjk);
       const double r2 = dot3(dvjk, dvjk);

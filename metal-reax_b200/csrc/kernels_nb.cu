@@ -210,8 +210,10 @@ __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d) {
 // The rows of this evaluation, one warp per atom: the entries of the Verlet row within nonb_cut, in Verlet-row order,
 // with the exact FP64 distance test of build_far_list (every cut-off decision is the reference's). Fused: the
 // charge-matrix entry H = 14.4 Tap(r) / cbrt(r^3 + (gamma_i gamma_j)^-1.5) for r <= swb (ENGINE_SPEC 7; fix_qeq_reaxff
-// compute_H) stored as hi + lo single-precision parts, and the near row (entries within max(bond_cut, hbond_cut)) the
-// bond and H-bond kernels scan. Also clears the per-system rebuild flags for the next evaluation.
+// compute_H) stored as hi + lo single-precision parts; the near row (entries within bond_cut) k_bonds scans; and, for a
+// hydrogen of the H-bonds (p_hbond = 1), its acceptor row (p_hbond = 2 atoms within hbond_cut) k_hbond scans. Both
+// short rows are supersets (cut-offs widened by 1e-9) of what their consumers accept with their own exact tests. Also
+// clears the per-system rebuild flags for the next evaluation.
 __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (gid < d.nsys) d.sys_flag[gid] = 0;
@@ -227,7 +229,8 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   const double4 xi = d.x[i];
   const int ti = d.type[i];
   const double* shld_i = ff.shld + static_cast<size_t>(ti) * ff.nt;
-  int count = 0, count_near = 0;
+  int count = 0, count_near = 0, count_acc = 0;
+  const bool hb_i = static_cast<int>(ff.sb[ti * SB_N + SB_P_HBOND]) == 1;
   const unsigned lt = (1u << lane) - 1u;
   const size_t vbase = static_cast<size_t>(i) * d.vcap, rowbase = static_cast<size_t>(i) * d.ncap;
   const int nv = min(d.vcnt[i], d.vcap);
@@ -253,6 +256,15 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
       if (posn < d.ncap_near) d.near[static_cast<size_t>(i) * d.ncap_near + posn] = code;
     }
     count_near += __popc(mn);
+    if (hb_i) {   // warp-uniform
+      const bool ac = ok && r2 <= d.racc2 && static_cast<int>(ff.sb[d.type[j] * SB_N + SB_P_HBOND]) == 2;
+      const unsigned ma = __ballot_sync(0xffffffffu, ac);
+      if (ac) {
+        const int posa = count_acc + __popc(ma & lt);
+        if (posa < d.ncap_acc) d.acc[static_cast<size_t>(i) * d.ncap_acc + posa] = code;
+      }
+      count_acc += __popc(ma);
+    }
     if (ok) {
       const int pos = count + __popc(m & lt);
       if (pos < d.ncap) {
@@ -279,6 +291,11 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   if (lane == 0) {
     d.nbr_cnt[i] = count;
     d.near_cnt[i] = count_near;
+    d.acc_cnt[i] = count_acc;
+    if (count_acc > d.ncap_acc) {
+      atomicOr(d.status, ST_ACC_OVERFLOW);
+      atomicMax(d.status + 5, count_acc);
+    }
     if (count > d.ncap) {
       atomicOr(d.status, ST_NBR_OVERFLOW);
       atomicMax(d.status + 1, count);
