@@ -353,6 +353,7 @@ struct Context {
       throw Error(RX_ERR_INVALID, "cut-offs must be finite, bond_cut > 0, hbond_cut >= 0");
     ctl = DevCtl{bond_cut, hbond_cut, thb_cut, thb_cutsq, enobonds};
     drop_graph();
+    if (have_ff && nsys > 0) layout_systems();   // the short Verlet rows hold the cut-offs: rebuild them
   }
 
   void set_neighbor(double sk) {
@@ -568,7 +569,7 @@ struct Context {
     const double expect_v = 4.0 / 3.0 * M_PI * rc * rc * rc * max_density;
     const int want_vcap = static_cast<int>(std::ceil((expect_v * 1.3 + 32) / 32.0)) * 32;
     if (vcap < want_vcap) vcap = want_vcap;
-    const double rn = ctl.bond_cut, ra = ctl.hbond_cut;
+    const double rn = ctl.bond_cut + skin, ra = ctl.hbond_cut + skin;
     const int want_near = static_cast<int>(std::ceil((4.0 / 3.0 * M_PI * rn * rn * rn * max_density * 1.3 + 32) / 32.0)) * 32;
     if (ncap_near < want_near) ncap_near = want_near;
     // acceptors are a fraction of the atoms; the estimate takes half of them and grows on overflow
@@ -632,8 +633,9 @@ struct Context {
     d.abits = abits; d.amask = (abits >= 32) ? 0xffffffffu : ((1u << abits) - 1u); d.smax = smax; d.S = S;
     d.shifts = shifts.p; d.ncap_near = ncap_near; d.near = near.p; d.near_cnt = near_cnt.p;
     d.ncap_acc = ncap_acc; d.acc = acc.p; d.acc_cnt = acc_cnt.p;
-    {  // supersets of the consumers' sqrt(r2) <= cut tests
-      const double rn = ctl.bond_cut * (1.0 + 1e-9), ra = ctl.hbond_cut * (1.0 + 1e-9);
+    {  // the short Verlet rows (rebuilt with the Verlet rows): supersets of the consumers' exact sqrt(r2) <= cut tests for
+       // every position until the next rebuild (each atom moves less than skin/2 meanwhile)
+      const double rn = (ctl.bond_cut + skin) * (1.0 + 1e-9), ra = (ctl.hbond_cut + skin) * (1.0 + 1e-9);
       d.rnear2 = rn * rn;
       d.racc2 = ra * ra;
     }
@@ -689,7 +691,7 @@ struct Context {
     size_t tmp = cub_tmp.n;
     RXCU(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, key_bits, stream));
     k_cell_start<<<blocks(na + 1, 256), 256, 0, stream>>>(d, cell_key_sorted.p);
-    k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d);
+    k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff);
     k_pairs<<<blocks(static_cast<long long>(na) * 32, tune.tpb_pairs), tune.tpb_pairs, 0, stream>>>(d, dff, qp);
     toc(0);
   }

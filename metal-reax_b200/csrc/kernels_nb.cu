@@ -118,7 +118,7 @@ __device__ inline void taper_horner(const double* c, double r, double& Tap, doub
 // are visited as runs of consecutive cells along x (one contiguous range of the cell-ordered atoms per run and periodic
 // image), so the candidate loads are coalesced. Entries are written through a warp ballot in visiting order
 // (deterministic).
-__global__ void __launch_bounds__(128, 6) k_neighbors(Dev d) {
+__global__ void __launch_bounds__(128, 6) k_neighbors(Dev d, DevFF ff) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
@@ -129,10 +129,11 @@ __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d) {
   const int key = d.cell_key[i] - s.cell_begin;
   const int cx = key % s.nc[0], cy = (key / s.nc[0]) % s.nc[1], cz = key / (s.nc[0] * s.nc[1]);
   const double4 xi = d.x[i];
-  int count = 0;
+  int count = 0, count_near = 0, count_acc = 0;
   const unsigned lt = (1u << lane) - 1u;
   const int center = (d.S * d.S * d.S - 1) / 2;
   const size_t rowbase = static_cast<size_t>(i) * d.vcap;
+  const bool hb_i = static_cast<int>(ff.sb[d.type[i] * SB_N + SB_P_HBOND]) == 1;
   // fractional coordinates of i: lower bounds of the distance to a cell slab prune whole runs and clip the x range
   double fi[3];
   for (int k = 0; k < 3; ++k)
@@ -179,21 +180,41 @@ __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d) {
           const int p = base + lane;
           bool ok = false;
           int j = 0;
+          double r2 = 0.0;
           if (p < c1) {
             j = d.cell_atoms[p];
             const double4 xj = d.xs[p];
             if (!(j == i && sidx == center)) {
               double dv[3];
               pair_dvec_x(d, s, i, j, sidx, xi, xj, dv);
-              ok = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2] <= d.rv2;
+              r2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+              ok = r2 <= d.rv2;
             }
           }
+          const unsigned code = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
           const unsigned m = __ballot_sync(0xffffffffu, ok);
           if (ok) {
             const int pos = count + __popc(m & lt);
-            if (pos < d.vcap) d.vrow[rowbase + pos] = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
+            if (pos < d.vcap) d.vrow[rowbase + pos] = code;
           }
           count += __popc(m);
+          // the short Verlet rows of the bond and H-bond kernels (their own exact tests run on every evaluation)
+          const bool nr = ok && r2 <= d.rnear2;
+          const unsigned mn = __ballot_sync(0xffffffffu, nr);
+          if (nr) {
+            const int posn = count_near + __popc(mn & lt);
+            if (posn < d.ncap_near) d.near[static_cast<size_t>(i) * d.ncap_near + posn] = code;
+          }
+          count_near += __popc(mn);
+          if (hb_i) {   // warp-uniform
+            const bool ac = ok && r2 <= d.racc2 && static_cast<int>(ff.sb[d.type[j] * SB_N + SB_P_HBOND]) == 2;
+            const unsigned ma = __ballot_sync(0xffffffffu, ac);
+            if (ac) {
+              const int posa = count_acc + __popc(ma & lt);
+              if (posa < d.ncap_acc) d.acc[static_cast<size_t>(i) * d.ncap_acc + posa] = code;
+            }
+            count_acc += __popc(ma);
+          }
         }
       }
     }
@@ -204,16 +225,23 @@ __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d) {
       atomicOr(d.status, ST_VERLET_OVERFLOW);
       atomicMax(d.status + 4, count);
     }
+    d.near_cnt[i] = count_near;
+    if (count_near > d.ncap_near) {
+      atomicOr(d.status, ST_NEAR_OVERFLOW);
+      atomicMax(d.status + 3, count_near);
+    }
+    d.acc_cnt[i] = count_acc;
+    if (count_acc > d.ncap_acc) {
+      atomicOr(d.status, ST_ACC_OVERFLOW);
+      atomicMax(d.status + 5, count_acc);
+    }
   }
 }
 
 // The rows of this evaluation, one warp per atom: the entries of the Verlet row within nonb_cut, in Verlet-row order,
 // with the exact FP64 distance test of build_far_list (every cut-off decision is the reference's). Fused: the
 // charge-matrix entry H = 14.4 Tap(r) / cbrt(r^3 + (gamma_i gamma_j)^-1.5) for r <= swb (ENGINE_SPEC 7; fix_qeq_reaxff
-// compute_H) stored as hi + lo single-precision parts; the near row (entries within bond_cut) k_bonds scans; and, for a
-// hydrogen of the H-bonds (p_hbond = 1), its acceptor row (p_hbond = 2 atoms within hbond_cut) k_hbond scans. Both
-// short rows are supersets (cut-offs widened by 1e-9) of what their consumers accept with their own exact tests. Also
-// clears the per-system rebuild flags for the next evaluation.
+// compute_H) stored as hi + lo single-precision parts. Also clears the per-system rebuild flags for the next evaluation.
 __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (gid < d.nsys) d.sys_flag[gid] = 0;
@@ -229,8 +257,7 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   const double4 xi = d.x[i];
   const int ti = d.type[i];
   const double* shld_i = ff.shld + static_cast<size_t>(ti) * ff.nt;
-  int count = 0, count_near = 0, count_acc = 0;
-  const bool hb_i = static_cast<int>(ff.sb[ti * SB_N + SB_P_HBOND]) == 1;
+  int count = 0;
   const unsigned lt = (1u << lane) - 1u;
   const size_t vbase = static_cast<size_t>(i) * d.vcap, rowbase = static_cast<size_t>(i) * d.ncap;
   const int nv = min(d.vcnt[i], d.vcap);
@@ -249,22 +276,6 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
       ok = r2 <= rc2;
     }
     const unsigned m = __ballot_sync(0xffffffffu, ok);
-    const bool nr = ok && r2 <= d.rnear2;
-    const unsigned mn = __ballot_sync(0xffffffffu, nr);
-    if (nr) {
-      const int posn = count_near + __popc(mn & lt);
-      if (posn < d.ncap_near) d.near[static_cast<size_t>(i) * d.ncap_near + posn] = code;
-    }
-    count_near += __popc(mn);
-    if (hb_i) {   // warp-uniform
-      const bool ac = ok && r2 <= d.racc2 && static_cast<int>(ff.sb[d.type[j] * SB_N + SB_P_HBOND]) == 2;
-      const unsigned ma = __ballot_sync(0xffffffffu, ac);
-      if (ac) {
-        const int posa = count_acc + __popc(ma & lt);
-        if (posa < d.ncap_acc) d.acc[static_cast<size_t>(i) * d.ncap_acc + posa] = code;
-      }
-      count_acc += __popc(ma);
-    }
     if (ok) {
       const int pos = count + __popc(m & lt);
       if (pos < d.ncap) {
@@ -290,19 +301,9 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   }
   if (lane == 0) {
     d.nbr_cnt[i] = count;
-    d.near_cnt[i] = count_near;
-    d.acc_cnt[i] = count_acc;
-    if (count_acc > d.ncap_acc) {
-      atomicOr(d.status, ST_ACC_OVERFLOW);
-      atomicMax(d.status + 5, count_acc);
-    }
     if (count > d.ncap) {
       atomicOr(d.status, ST_NBR_OVERFLOW);
       atomicMax(d.status + 1, count);
-    }
-    if (count_near > d.ncap_near) {
-      atomicOr(d.status, ST_NEAR_OVERFLOW);
-      atomicMax(d.status + 3, count_near);
     }
   }
 }
