@@ -192,19 +192,16 @@ __device__ inline void decode_shift(int sidx, int S, int smax, int& sx, int& sy,
 // table built on the host (the same double-precision sum the reference uses, src/core/system.cpp:52-57).
 __device__ inline void pair_dvec_x(const Dev& d, const SysInfo& s, int i, int j, int sidx, const double4& xi, const double4& xj,
                                    double* dv) {
+  // forward: (x_j + L s) - x_i; backward: -((x_i + L(-s)) - x_j). Written with selects instead of a branch, so that the
+  // lanes of a warp that take different directions do not serialise; the negation is exact, the bits are the same.
   const int S3 = d.S * d.S * d.S;
   const bool fwd = (j > i) || (j == i && 2 * sidx > S3 - 1);
-  if (fwd) {
-    const double4 sh = d.shifts[s.shift_base + sidx];
-    dv[0] = (xj.x + sh.x) - xi.x;
-    dv[1] = (xj.y + sh.y) - xi.y;
-    dv[2] = (xj.z + sh.z) - xi.z;
-  } else {
-    const double4 sh = d.shifts[s.shift_base + (S3 - 1 - sidx)];
-    dv[0] = -((xi.x + sh.x) - xj.x);
-    dv[1] = -((xi.y + sh.y) - xj.y);
-    dv[2] = -((xi.z + sh.z) - xj.z);
-  }
+  const double4 sh = d.shifts[s.shift_base + (fwd ? sidx : S3 - 1 - sidx)];
+  const double4 xa = fwd ? xj : xi, xb = fwd ? xi : xj;
+  const double sg = fwd ? 1.0 : -1.0;
+  dv[0] = sg * ((xa.x + sh.x) - xb.x);
+  dv[1] = sg * ((xa.y + sh.y) - xb.y);
+  dv[2] = sg * ((xa.z + sh.z) - xb.z);
 }
 __device__ inline void pair_dvec(const Dev& d, const SysInfo& s, int i, int j, int sidx, double* dv) {
   pair_dvec_x(d, s, i, j, sidx, d.x[i], d.x[j], dv);
