@@ -19,6 +19,7 @@
 #ifndef RXCUDA_H
 #define RXCUDA_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -90,8 +91,14 @@ int rx_get_capacities(const rx_context* ctx, int* out3);
  * same either way, taken on the current positions). 0 rebuilds every evaluation. */
 int rx_set_neighbor(rx_context* ctx, double skin);
 /* x[3*NA], in any periodic image (each atom is moved to the image the engine's lists use; the lists are rebuilt only
- * for systems whose atoms moved more than skin/2 since their last rebuild) */
+ * for systems whose atoms moved more than skin/2 since their last rebuild). An array in page-locked memory (from
+ * rx_host_alloc) is copied from directly; a pageable one through the context's staging buffer. */
 int rx_set_positions(rx_context* ctx, const double* x);
+/* Page-locked host memory for the arrays exchanged every step (positions in, gradient out): rx_set_positions and
+ * rx_compute copy from and into such arrays directly, without a host-side staging copy. NULL on failure. No
+ * counterpart in the reference (its adapter copies through LAMMPS's arrays). */
+void* rx_host_alloc(size_t bytes);
+void rx_host_free(void* p);
 /* positions as held: wrapped into the primary cell at the last list rebuild of their system, unwrapped since */
 int rx_get_positions(rx_context* ctx, double* x);
 int rx_set_charges(rx_context* ctx, const double* q);     /* q[NA] */

@@ -1060,12 +1060,31 @@ struct Context {
     if (any) layout_systems();
   }
 
+  // a caller array in page-locked memory is copied from and into directly (the layout change runs on the device);
+  // pageable arrays go through the context's own pinned staging buffer
+  static bool is_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+  }
+  DBuf<double> xyz3;   // device scratch in the caller's 3-per-atom layout
+
   void set_positions(const double* xin) {
     require_sys();
     fit_nonperiodic(xin);
-    double4* h = stage(static_cast<size_t>(na));
-    for (int a = 0; a < na; ++a) h[a] = make_double4(xin[3 * a], xin[3 * a + 1], xin[3 * a + 2], 0.0);
-    RXCU(cudaMemcpyAsync(x.p, h, sizeof(double4) * na, cudaMemcpyHostToDevice, stream));
+    if (is_pinned(xin)) {
+      xyz3.ensure(3 * static_cast<size_t>(na));
+      RXCU(cudaMemcpyAsync(xyz3.p, xin, sizeof(double) * 3 * na, cudaMemcpyHostToDevice, stream));
+      ++launches;
+      k_unpack3<<<blocks(na, 256), 256, 0, stream>>>(na, xyz3.p, x.p);
+    } else {
+      double4* h = stage(static_cast<size_t>(na));
+      for (int a = 0; a < na; ++a) h[a] = make_double4(xin[3 * a], xin[3 * a + 1], xin[3 * a + 2], 0.0);
+      RXCU(cudaMemcpyAsync(x.p, h, sizeof(double4) * na, cudaMemcpyHostToDevice, stream));
+    }
     // no forced rebuild: the next evaluation's Verlet check moves every atom to the periodic image of the engine's
     // rows and rebuilds the systems whose atoms moved more than skin/2 (or whose layout fit_nonperiodic changed)
     RXCU(cudaStreamSynchronize(stream));
@@ -1090,7 +1109,9 @@ struct Context {
       pe_on = want_pe;
       drop_graph();
     }
-    double4* g = g_out ? stage(static_cast<size_t>(na)) : nullptr;
+    const bool g_pinned = g_out && is_pinned(g_out);
+    double4* g = g_out && !g_pinned ? stage(static_cast<size_t>(na)) : nullptr;
+    if (g_pinned) xyz3.ensure(3 * static_cast<size_t>(na));
     double* eh = nullptr;
     evaluate_with((flags & RX_COMPUTE_QEQ) != 0, [&] {
       energy_sums();
@@ -1099,6 +1120,11 @@ struct Context {
         RXCU(cudaMemcpyAsync(eh, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
       }
       if (g) RXCU(cudaMemcpyAsync(g, grad.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, stream));
+      if (g_pinned) {
+        ++launches;
+        k_pack3<<<blocks(na, 256), 256, 0, stream>>>(na, grad.p, xyz3.p);
+        RXCU(cudaMemcpyAsync(g_out, xyz3.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, stream));
+      }
     });
     have_peratom = pe_on != 0;
     if (e_out) std::copy(eh, eh + static_cast<size_t>(kTerms) * nsys, e_out);
@@ -1111,7 +1137,7 @@ struct Context {
       RXCU(cudaMemcpyAsync(bc.data(), bcnt.p, sizeof(int) * na, cudaMemcpyDeviceToHost, stream));
     }
     if (cen_out || counts) RXCU(cudaStreamSynchronize(stream));
-    if (g_out)
+    if (g)
       for (int a = 0; a < na; ++a) { g_out[3 * a] = g[a].x; g_out[3 * a + 1] = g[a].y; g_out[3 * a + 2] = g[a].z; }
     if (counts) {
       long long sb = 0, sn = 0;
@@ -1711,6 +1737,19 @@ rx_context* rx_create(int device) {
 }
 
 void rx_destroy(rx_context* ctx) { delete ctx; }
+
+void* rx_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0 || cudaMallocHost(&p, bytes) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void rx_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
 
 const char* rx_last_error(const rx_context* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
 

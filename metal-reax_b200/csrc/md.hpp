@@ -41,5 +41,7 @@ __global__ void k_md_kick(MdDev m, const int* type, const int* sys_of, const dou
 __global__ void k_gather_state(int n, const int* src, const double4* ox, const double* oq, const double* osh,
                                const double* oth, double4* x, double* q, double* sh, double* th);
 __global__ void k_gather_vel(int n, const int* src, const double4* ov, double4* v);
+__global__ void k_unpack3(int n, const double* in3, double4* out);
+__global__ void k_pack3(int n, const double4* in, double* out3);
 
 }  // namespace rx

@@ -149,4 +149,19 @@ __global__ void k_gather_vel(int n, const int* src, const double4* ov, double4* 
   v[a] = ov[src[a]];
 }
 
+// host layout (3 doubles per atom) <-> device layout (double4), for copies straight from and into pinned caller memory
+__global__ void k_unpack3(int n, const double* in3, double4* out) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  out[a] = make_double4(in3[3 * static_cast<size_t>(a)], in3[3 * static_cast<size_t>(a) + 1], in3[3 * static_cast<size_t>(a) + 2], 0.0);
+}
+__global__ void k_pack3(int n, const double4* in, double* out3) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const double4 v = in[a];
+  out3[3 * static_cast<size_t>(a)] = v.x;
+  out3[3 * static_cast<size_t>(a) + 1] = v.y;
+  out3[3 * static_cast<size_t>(a) + 2] = v.z;
+}
+
 }  // namespace rx

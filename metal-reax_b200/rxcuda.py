@@ -34,7 +34,7 @@ EXPORTS = ["rx_create", "rx_destroy", "rx_last_error", "rx_set_forcefield", "rx_
            "rx_get_charges", "rx_set_qeq", "rx_qeq_solve", "rx_qeq_matvec", "rx_compute", "rx_md_setup", "rx_set_velocities",
            "rx_get_velocities", "rx_md_run", "rx_kernel_launches", "rx_stream", "rx_set_timing", "rx_phase_times",
            "rx_qeq_solve_static", "rx_set_capacities", "rx_get_capacities", "rx_qeq_last", "rx_get_virial", "rx_set_neighbor", "rx_qeq_cg", "rx_set_acks2", "rx_qeq_reset", "rx_update_systems", "rx_md_targets", "rx_get_gradient", "rx_md_charges", "rx_autotune", "rx_set_tuning", "rx_qeq_refinements", "rx_pvector", "rx_get_peratom",
-           "rx_get_bonds", "rx_forcefield_element"]
+           "rx_get_bonds", "rx_forcefield_element", "rx_host_alloc", "rx_host_free"]
 
 _V = ctypes.c_void_p
 _D = ctypes.c_double
@@ -77,6 +77,7 @@ def load():
         "rx_set_tuning": (_I, [_V, _I, _I]), "rx_qeq_refinements": (_I, [_V]), "rx_pvector": (_I, [_V, _V, _V, _V]), "rx_get_peratom": (_I, [_V, _V, _V]), "rx_forcefield_element": (_I, [_V, ctypes.c_char_p]),
         "rx_get_bonds": (ctypes.c_longlong, [_V, _V, _V, _V, _V, _V, _V, ctypes.c_longlong]),
         "rx_update_systems": (_I, [_V, _I, _V, _I, _V, _V, _V, _V, _V, _V, _V, _V]),
+        "rx_host_alloc": (_V, [ctypes.c_size_t]), "rx_host_free": (None, [_V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -88,6 +89,31 @@ def load():
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+class _PinnedBlock:
+    """Owns one page-locked allocation (rx_host_alloc); freed with the last array that views it."""
+
+    def __init__(self, nbytes):
+        self.lib = load()
+        self.ptr = self.lib.rx_host_alloc(nbytes)
+        if not self.ptr:
+            raise MemoryError("rx_host_alloc(%d) failed" % nbytes)
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            self.lib.rx_host_free(self.ptr)
+            self.ptr = None
+
+
+def pinned_array(shape, dtype=np.float64):
+    """A numpy array in page-locked host memory: rx_set_positions and rx_compute copy from and into it directly."""
+    dt = np.dtype(dtype)
+    n = int(np.prod(shape))
+    block = _PinnedBlock(max(1, n * dt.itemsize))
+    buf = (ctypes.c_char * max(1, n * dt.itemsize)).from_address(block.ptr)
+    buf.owner = block   # the array keeps the ctypes buffer alive (its base), the buffer the allocation
+    return np.frombuffer(buf, dtype=dt, count=n).reshape(shape)
 
 
 def pvector(e13):
@@ -239,9 +265,15 @@ class Engine:
         return q
 
     # ---- evaluation
-    def compute(self, qeq=False, census=False, counts=False, cold=False, peratom=False):
+    def compute(self, qeq=False, census=False, counts=False, cold=False, peratom=False, grad_out=None):
+        """grad_out: an (n, 3) float64 array to receive the gradient (page-locked, from pinned_array, for a direct copy)."""
         e = np.empty(13 * self.nsys)   # every entry is written by rx_compute
-        g = np.empty(3 * self.na)
+        if grad_out is not None:
+            if grad_out.dtype != np.float64 or grad_out.size != 3 * self.na or not grad_out.flags.c_contiguous:
+                raise ValueError("grad_out must be a contiguous float64 array of 3 entries per atom")
+            g = grad_out.reshape(-1)
+        else:
+            g = np.empty(3 * self.na)
         cen = np.zeros(7 * self.na, dtype=np.int32) if census else None
         cnt = np.zeros(4, dtype=np.int64) if counts else None
         flags = (RX_COMPUTE_QEQ if qeq else 0) | (RX_COMPUTE_CENSUS if census else 0) | (RX_COMPUTE_QEQ_COLD if cold else 0) | \

@@ -475,3 +475,25 @@ def test_peratom_energies_and_bond_table_match_reference(engine):
             theirs = sorted(zip(ref["partner"][ref["start"][a]:ref["start"][a + 1]], ref["bo"][ref["start"][a]:ref["start"][a + 1]]))
             assert [p for p, _ in mine] == [p for p, _ in theirs], (s["name"], a)
             assert np.allclose([v for _, v in mine], [v for _, v in theirs], rtol=0, atol=1e-9), (s["name"], a)
+
+
+def test_pinned_arrays_give_the_same_bits(engine):
+    """rx_set_positions from page-locked memory and the gradient copied straight into page-locked memory (the device
+    does the layout change) give bitwise the results of the pageable path."""
+    import rxcuda
+    s = small_systems()[0]
+    q = fixed_charges(s)
+    engine.set_systems([s])
+    engine.set_charges(q)
+    engine.set_positions(s["x"])
+    ref = engine.compute()
+    n = len(s["type"])
+    x = rxcuda.pinned_array((n, 3))
+    x[:] = s["x"]
+    g = rxcuda.pinned_array((n, 3))
+    engine.set_systems([s])
+    engine.set_charges(q)
+    engine.set_positions(x)
+    out = engine.compute(grad_out=g)
+    assert np.array_equal(out["e"], ref["e"])
+    assert np.array_equal(g, ref["grad"])
