@@ -79,6 +79,7 @@ struct Context {
   // concurrent branches of an evaluation: the bonded chain (side), H-bonds (side_h) and torsions (side_t) next to
   // the charge solve and the non-bonded pairs on `stream`
   cudaStream_t side = nullptr, side_h = nullptr, side_t = nullptr;
+  cudaStream_t side_c = nullptr;   // capture of the rebuild kernels into their graph conditional
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join_h = nullptr, ev_join_t = nullptr;
   // one captured MD step (replayed for every step of rx_md_run); dropped whenever a buffer or a parameter it holds
   // changes
@@ -221,7 +222,7 @@ struct Context {
     RXCU(cudaSetDevice(dev));
     RXCU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     RXCU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    for (cudaStream_t* st : {&side, &side_h, &side_t}) RXCU(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
+    for (cudaStream_t* st : {&side, &side_h, &side_t, &side_c}) RXCU(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
     for (cudaEvent_t* ev : {&ev_fork, &ev_join, &ev_fork2, &ev_join_h, &ev_join_t}) RXCU(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
     status.ensure(kStatusWords);
     counters.ensure(8);
@@ -236,7 +237,7 @@ struct Context {
     for (auto& p : phases) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (cudaEvent_t ev : {ev_fork, ev_join, ev_fork2, ev_join_h, ev_join_t})
       if (ev) cudaEventDestroy(ev);
-    for (cudaStream_t st : {side, side_h, side_t})
+    for (cudaStream_t st : {side, side_h, side_t, side_c})
       if (st) cudaStreamDestroy(st);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -683,15 +684,51 @@ struct Context {
 
   // Verlet maintenance + this evaluation's rows (neighbor rows, charge matrix, near rows). The wrap/bin, sort and
   // cell-start kernels run every evaluation but do work only for systems whose flag is set; k_neighbors likewise.
+  // While an evaluation is being captured, the rebuild kernels go into the body of a graph conditional that
+  // k_rebuild_flag opens only when some system's flag is set: an evaluation that rebuilds nothing skips them (and the
+  // radix sort) altogether. Launched one by one (timing, or a runtime without conditionals), they run every
+  // evaluation and do work only for the flagged systems.
+  bool cond_ok = true;
+  void launch_rebuild(const Dev& d, cudaStream_t st) {
+    launches += 4;
+    k_wrap_bin<<<blocks(na, 256), 256, 0, st>>>(d);
+    size_t tmp = cub_tmp.n;
+    RXCU(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, key_bits, st));
+    k_cell_start<<<blocks(na + 1, 256), 256, 0, st>>>(d, cell_key_sorted.p);
+    k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, st>>>(d, dff);
+  }
   void build_lists(const Dev& d) {
     tic(0, "neighbors");
-    launches += 5;
+    ++launches;
     k_nbr_check<<<blocks(na, 256), 256, 0, stream>>>(d);
-    k_wrap_bin<<<blocks(na, 256), 256, 0, stream>>>(d);
-    size_t tmp = cub_tmp.n;
-    RXCU(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp, cell_key.p, cell_key_sorted.p, atom_iota.p, cell_atoms.p, na, 0, key_bits, stream));
-    k_cell_start<<<blocks(na + 1, 256), 256, 0, stream>>>(d, cell_key_sorted.p);
-    k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cond_ok && !timing) RXCU(cudaStreamIsCapturing(stream, &cs));
+    if (cs == cudaStreamCaptureStatusActive) {
+      cudaGraph_t g = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t nd = 0;
+      RXCU(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &g, &deps, &nd));
+      cudaGraphConditionalHandle h;
+      RXCU(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+      ++launches;
+      k_rebuild_flag<<<1, 256, 0, stream>>>(d, h);
+      RXCU(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &g, &deps, &nd));
+      cudaGraphNodeParams p{};
+      p.type = cudaGraphNodeTypeConditional;
+      p.conditional.handle = h;
+      p.conditional.type = cudaGraphCondTypeIf;
+      p.conditional.size = 1;
+      cudaGraphNode_t node = nullptr;
+      RXCU(cudaGraphAddNode(&node, g, deps, nd, &p));
+      RXCU(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+      RXCU(cudaStreamBeginCaptureToGraph(side_c, p.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      launch_rebuild(d, side_c);
+      cudaGraph_t body = nullptr;
+      RXCU(cudaStreamEndCapture(side_c, &body));
+    } else {
+      launch_rebuild(d, stream);
+    }
+    ++launches;
     k_pairs<<<blocks(static_cast<long long>(na) * 32, tune.tpb_pairs), tune.tpb_pairs, 0, stream>>>(d, dff, qp);
     toc(0);
   }
@@ -893,7 +930,7 @@ struct Context {
     for (int attempt = 0;; ++attempt) {
       RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * kStatusWords, stream));
       const int gi = do_qeq ? 1 : 0;
-      if (graphs_ok && !timing && !eval_graph[gi]) capture(eval_graph[gi], eval_launches[gi], [&] { enqueue_eval(do_qeq); });
+      if (graphs_ok && !timing && !eval_graph[gi]) capture_retry(eval_graph[gi], eval_launches[gi], [&] { enqueue_eval(do_qeq); });
       if (graphs_ok && !timing && eval_graph[gi]) {
         RXCU(cudaGraphLaunch(eval_graph[gi], stream));
         launches += eval_launches[gi];
@@ -1602,8 +1639,17 @@ struct Context {
     }
     return ok;
   }
+  // a capture that fails with the rebuild conditional is repeated once without it
+  template <class F>
+  bool capture_retry(cudaGraphExec_t& exec, long long& count, F&& fn) {
+    if (capture(exec, count, fn)) return true;
+    if (!cond_ok) return false;
+    cond_ok = false;
+    graphs_ok = true;
+    return capture(exec, count, fn);
+  }
   long long step_launches = 0;   // this engine's kernels in one captured MD step
-  bool capture_step() { return capture(md_graph, step_launches, [&] { enqueue_step(); }); }
+  bool capture_step() { return capture_retry(md_graph, step_launches, [&] { enqueue_step(); }); }
 
   // state that a chunk of steps changes, saved before the chunk so that an overflow (lists grown, chunk repeated)
   // restarts from it

@@ -47,6 +47,7 @@ struct CgArgs {
 __global__ void k_wrap_bin(Dev d);
 __global__ void k_cell_start(Dev d, const int* sorted_keys);
 __global__ void k_nbr_check(Dev d);
+__global__ void k_rebuild_flag(Dev d, cudaGraphConditionalHandle h);
 __global__ void k_neighbors(Dev d, DevFF ff);
 __global__ void k_pairs(Dev d, DevFF ff, QeqParams qp);
 __global__ void k_nonbonded(Dev d, DevFF ff);

@@ -87,6 +87,19 @@ __global__ void k_wrap_bin(Dev d) {
   d.cell_key[a] = s.cell_begin + (c[2] * s.nc[1] + c[1]) * s.nc[0] + c[0];
 }
 
+// Sets the captured evaluation's rebuild conditional: 1 when any system's Verlet rows are to be rebuilt (its flag set
+// by k_nbr_check or by the host), 0 otherwise, so that the wrap/bin, sort, cell-start and row kernels are skipped.
+__global__ void k_rebuild_flag(Dev d, cudaGraphConditionalHandle h) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int s = threadIdx.x; s < d.nsys; s += blockDim.x) mine |= d.sys_flag[s];
+  if (mine) atomicOr(&any, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
 // cell_start[c] = first position in the sorted order whose key is >= c; positions gathered into cell order
 __global__ void k_cell_start(Dev d, const int* sorted_keys) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
