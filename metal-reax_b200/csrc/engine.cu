@@ -1590,23 +1590,26 @@ struct Context {
     for (int a = 0; a < na; ++a) { vout[3 * a] = h[a].x; vout[3 * a + 1] = h[a].y; vout[3 * a + 2] = h[a].z; }
   }
 
-  void thermostat_half(int advance) {
-    launches += 3;
+  // the kinetic energy of the velocities as they stand, into md.ke (the chain's first half of a step starts from it)
+  void kinetic_now() {
+    launches += 2;
     k_md_kinetic_part<<<md.nchunks, 256, 0, stream>>>(md, sys.p, type.p);
-    k_md_chain<<<blocks(nsys, 64), 64, 0, stream>>>(md, sys.p, nsys);
-    k_md_scale<<<blocks(na, 256), 256, 0, stream>>>(md, sys_of.p, na, advance);
+    k_md_kinetic_sum<<<blocks(nsys, 64), 64, 0, stream>>>(md, nsys);
   }
 
-  // one velocity-Verlet step with the chain applied for dt/2 on each side (see md_kernels.cu), enqueued only
+  // one velocity-Verlet step with the chain applied for dt/2 on each side (see md_kernels.cu), enqueued only. First
+  // half: the chain from the kinetic energy the previous half left in md.ke, then scale, kick and drift in one kernel;
+  // second half: kick and the kinetic-energy partials in one kernel, the chain, the scale (and the ramp's step).
   bool md_qeq = true;   // charges re-equilibrated at every step of rx_md_run
   void enqueue_step() {
-    thermostat_half(0);
-    ++launches;
-    k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, sys_of.p, grad.p, x.p, na, 1);
+    launches += 2;
+    k_md_chain<<<blocks(nsys, 64), 64, 0, stream>>>(md, sys.p, nsys, 1);
+    k_md_scale_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, sys_of.p, grad.p, x.p, na);
     enqueue_eval(md_qeq);
-    ++launches;
-    k_md_kick<<<blocks(na, 256), 256, 0, stream>>>(md, type.p, sys_of.p, grad.p, x.p, na, 0);
-    thermostat_half(1);
+    launches += 3;
+    k_md_kick_kinetic<<<md.nchunks, 256, 0, stream>>>(md, sys.p, type.p, sys_of.p, grad.p);
+    k_md_chain<<<blocks(nsys, 64), 64, 0, stream>>>(md, sys.p, nsys, 0);
+    k_md_scale<<<blocks(na, 256), 256, 0, stream>>>(md, sys_of.p, na, 1);
   }
 
   // Capture the launches `fn` enqueues into a CUDA graph (every kernel argument is fixed at capture; what changes
@@ -1693,6 +1696,7 @@ struct Context {
       const int chunk = std::min(nsteps - done, kChunk);
       for (int attempt = 0;; ++attempt) {
         snapshot(true);
+        kinetic_now();   // md.ke of the chunk's starting velocities (set by the caller or restored by a repeat)
         RXCU(cudaMemsetAsync(status.p, 0, sizeof(int) * kStatusWords, stream));
         const bool use_graph = graphs_ok && !timing;
         if (use_graph && !md_graph) capture_step();

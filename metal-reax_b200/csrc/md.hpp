@@ -34,9 +34,10 @@ constexpr int kKeChunk = 1024;
 
 __global__ void k_md_kinetic_part(MdDev m, const SysInfo* sys, const int* type);
 __global__ void k_md_kinetic_sum(MdDev m, int nsys);
-__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys);
+__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys, int from_ke);
+__global__ void k_md_scale_kick(MdDev m, const int* type, const int* sys_of, const double4* grad, double4* x, int na);
+__global__ void k_md_kick_kinetic(MdDev m, const SysInfo* sys, const int* type, const int* sys_of, const double4* grad);
 __global__ void k_md_scale(MdDev m, const int* sys_of, int na, int advance);
-__global__ void k_md_kick(MdDev m, const int* type, const int* sys_of, const double4* grad, double4* x, int na, int drift);
 
 __global__ void k_gather_state(int n, const int* src, const double4* ox, const double* oq, const double* osh,
                                const double* oth, double4* x, double* q, double* sh, double* th);

@@ -49,8 +49,10 @@ __global__ void k_md_kinetic_sum(MdDev m, int nsys) {
   if (s < nsys) m.ke[s] = system_ke(m, s);
 }
 
-// one thread per system: advance the chain by dt/2 and produce the velocity scale factor
-__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys) {
+// one thread per system: advance the chain by dt/2 and produce the velocity scale factor. The kinetic energy is the
+// chunk partials' sum (from_ke 0) or m.ke (from_ke 1: the value the previous half step left, s^2 times the energy it
+// scaled, which is the kinetic energy of the velocities as they stand)
+__global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys, int from_ke) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
   if (m.active && !m.active[s]) {
@@ -60,7 +62,7 @@ __global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys) {
   const int M = m.chain;
   if (M == 0) {   // NVE: no thermostat; the current kinetic energy and temperature only
     const double nf0 = 3.0 * sys[s].natoms - 3.0;
-    const double ke = system_ke(m, s);
+    const double ke = from_ke ? m.ke[s] : system_ke(m, s);
     m.scale[s] = 1.0;
     m.ke[s] = ke;
     m.temp[s] = nf0 > 0.0 ? 2.0 * ke / (nf0 * kBoltz) : 0.0;
@@ -77,7 +79,7 @@ __global__ void k_md_chain(MdDev m, const SysInfo* sys, int nsys) {
   Q[0] = nf * kT * tau2;
   for (int k = 1; k < M; ++k) Q[k] = kT * tau2;
   const double dt = m.dt, dt2 = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
-  double ke2 = 2.0 * system_ke(m, s);
+  double ke2 = 2.0 * (from_ke ? m.ke[s] : system_ke(m, s));
   auto G = [&](int k) { return k == 0 ? (ke2 - nf * kT) / Q[0] : (Q[k - 1] * vx[k - 1] * vx[k - 1] - kT) / Q[k]; };
   vx[M - 1] += G(M - 1) * dt4;
   for (int k = M - 2; k >= 0; --k) {
@@ -112,21 +114,53 @@ __global__ void k_md_scale(MdDev m, const int* sys_of, int na, int advance) {
   m.v[a] = v;
 }
 
-// v += dt/2 * F/m (F = -grad); with drift: x += dt * v
-__global__ void k_md_kick(MdDev m, const int* type, const int* sys_of, const double4* grad, double4* x, int na, int drift) {
+// first half of a step, fused: v *= the chain's scale, v += dt/2 F/m (F = -grad), x += dt v
+__global__ void k_md_scale_kick(MdDev m, const int* type, const int* sys_of, const double4* grad, double4* x, int na) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= na) return;
-  if (m.active && !m.active[sys_of[a]]) return;
+  const int s = sys_of[a];
+  if (m.active && !m.active[s]) return;
+  const double sc = m.scale[s];
   const double c = 0.5 * m.dt * kFtm2v / m.mass[type[a]];
   const double4 g = grad[a];
   double4 v = m.v[a];
+  v.x *= sc; v.y *= sc; v.z *= sc;
   v.x -= c * g.x; v.y -= c * g.y; v.z -= c * g.z;
   m.v[a] = v;
-  if (drift) {
-    double4 p = x[a];
-    p.x += m.dt * v.x; p.y += m.dt * v.y; p.z += m.dt * v.z;
-    x[a] = p;
+  double4 p = x[a];
+  p.x += m.dt * v.x; p.y += m.dt * v.y; p.z += m.dt * v.z;
+  x[a] = p;
+}
+
+// second half of a step, fused: v += dt/2 F/m for the atoms of one kinetic-energy chunk, then the chunk's sum of
+// m v^2 in the fixed order of k_md_kinetic_part
+__global__ void k_md_kick_kinetic(MdDev m, const SysInfo* sys, const int* type, const int* sys_of, const double4* grad) {
+  const int c = blockIdx.x;
+  const int s = m.kchunk_sys[c];
+  const SysInfo& si = sys[s];
+  const int a0 = si.begin + (c - m.kchunk_first[s]) * kKeChunk;
+  const int a1 = min(a0 + kKeChunk, si.begin + si.natoms);
+  const bool act = !(m.active && !m.active[s]);
+  __shared__ double sh[256];
+  double v2 = 0.0;
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    const double mass = m.mass[type[a]];
+    double4 v = m.v[a];
+    if (act) {
+      const double cf = 0.5 * m.dt * kFtm2v / mass;
+      const double4 g = grad[a];
+      v.x -= cf * g.x; v.y -= cf * g.y; v.z -= cf * g.z;
+      m.v[a] = v;
+    }
+    v2 += mass * (v.x * v.x + v.y * v.y + v.z * v.z);
   }
+  sh[threadIdx.x] = v2;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) m.kpart[c] = sh[0];
 }
 
 // continuous batching: carry the state of kept atoms (new index a, old index src[a]) into the re-laid-out arrays
