@@ -115,8 +115,6 @@ struct Dev {
   int smax, S;
   const double4* shifts; // per system and shift index: L.s (xyz), summed as the reference sums lattice shifts
   // near rows: the entries of the full row within max(bond_cut, hbond_cut), in the same order
-  int* cpos;             // atom -> its position in cell order (written at every rebuild)
-  unsigned* pcol;        // per neighbor-row entry: cpos of the partner (column of the cell-ordered charge solve)
   int ncap_near;         // bond-candidate rows: entries within bond_cut (k_bonds)
   unsigned* near;
   int* near_cnt;

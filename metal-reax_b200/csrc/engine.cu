@@ -129,8 +129,7 @@ struct Context {
   // lists
   int ncap = 0, bcap = 0, ncap_near = 0, ncap_acc = 0, vcap = 0;
   double skin = 1.0;   // Verlet skin [A]: rows hold every image within nonb_cut + skin, rebuilt per system on demand
-  DBuf<unsigned> nbr, bcode, near, acc, vrow, pcol;
-  DBuf<int> cpos;
+  DBuf<unsigned> nbr, bcode, near, acc, vrow;
   DBuf<int> nbr_cnt, bsym, bcnt, near_cnt, acc_cnt, vcnt;
   DBuf<double4> shifts, xref;
   DBuf<float> hhi, hlo;
@@ -588,7 +587,7 @@ struct Context {
     Deltap.ensure(n); Deltap_boc.ensure(n); cdtot.ensure(n); W.ensure(n); eatom.ensure(n * kTerms);
     dDp_self.ensure(n); fown.ensure(n); fdb.ensure(n); fnb.ensure(n); grad.ensure(n);
     aq.ensure(n); census.ensure(n * kCensus);
-    nbr_cnt.ensure(n); bcnt.ensure(n); near_cnt.ensure(n); acc_cnt.ensure(n); vcnt.ensure(n); cpos.ensure(n); xref.ensure(n);
+    nbr_cnt.ensure(n); bcnt.ensure(n); near_cnt.ensure(n); acc_cnt.ensure(n); vcnt.ensure(n); xref.ensure(n);
     sys_flag.ensure(static_cast<size_t>(nsys)); cg_nref.ensure(1); cg_brk.ensure(static_cast<size_t>(nsys));
     energies.ensure(static_cast<size_t>(nsys) * kTerms);
     virial.ensure(static_cast<size_t>(nsys) * kVir);
@@ -606,7 +605,6 @@ struct Context {
     const size_t n = static_cast<size_t>(na);
     vrow.ensure(n * vcap);
     nbr.ensure(n * ncap);
-    pcol.ensure(n * ncap);
     hhi.ensure(n * ncap);
     hlo.ensure(n * ncap);
     near.ensure(n * ncap_near);
@@ -636,7 +634,6 @@ struct Context {
     d.abits = abits; d.amask = (abits >= 32) ? 0xffffffffu : ((1u << abits) - 1u); d.smax = smax; d.S = S;
     d.shifts = shifts.p; d.ncap_near = ncap_near; d.near = near.p; d.near_cnt = near_cnt.p;
     d.ncap_acc = ncap_acc; d.acc = acc.p; d.acc_cnt = acc_cnt.p;
-    d.cpos = cpos.p; d.pcol = pcol.p;
     {  // the short Verlet rows (rebuilt with the Verlet rows): supersets of the consumers' exact sqrt(r2) <= cut tests for
        // every position until the next rebuild (each atom moves less than skin/2 meanwhile)
       const double rn = (ctl.bond_cut + skin) * (1.0 + 1e-9), ra = (ctl.hbond_cut + skin) * (1.0 + 1e-9);
@@ -736,13 +733,8 @@ struct Context {
     toc(0);
   }
 
-  bool lone_cg() const { return nsys == 1 && na > tune.lone_grid_min; }   // the single-system (cell-ordered) CG
   CgArgs cg_args() {
     CgArgs a{};
-    if (lone_cg()) {
-      a.pos = cpos.p;
-      a.perm = cell_atoms.p;
-    }
     a.imax = qeq_imax; a.tol = qeq_tol;
     a.x = cg_x.p; a.b = cg_b.p; a.r = cg_r.p; a.d = cg_d.p; a.p = cg_p.p; a.q = cg_q.p; a.df = cg_df.p; a.eta = cg_eta.p; a.part = cg_part.p;
     a.out_iters = cg_iters.p; a.out_rel = cg_rel.p; a.out_nref = cg_nref.p; a.out_brk = cg_brk.p; a.write_q = 1;
@@ -762,7 +754,7 @@ struct Context {
   } tune;
   int grid_per_sm = 0, seg_per_sm = 0;
   void launch_cg(const Dev& d, CgArgs a) {
-    if (lone_cg()) {   // one large system: all SMs on its rows (in cell order), block partials in block order
+    if (nsys == 1 && na > tune.lone_grid_min) {   // one large system: all SMs on its rows, block partials in block order
       const int threads = 256;
       if (!grid_per_sm) RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k_cg_grid, threads, 0));
       const int per_sm = tune.cg_per_sm > 0 ? std::min(tune.cg_per_sm, grid_per_sm) : grid_per_sm;
@@ -795,7 +787,7 @@ struct Context {
     k_qeq_prepare<<<blocks(na, 256), 256, 0, stream>>>(d, dff, a, s_hist.p, t_hist.p);
     launch_cg(d, a);
     ++launches;
-    k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, a.pos, s_hist.p, t_hist.p, qeq_strict);
+    k_qeq_history<<<blocks(na, 256), 256, 0, stream>>>(d, cg_x.p, s_hist.p, t_hist.p, qeq_strict);
     toc(1);
   }
 
@@ -1346,13 +1338,7 @@ struct Context {
     fetch_qeq_counts();
     std::vector<double2> xh(static_cast<size_t>(na));
     std::vector<int> brk(static_cast<size_t>(nsys));
-    const double2* xs = cg_x.p;
-    if (a.pos) {   // the cell-ordered solution, back in atom order (into the residual vector, free after the solve)
-      ++launches;
-      k_cg_to_atoms<<<blocks(na, 256), 256, 0, stream>>>(na, a.pos, cg_x.p, cg_r.p);
-      xs = cg_r.p;
-    }
-    RXCU(cudaMemcpyAsync(xh.data(), xs, sizeof(double2) * na, cudaMemcpyDeviceToHost, stream));
+    RXCU(cudaMemcpyAsync(xh.data(), cg_x.p, sizeof(double2) * na, cudaMemcpyDeviceToHost, stream));
     RXCU(cudaMemcpyAsync(brk.data(), cg_brk.p, sizeof(int) * nsys, cudaMemcpyDeviceToHost, stream));
     RXCU(cudaStreamSynchronize(stream));
     RXCU(cudaGetLastError());

@@ -37,10 +37,6 @@ struct CgArgs {
   int* out_nref;   // FP64 residual passes of the last single-system solve (may be null)
   int* out_brk;    // per system: 1 after a breakdown (a step length that is not finite)
   int write_q;     // 1: calculate_Q into the charges (the fix's solve); 0: solutions only
-  // single-system CG: the vectors are held in cell order (spatially sorted), so that the gathers of a row product
-  // touch neighbouring entries. pos[atom] = vector index, perm[vector index] = atom; null: atom order
-  const int* pos;
-  const int* perm;
   // segmented CG only
   SysCg* sc;       // nsys
   double2* rb0;    // per-row dot-product terms (fixed-order per-system sums)
@@ -60,8 +56,7 @@ __global__ void k_cg_grid(Dev d, CgArgs a);
 __global__ void k_cg_seg(Dev d, CgArgs a);
 __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, const double* t_hist);
 __global__ void k_qeq_prepare_given(Dev d, DevFF ff, CgArgs a, const double* b, const double* x0);
-__global__ void k_qeq_history(Dev d, const double2* x, const int* pos, double* s_hist, double* t_hist, int strict);
-__global__ void k_cg_to_atoms(int n, const int* pos, const double2* src, double2* dst);
+__global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist, int strict);
 __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y);
 __global__ void k_energy_sum(Dev d, double* out, double* out_vir);
 

@@ -112,7 +112,6 @@ __global__ void k_cell_start(Dev d, const int* sorted_keys) {
     double4 x = d.x[a];
     x.w = static_cast<double>(d.type[a]);
     d.xs[p] = x;
-    d.cpos[a] = p;
   }
 }
 
@@ -294,7 +293,6 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
       const int pos = count + __popc(m & lt);
       if (pos < d.ncap) {
         d.nbr[rowbase + pos] = code;
-        d.pcol[rowbase + pos] = static_cast<unsigned>(d.cpos[j]);
         const double r = sqrt(r2);
         double h = 0.0;
         if (r <= qp.swb) {
@@ -561,60 +559,28 @@ __device__ inline double2 row_mv(const Dev& d, int i, double eta, const double2*
   return make_double2(eta * vi.x + __shfl_sync(0xffffffffu, ys, 0), eta * vi.y + __shfl_sync(0xffffffffu, yt, 0));
 }
 
-// Row products of the cell-ordered single-system solve: the row of atom `row` (stored in atom order), its columns
-// pcol in cell order, the vector v (and its FP32 copy vf) in cell order with this row's own entry at vr. Lane l takes
-// entries l, l + 32, ..., so that one gather instruction of the warp reads 32 consecutive row entries - neighbours in
-// the cell-run order of the row, hence close together in the cell-ordered vector.
-__device__ inline double2 row_mv_cell_f32(const Dev& d, int row, int vr, double eta, const double2* v, const float2* vf) {
-  const int cnt = min(d.nbr_cnt[row], d.ncap);
+// (A v)_i of the single-precision-matrix iterations: FP32 values of the matrix (hhi) times the FP32 copy vf of v,
+// products and sums in FP64; the diagonal term takes v_i itself. Gathering 8-byte float2 halves the bytes of the
+// gathers (the vector of a 24k-atom system then fits in an SM's L1).
+__device__ inline double2 row_mv_f32(const Dev& d, int i, double eta, const double2* v, const float2* vf) {
+  const int cnt = min(d.nbr_cnt[i], d.ncap);
   const int lane = threadIdx.x & 31;
-  const double2 vi = v[vr];
+  const double2 vi = v[i];
   double ys = 0.0, yt = 0.0;
-  const size_t base = static_cast<size_t>(row) * d.ncap;
-  for (int e0 = lane; e0 < cnt; e0 += 256) {
-    unsigned cc[8];
-    float hh[8];
+  const size_t base = static_cast<size_t>(i) * d.ncap;
+  for (int e0 = lane * 8; e0 < cnt; e0 += 256) {   // eight entries per lane in flight (rows hold ncap, a multiple of 32)
+    const uint4 c4a = *reinterpret_cast<const uint4*>(d.nbr + base + e0);
+    const uint4 c4b = *reinterpret_cast<const uint4*>(d.nbr + base + e0 + 4);
+    const float4 h4a = *reinterpret_cast<const float4*>(d.hhi + base + e0);
+    const float4 h4b = *reinterpret_cast<const float4*>(d.hhi + base + e0 + 4);
+    const unsigned cc[8] = {c4a.x, c4a.y, c4a.z, c4a.w, c4b.x, c4b.y, c4b.z, c4b.w};
+    const float hh[8] = {h4a.x, h4a.y, h4a.z, h4a.w, h4b.x, h4b.y, h4b.z, h4b.w};
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const int e = e0 + 32 * k;
-      cc[k] = e < cnt ? d.pcol[base + e] : 0u;
-      hh[k] = e < cnt ? d.hhi[base + e] : 0.f;
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      if (e0 + 32 * k < cnt) {
-        const float2 vj = vf[cc[k]];
+      if (e0 + k < cnt) {
+        const float2 vj = vf[cc[k] & d.amask];
         ys += static_cast<double>(hh[k]) * static_cast<double>(vj.x);
         yt += static_cast<double>(hh[k]) * static_cast<double>(vj.y);
-      }
-    }
-  }
-  ys = warp_sum(ys);
-  yt = warp_sum(yt);
-  return make_double2(eta * vi.x + __shfl_sync(0xffffffffu, ys, 0), eta * vi.y + __shfl_sync(0xffffffffu, yt, 0));
-}
-// the same with the FP64 matrix (hi + lo) and the FP64 vector
-__device__ inline double2 row_mv_cell(const Dev& d, int row, int vr, double eta, const double2* v) {
-  const int cnt = min(d.nbr_cnt[row], d.ncap);
-  const int lane = threadIdx.x & 31;
-  const double2 vi = v[vr];
-  double ys = 0.0, yt = 0.0;
-  const size_t base = static_cast<size_t>(row) * d.ncap;
-  for (int e0 = lane; e0 < cnt; e0 += 128) {
-    unsigned cc[4];
-    double hh[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int e = e0 + 32 * k;
-      cc[k] = e < cnt ? d.pcol[base + e] : 0u;
-      hh[k] = e < cnt ? static_cast<double>(d.hhi[base + e]) + static_cast<double>(d.hlo[base + e]) : 0.0;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (e0 + 32 * k < cnt) {
-        const double2 vj = v[cc[k]];
-        ys += hh[k] * vj.x;
-        yt += hh[k] * vj.y;
       }
     }
   }
@@ -669,10 +635,8 @@ __device__ inline void grid_totals(const double* part, int nblocks, double* tot,
 // direction (products and sums in FP64), the vectors and every dot product are FP64, and the residual is recomputed with the FP64 matrix (hi + lo) whenever the iterations have
 // converged - or have reduced the residual by kRefineDrop, below which the single-precision matrix stops helping. The
 // solve ends only on that FP64 residual, so the tolerance and the reported residuals are those of the FP64 system.
-// Rows are distributed over all warps of the grid in cell order (the vectors are held in cell order, a.pos / a.perm,
-// so that the gathers of neighbouring rows and lanes touch neighbouring entries); reductions are fixed-order
-// (per-block partials summed in block order), so the result is bitwise reproducible. Only grid.sync() waits; the kernel
-// is launched cooperatively.
+// Rows are distributed over all warps of the grid; reductions are fixed-order (per-block partials summed in block
+// order), so the result is bitwise reproducible. Only grid.sync() waits; the kernel is launched cooperatively.
 constexpr double kRefineDrop = 1e-6;
 
 __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
@@ -696,7 +660,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
     for (int r = gw; r < n; r += nwarps) {
       const int i = i0 + r;
       const double eta = a.eta[i];
-      const double2 y = row_mv_cell(d, a.perm[i], i, eta, a.x);
+      const double2 y = row_mv(d, i, eta, a.x);
       if (lane == 0) {
         const double2 b = a.b[i];
         const double2 rr = make_double2(b.x - y.x, b.y - y.y);
@@ -734,7 +698,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
       loc[0] = loc[1] = 0.0;
       for (int r = gw; r < n; r += nwarps) {
         const int i = i0 + r;
-        const double2 y = row_mv_cell_f32(d, a.perm[i], i, a.eta[i], a.d, a.df);
+        const double2 y = row_mv_f32(d, i, a.eta[i], a.d, a.df);
         if (lane == 0) {
           a.q[i] = y;
           const double2 dd = a.d[i];
@@ -799,7 +763,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
   if (a.write_q)
     for (int r = gw * 32 + lane; r < n; r += nwarps * 32) {
       const double2 xx = a.x[i0 + r];
-      d.q[a.perm[i0 + r]] = xx.x - u * xx.y;
+      d.q[i0 + r] = xx.x - u * xx.y;
     }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (a.out_brk) a.out_brk[0] = breakdown ? 1 : 0;
@@ -1048,10 +1012,9 @@ __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, c
   const int t = d.type[i];
   const double* sh = s_hist + 4 * static_cast<size_t>(i);
   const double* th = t_hist + 4 * static_cast<size_t>(i);
-  const int v = a.pos ? a.pos[i] : i;
-  a.x[v] = make_double2(4 * (sh[0] + sh[2]) - (6 * sh[1] + sh[3]), th[2] + 3 * (th[0] - th[1]));
-  a.b[v] = make_double2(-ff.sb[t * SB_N + SB_CHI], -1.0);
-  a.eta[v] = ff.sb[t * SB_N + SB_ETA];
+  a.x[i] = make_double2(4 * (sh[0] + sh[2]) - (6 * sh[1] + sh[3]), th[2] + 3 * (th[0] - th[1]));
+  a.b[i] = make_double2(-ff.sb[t * SB_N + SB_CHI], -1.0);
+  a.eta[i] = ff.sb[t * SB_N + SB_ETA];
 }
 
 // A solve of given right-hand sides from given guesses (mtl::Context::qeq_solve, metal_backend.hpp:84-86): b and x0
@@ -1059,22 +1022,15 @@ __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, c
 __global__ void k_qeq_prepare_given(Dev d, DevFF ff, CgArgs a, const double* b, const double* x0) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.na) return;
-  const int v = a.pos ? a.pos[i] : i;
-  a.x[v] = x0 ? make_double2(x0[i], x0[d.na + i]) : make_double2(0.0, 0.0);
-  a.b[v] = make_double2(b[i], b[d.na + i]);
-  a.eta[v] = ff.sb[d.type[i] * SB_N + SB_ETA];
-}
-
-// the solution in atom order (dst[atom] = src[pos[atom]]) for a caller of the cell-ordered solve
-__global__ void k_cg_to_atoms(int n, const int* pos, const double2* src, double2* dst) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) dst[i] = src[pos[i]];
+  a.x[i] = x0 ? make_double2(x0[i], x0[d.na + i]) : make_double2(0.0, 0.0);
+  a.b[i] = make_double2(b[i], b[d.na + i]);
+  a.eta[i] = ff.sb[d.type[i] * SB_N + SB_ETA];
 }
 
 // the solve just finished becomes the newest history entry; not after a list overflow (the evaluation is repeated),
 // nor after a failed solve (a breakdown, or a system above its tolerance in strict mode): the call then reports an
 // error and leaves the histories as they were
-__global__ void k_qeq_history(Dev d, const double2* x, const int* pos, double* s_hist, double* t_hist, int strict) {
+__global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist, int strict) {
   if (lists_failed(d)) return;
   const int st = *reinterpret_cast<volatile const int*>(d.status);
   if ((st & ST_CG_BREAKDOWN) || (strict && (st & ST_CG_NOTCONV))) return;
@@ -1083,9 +1039,8 @@ __global__ void k_qeq_history(Dev d, const double2* x, const int* pos, double* s
   double* sh = s_hist + 4 * static_cast<size_t>(i);
   double* th = t_hist + 4 * static_cast<size_t>(i);
   for (int k = 3; k > 0; --k) { sh[k] = sh[k - 1]; th[k] = th[k - 1]; }
-  const double2 xi = x[pos ? pos[i] : i];
-  sh[0] = xi.x;
-  th[0] = xi.y;
+  sh[0] = x[i].x;
+  th[0] = x[i].y;
 }
 
 // y = (diag(eta) + H) v, owned rows (mtl::Context::qeq_matvec)
