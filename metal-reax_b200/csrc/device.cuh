@@ -52,6 +52,11 @@ struct SysInfo {
   double h[3];    // distances between opposite faces (heights) along each lattice direction
   int ortho;      // lattice vectors mutually orthogonal
   int per[3];     // periodic directions; along the others the lattice vector is the engine's own padded extent
+  double ext;     // |a| + |b| + |c|: bounds every coordinate of a wrapped position relative to origin
+  double inv_nc[3], inv_h[3];
+  float inv_ncf0;
+  // single-precision r^2 thresholds of the Verlet, bond-candidate and acceptor rows (see layout_systems)
+  float vthr[3];
 };
 
 struct DevFF {
@@ -92,7 +97,7 @@ struct Dev {
   // cells
   int* cell_key;         // global cell of every atom (sort key)
   int* cell_atoms;       // atoms sorted by cell
-  double4* xs;           // positions in cell order (w = type), so candidate loads are contiguous
+  float4* xs;            // positions in cell order relative to their system's origin, single precision (w = type)
   int* cell_start;       // ncell_total + 1
   int ncell_total;
   // Verlet rows: every image within nonb_cut + skin at the last rebuild of the atom's system (rebuilt when an atom of

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -117,7 +118,7 @@ struct Context {
   std::vector<SysInfo> huser;   // systems as the caller gave them
   DBuf<SysInfo> sys;
   DBuf<int> sys_of, type, cell_key, cell_key_sorted, cell_atoms, atom_iota, cell_start, sys_flag;
-  DBuf<double4> xs;
+  DBuf<float4> xs;
   DBuf<long long> tag;
   DBuf<double4> x;
   DBuf<double> q;
@@ -500,6 +501,8 @@ struct Context {
                            det / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2])};
       long long ncell = 1;
       for (int k = 0; k < 3; ++k) si.h[k] = h[k];
+      si.ext = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]) + std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) +
+               std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
       {
         auto dotp = [](const double* u, const double* w) { return u[0] * w[0] + u[1] * w[1] + u[2] * w[2]; };
         si.ortho = (dotp(a, b) == 0.0 && dotp(a, c) == 0.0 && dotp(b, c) == 0.0) ? 1 : 0;
@@ -522,6 +525,26 @@ struct Context {
     }
     smax = sm;
     S = 2 * smax + 1;
+    // Thresholds of the single-precision candidate test of the Verlet build (rows need only be supersets). With
+    // u = 2^-24, each component of the separation (x_j - o) + (L s - (x_i - o)), both terms rounded to single precision
+    // and then added, is off by at most delta = u (|x_j - o| + |L s - (x_i - o)| + |dv|) <= u ((2 + smax) ext + R_v)
+    // (wrapped coordinates are within ext of the origin, |L s| <= smax ext). For a true distance r <= R the computed
+    // r^2 is then at most R^2 (1 + 3u) + 2 sqrt(3) R delta + 3 delta^2: the thresholds exceed that and round up.
+    for (auto& si : hsys) {
+      const double u = 5.9604644775390625e-8, Rv = rc;
+      const double delta = u * 1.001 * ((2.0 + smax) * si.ext + Rv);
+      auto thr = [&](double R) {
+        const double t = R * R * (1.0 + 6.0 * u) + 3.5 * R * delta + 3.0 * delta * delta;
+        float f = static_cast<float>(t);
+        if (static_cast<double>(f) < t) f = std::nextafter(f, std::numeric_limits<float>::infinity());
+        return f;
+      };
+      si.vthr[0] = thr(Rv);
+      si.vthr[1] = thr((ctl.bond_cut + skin) * (1.0 + 1e-9));
+      si.vthr[2] = thr((ctl.hbond_cut + skin) * (1.0 + 1e-9));
+      for (int k = 0; k < 3; ++k) { si.inv_nc[k] = 1.0 / si.nc[k]; si.inv_h[k] = 1.0 / si.h[k]; }
+      si.inv_ncf0 = 1.0f / static_cast<float>(si.nc[0]);
+    }
     const long long nshift = static_cast<long long>(S) * S * S;
     int sbits = 0;
     while ((1LL << sbits) < nshift) ++sbits;
@@ -698,6 +721,11 @@ struct Context {
     k_neighbors<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, st>>>(d, dff);
   }
   void build_lists(const Dev& d) {
+    build_rows(d);
+    launch_pairs(d);
+  }
+  // the Verlet check and, where some system is flagged, the rebuild of its rows (the bonded chain needs only these)
+  void build_rows(const Dev& d) {
     tic(0, "neighbors");
     ++launches;
     k_nbr_check<<<blocks(na, 256), 256, 0, stream>>>(d);
@@ -728,6 +756,9 @@ struct Context {
     } else {
       launch_rebuild(d, stream);
     }
+  }
+  // the per-step exact filter of the Verlet rows into the neighbor rows and the charge matrix
+  void launch_pairs(const Dev& d) {
     ++launches;
     k_pairs<<<blocks(static_cast<long long>(na) * 32, tune.tpb_pairs), tune.tpb_pairs, 0, stream>>>(d, dff, qp);
     toc(0);
@@ -791,9 +822,9 @@ struct Context {
     toc(1);
   }
 
-  // After the rows, the bonded chain (bond orders, then k_bonded_atom, with the H-bonds on `side_h` and the torsions
-  // on `side_t`, then the bonded gathers k_fold and k_dbond) needs no charge, so with tune.overlap it runs on `side`
-  // next to the charge solve; the non-bonded pairs follow the charges on `stream`, and k_force_final joins both. Each branch writes its own arrays (fnb, vir_nb; bacc/bfn/fown; *_h; *_t, Tl), and
+  // After the Verlet check and rebuild, the bonded chain (bond orders, then k_bonded_atom, with the H-bonds on `side_h`
+  // and the torsions on `side_t`, then the bonded gathers k_fold and k_dbond) needs neither the neighbor rows nor the
+  // charges, so with tune.overlap it runs on `side` next to the row filter and the charge solve; the non-bonded pairs follow the charges on `stream`, and k_force_final joins both. Each branch writes its own arrays (fnb, vir_nb; bacc/bfn/fown; *_h; *_t, Tl), and
   // all join before the gathers, which add them in fixed order, so the schedule changes no result bit. With timing
   // on, every branch runs on `stream`, one after the other, so each phase is timed alone.
   void launch_bonded(const Dev& d) {
@@ -865,11 +896,18 @@ struct Context {
   // bonded chain is forked after the charges instead (the non-bonded pairs then run beside it).
   void enqueue_eval(bool do_qeq) {
     const Dev d = dev();
-    build_lists(d);
-    if (tune.overlap) {
+    build_rows(d);
+    if (tune.overlap && !timing) {
+      // the bonded chain forks off before the row filter: it reads only the short rows and the positions
+      launch_bonded(d);
+      launch_pairs(d);
+      if (do_qeq) launch_qeq(d);
+    } else if (tune.overlap) {
+      launch_pairs(d);
       launch_bonded(d);
       if (do_qeq) launch_qeq(d);
     } else {
+      launch_pairs(d);
       if (do_qeq) launch_qeq(d);
       launch_bonded(d);
     }

@@ -14,6 +14,10 @@ namespace rx {
 __global__ void k_nbr_check(Dev d) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= d.na) return;
+  // this evaluation's H-bond acceptor accumulators and per-atom energy tallies start from zero (the first kernel of an
+  // evaluation: the bonded branch may start before the row filter)
+  for (int c = 0; c < 3; ++c) d.fix_h[3 * static_cast<size_t>(a) + c] = 0ull;
+  if (d.pe_on) d.pe_fix[a] = 0ull;
   const int s = d.sys_of[a];
   const double4 x = d.x[a];
   if (!(isfinite(x.x) && isfinite(x.y) && isfinite(x.z))) {
@@ -100,7 +104,8 @@ __global__ void k_rebuild_flag(Dev d, cudaGraphConditionalHandle h) {
   if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
 }
 
-// cell_start[c] = first position in the sorted order whose key is >= c; positions gathered into cell order
+// cell_start[c] = first position in the sorted order whose key is >= c; positions gathered into cell order, relative to
+// their system's origin and rounded to single precision (the candidate scan of the Verlet rows reads only these)
 __global__ void k_cell_start(Dev d, const int* sorted_keys) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p > d.na) return;
@@ -109,9 +114,10 @@ __global__ void k_cell_start(Dev d, const int* sorted_keys) {
   for (int c = prev + 1; c <= cur; ++c) d.cell_start[c] = p;
   if (p < d.na) {
     const int a = d.cell_atoms[p];
-    double4 x = d.x[a];
-    x.w = static_cast<double>(d.type[a]);
-    d.xs[p] = x;
+    const double4 x = d.x[a];
+    const double* o = d.sys[d.sys_of[a]].origin;
+    d.xs[p] = make_float4(static_cast<float>(x.x - o[0]), static_cast<float>(x.y - o[1]), static_cast<float>(x.z - o[2]),
+                          static_cast<float>(d.type[a]));
   }
 }
 
@@ -130,7 +136,10 @@ __device__ inline void taper_horner(const double* c, double r, double& Tap, doub
 // owned-row cut-off of build_far_list, src/neighbor/neighbor.cpp:180-212). The cells within `range` of the atom's cell
 // are visited as runs of consecutive cells along x (one contiguous range of the cell-ordered atoms per run and periodic
 // image), so the candidate loads are coalesced. Entries are written through a warp ballot in visiting order
-// (deterministic).
+// (deterministic). Rows only need to be supersets (every consumer re-tests its entries exactly in FP64 on the current
+// positions), so candidates are tested in single precision against the system's thresholds SysInfo::vthr, which add
+// the largest rounding error of that r^2 to the FP64 radii. The loops carry the wrapped cell and image of each row
+// incrementally and prune with precomputed reciprocals: no division per run.
 __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d, DevFF ff) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -138,70 +147,81 @@ __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d, DevFF ff) {
   const int i = warp;
   const int sy = d.sys_of[i];
   if (!d.sys_flag[sy]) return;
-  const SysInfo s = d.sys[sy];
+  const SysInfo& s = d.sys[sy];
+  const int nc0 = s.nc[0], nc1 = s.nc[1], nc2 = s.nc[2];
   const int key = d.cell_key[i] - s.cell_begin;
-  const int cx = key % s.nc[0], cy = (key / s.nc[0]) % s.nc[1], cz = key / (s.nc[0] * s.nc[1]);
+  const int cx = key % nc0, cy = (key / nc0) % nc1, cz = key / (nc0 * nc1);
   const double4 xi = d.x[i];
   int count = 0, count_near = 0, count_acc = 0;
   const unsigned lt = (1u << lane) - 1u;
   const int center = (d.S * d.S * d.S - 1) / 2;
   const size_t rowbase = static_cast<size_t>(i) * d.vcap;
   const bool hb_i = static_cast<int>(ff.sb[d.type[i] * SB_N + SB_P_HBOND]) == 1;
+  const float tv = s.vthr[0], tn = s.vthr[1], ta = s.vthr[2];
+  const int smax = d.smax, S = d.S, sbase = s.shift_base;
+  const double oxi = xi.x - s.origin[0], oyi = xi.y - s.origin[1], ozi = xi.z - s.origin[2];
   // fractional coordinates of i: lower bounds of the distance to a cell slab prune whole runs and clip the x range
   double fi[3];
-  for (int k = 0; k < 3; ++k)
-    fi[k] = s.R[3 * k] * (xi.x - s.origin[0]) + s.R[3 * k + 1] * (xi.y - s.origin[1]) + s.R[3 * k + 2] * (xi.z - s.origin[2]);
-  const double rcut = sqrt(d.rv2);
-  const double rc = rcut * (1.0 + 1e-9) + 1e-9;
+  for (int k = 0; k < 3; ++k) fi[k] = s.R[3 * k] * oxi + s.R[3 * k + 1] * oyi + s.R[3 * k + 2] * ozi;
+  const double rc = sqrt(d.rv2) * (1.0 + 1e-9) + 1e-9;
   auto slab_gap = [&](int k, int c) {   // distance from i to the slab of cell index c (unwrapped) along direction k
-    const double lo = static_cast<double>(c) / s.nc[k], hi = static_cast<double>(c + 1) / s.nc[k];
+    const double lo = static_cast<double>(c) * s.inv_nc[k], hi = static_cast<double>(c + 1) * s.inv_nc[k];
     const double g = fmax(0.0, fmax(lo - fi[k], fi[k] - hi));
     return fmax(0.0, g * s.h[k] - 1e-9 * s.h[k]);
   };
-  for (int oz = -s.range[2]; oz <= s.range[2]; ++oz) {
-    const int zz = cz + oz, shz = floor_div(zz, s.nc[2]), wz = zz - shz * s.nc[2];
+  auto advance = [](int& w, int& sh, int n) { if (++w == n) { w = 0; ++sh; } };
+  int shz = floor_div(cz - s.range[2], nc2), wz = cz - s.range[2] - shz * nc2;
+  const int shy0 = floor_div(cy - s.range[1], nc1), wy0 = cy - s.range[1] - shy0 * nc1;
+  for (int zz = cz - s.range[2]; zz <= cz + s.range[2]; ++zz, advance(wz, shz, nc2)) {
     const double gz = slab_gap(2, zz);
     if (gz > rc) continue;
-    for (int oy = -s.range[1]; oy <= s.range[1]; ++oy) {
-      const int yy = cy + oy, shy = floor_div(yy, s.nc[1]), wy = yy - shy * s.nc[1];
+    int shy = shy0, wy = wy0;
+    for (int yy = cy - s.range[1]; yy <= cy + s.range[1]; ++yy, advance(wy, shy, nc1)) {
       const double gy = slab_gap(1, yy);
       double rx;
       if (s.ortho) {
         const double g2 = gy * gy + gz * gz;
         if (g2 > rc * rc) continue;
-        rx = sqrt(rc * rc - g2);
+        // single-precision square root widened past its rounding error: the x range only needs to be a superset
+        rx = static_cast<double>(sqrtf(static_cast<float>(rc * rc - g2)) * 1.000001f) + 1e-6;
       } else {
         if (gy > rc) continue;
         rx = rc;
       }
-      const int rowcell = s.cell_begin + (wz * s.nc[1] + wy) * s.nc[0];
-      const double fx_lo = fi[0] - rx / s.h[0], fx_hi = fi[0] + rx / s.h[0];
-      int xx = max(cx - s.range[0], static_cast<int>(floor(fx_lo * s.nc[0])));
-      const int xend = min(cx + s.range[0], static_cast<int>(floor(fx_hi * s.nc[0])));
-      while (xx <= xend) {
-        const int shx = floor_div(xx, s.nc[0]);
-        const int wx0 = xx - shx * s.nc[0];
-        const int len = min(s.nc[0] - wx0, xend - xx + 1);
+      const int rowcell = s.cell_begin + (wz * nc1 + wy) * nc0;
+      const double dfx = rx * s.inv_h[0];
+      int xx = max(cx - s.range[0], static_cast<int>(floor((fi[0] - dfx) * nc0)));
+      const int xend = min(cx + s.range[0], static_cast<int>(floor((fi[0] + dfx) * nc0)));
+      if (xx > xend) continue;
+      // wrapped cell and image of the first run; each further run starts a new image at cell 0
+      int shx = __float2int_rd(static_cast<float>(xx) * s.inv_ncf0), wx0 = xx - shx * nc0;
+      if (wx0 < 0) { wx0 += nc0; --shx; } else if (wx0 >= nc0) { wx0 -= nc0; ++shx; }
+      for (; xx <= xend; wx0 = 0, ++shx) {
+        const int len = min(nc0 - wx0, xend - xx + 1);
         xx += len;
-        if (shx < -d.smax || shx > d.smax || shy < -d.smax || shy > d.smax || shz < -d.smax || shz > d.smax) {
+        if (shx < -smax || shx > smax || shy < -smax || shy > smax || shz < -smax || shz > smax) {
           if (lane == 0) atomicOr(d.status, ST_SHIFT_RANGE);
           continue;
         }
-        const int sidx = ((shx + d.smax) * d.S + (shy + d.smax)) * d.S + (shz + d.smax);
+        const int sidx = ((shx + smax) * S + (shy + smax)) * S + (shz + smax);
         const int c0 = d.cell_start[rowcell + wx0], c1 = d.cell_start[rowcell + wx0 + len];
+        if (c0 >= c1) continue;
+        // the run's image: separation = xs[p] + cimg, cimg = L s - (x_i - origin) in FP64 rounded once
+        const double4 sh = d.shifts[sbase + sidx];
+        const float3 cimg = make_float3(static_cast<float>(sh.x - oxi), static_cast<float>(sh.y - oyi), static_cast<float>(sh.z - ozi));
         for (int base = c0; base < c1; base += 32) {
           const int p = base + lane;
           bool ok = false;
           int j = 0;
-          double r2 = 0.0;
+          float r2 = 0.f, tj = 0.f;
           if (p < c1) {
             j = d.cell_atoms[p];
-            const double4 xj = d.xs[p];
+            const float4 xj = d.xs[p];
+            tj = xj.w;
             if (!(j == i && sidx == center)) {
-              double dv[3];
-              pair_dvec_x(d, s, i, j, sidx, xi, xj, dv);
-              r2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
-              ok = r2 <= d.rv2;
+              const float dx = xj.x + cimg.x, dy = xj.y + cimg.y, dz = xj.z + cimg.z;
+              r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+              ok = r2 <= tv;
             }
           }
           const unsigned code = static_cast<unsigned>(j) | (static_cast<unsigned>(sidx) << d.abits);
@@ -212,7 +232,7 @@ __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d, DevFF ff) {
           }
           count += __popc(m);
           // the short Verlet rows of the bond and H-bond kernels (their own exact tests run on every evaluation)
-          const bool nr = ok && r2 <= d.rnear2;
+          const bool nr = ok && r2 <= tn;
           const unsigned mn = __ballot_sync(0xffffffffu, nr);
           if (nr) {
             const int posn = count_near + __popc(mn & lt);
@@ -220,7 +240,7 @@ __global__ void __launch_bounds__(128, 6) k_neighbors(Dev d, DevFF ff) {
           }
           count_near += __popc(mn);
           if (hb_i) {   // warp-uniform
-            const bool ac = ok && r2 <= d.racc2 && static_cast<int>(ff.sb[d.type[j] * SB_N + SB_P_HBOND]) == 2;
+            const bool ac = ok && r2 <= ta && static_cast<int>(ff.sb[static_cast<int>(tj) * SB_N + SB_P_HBOND]) == 2;
             const unsigned ma = __ballot_sync(0xffffffffu, ac);
             if (ac) {
               const int posa = count_acc + __popc(ma & lt);
@@ -261,8 +281,6 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
   const int warp = gid >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= d.na) return;
-  if (lane < 3) d.fix_h[3 * static_cast<size_t>(warp) + lane] = 0ull;   // the H-bond acceptor accumulators of this step
-  if (lane == 3 && d.pe_on) d.pe_fix[warp] = 0ull;
   if (lists_failed(d)) return;
   const int i = warp;
   const SysInfo s = d.sys[d.sys_of[i]];
