@@ -294,12 +294,28 @@ def run_engine(args, rank, world, local_rank):
     n = len(s["type"])
     eng = make_engine(local_rank, s, v)
     stream = torch.cuda.ExternalStream(eng.stream(), device=torch.device("cuda", local_rank))
+    if args.rebuild_evals > 0:
+        eng.set_timing(True)   # eager launches, each phase timed alone
+        ms = []
+        for k in range(args.rebuild_evals):
+            if k > 0:
+                eng.set_capacities(*eng.capacities())   # same capacities: flags every system for a rebuild
+            t0 = eng.phase_times().get("neighbors", 0.0)
+            eng.compute(qeq=True)
+            ms.append(eng.phase_times()["neighbors"] - t0)
+        print(json.dumps({"rebuild_evals": args.rebuild_evals, "neighbors_ms": ms, "atoms": n}), flush=True)
+        eng.close()
+        if dist:
+            dist.destroy_process_group()
+        return
     eng.md_run(max(args.warmup, 3))
     if args.qeq_passes > 0:
         eng.set_qeq(QEQ["swa"], QEQ["swb"], 1e-300, args.qeq_passes)
         r = eng.qeq_solve()
         print(json.dumps({"qeq_passes": int(r["iters"].max()), "atoms": n}), flush=True)
         eng.close()
+        if dist:
+            dist.destroy_process_group()
         return
     clocks = Clocks(local_rank) if rank == 0 else None
     if dist:
@@ -604,6 +620,10 @@ def main():
     ap.add_argument("--qeq-passes", type=int, default=0,
                     help="profiling case: after the warm-up steps, one charge solve of exactly this many matrix passes "
                          "(tolerance 0), then print the counts and exit")
+    ap.add_argument("--rebuild-evals", type=int, default=0,
+                    help="profiling case: evaluations launched one kernel at a time (no graph), each with every "
+                         "system's Verlet rows rebuilt (the first is the initial build); print the neighbor-phase "
+                         "times and exit")
     ap.add_argument("--precision-form", action="store_true",
                     help="run only the precision form (30k carbon, 2013 C force field: NVT at 4000 K, then NVE drift) "
                          "and print its JSON line")

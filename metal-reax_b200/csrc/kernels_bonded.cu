@@ -624,7 +624,7 @@ __device__ inline bool hbond_triple(const DevFF& ff, const HbDonor& dn, int tj, 
 // One warp per hydrogen j (p_hbond = 1): for every donor bond of j, the lanes walk j's acceptor row (p_hbond = 2 atoms,
 // r <= hbond_cut taken again exactly here); each triple is evaluated once. Energy, the gradient of j and the coefficient /
 // gradient of the donor bond are reduced over the warp in fixed order (the donor's share goes to j's slot for the
-// donor to gather); the acceptor's gradient is added to its fixed-point accumulator (zeroed by k_pairs).
+// donor to gather); the acceptor's gradient is added to its fixed-point accumulator (zeroed by k_nbr_check).
 __global__ void __launch_bounds__(256) k_hbond(Dev d, DevFF ff, DevCtl ctl) {
   if (lists_failed(d)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
