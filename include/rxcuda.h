@@ -238,8 +238,8 @@ int rx_md_targets(rx_context* ctx, const double* t_target, const int* active);
  * system of more atoms takes the single-system CG (all SMs on its rows, default 4096; a batch always takes the
  * segmented CG, so a system alone and in a batch give the same bits only below this size); RX_TUNE_OVERLAP: 1 (the
  * default) runs the bonded terms, which need no charge, concurrently with the charge solve, 0 after it;
- * RX_TUNE_CG_BLOCKS_PER_SM: blocks per SM of the single-system CG (default 2, leaving room for the concurrent bonded
- * terms; 0: as many as fit) - unlike the other keys this changes the order of the CG's sums, so the charges' last
+ * RX_TUNE_CG_BLOCKS_PER_SM: threads per SM of the single-system CG in units of 256, as one block per SM (1-4, default
+ * 2, leaving room for the concurrent bonded terms; 0: four) - unlike the other keys this changes the order of the CG's sums, so the charges' last
  * bits (a fixed setting stays bitwise reproducible), and rx_autotune does not touch it. rx_autotune times every
  * candidate shape on the current systems (reps launches each, CUDA events) and keeps the fastest; chosen[5] (may be
  * NULL) receives pairs, bonds, non-bonded, H-bond and per-atom shapes. */

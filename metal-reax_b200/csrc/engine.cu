@@ -778,19 +778,21 @@ struct Context {
     int tpb_pairs = 128, tpb_nb = 128, tpb_hb = 128, tpb_bonds = 128, tpb_atom = 64;
     int lone_grid_min = 4096;
     int overlap = 1;   // bonded chain beside the charge solve
-    // blocks of the single-system CG per SM (0: as many as fit). Two leave half of every SM to the bonded terms that
-    // run beside the solve: on the 24,000-atom water step the solve alone is slower, the step faster. The setting
-    // changes the CG's summation order, so it is one value for every solve of the context.
+    // threads per SM of the single-system CG in units of 256 (1-4; 0: four), launched as one block per SM. Two leave
+    // half of every SM to the bonded terms that run beside the solve: on the 24,000-atom water step the solve alone
+    // is slower, the step faster. One block per SM rather than several smaller ones halves the blocks that meet at
+    // each grid barrier. The setting changes the CG's summation order, so it is one value for every solve of the
+    // context.
     int cg_per_sm = 2;
   } tune;
-  int grid_per_sm = 0, seg_per_sm = 0;
+  int grid_occ[5] = {0, 0, 0, 0, 0}, seg_per_sm = 0;
   void launch_cg(const Dev& d, CgArgs a) {
     if (nsys == 1 && na > tune.lone_grid_min) {   // one large system: all SMs on its rows, block partials in block order
-      const int threads = 256;
-      if (!grid_per_sm) RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k_cg_grid, threads, 0));
-      const int per_sm = tune.cg_per_sm > 0 ? std::min(tune.cg_per_sm, grid_per_sm) : grid_per_sm;
-      int grid = std::max(1, std::min(per_sm * nsm, (na + (threads / 32) - 1) / (threads / 32)));
-      grid = std::min(grid, nsm * 32);
+      const int units = tune.cg_per_sm > 0 ? std::min(tune.cg_per_sm, 4) : 4;
+      const int threads = 256 * units;
+      if (!grid_occ[units]) RXCU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_occ[units], k_cg_grid, threads, 0));
+      if (grid_occ[units] < 1) throw Error(RX_ERR_CUDA, "the single-system CG block does not fit on an SM");
+      int grid = std::max(1, std::min(nsm, (na + (threads / 32) - 1) / (threads / 32)));
       a.begin = 0;
       a.n = na;
       void* args[] = {const_cast<Dev*>(&d), &a};
@@ -1077,7 +1079,7 @@ struct Context {
       case RX_TUNE_ATOM_TPB: check(value == 32 || value == 64 || value == 128); tune.tpb_atom = value; break;
       case RX_TUNE_LONE_GRID_MIN: check(value >= 0); tune.lone_grid_min = value; break;
       case RX_TUNE_OVERLAP: check(value == 0 || value == 1); tune.overlap = value; break;
-      case RX_TUNE_CG_BLOCKS_PER_SM: check(value >= 0 && value <= 32); tune.cg_per_sm = value; break;
+      case RX_TUNE_CG_BLOCKS_PER_SM: check(value >= 0 && value <= 4); tune.cg_per_sm = value; break;
       default: throw Error(RX_ERR_INVALID, "unknown tuning key");
     }
     drop_graph();

@@ -657,7 +657,7 @@ __device__ inline void grid_totals(const double* part, int nblocks, double* tot,
 // order), so the result is bitwise reproducible. Only grid.sync() waits; the kernel is launched cooperatively.
 constexpr double kRefineDrop = 1e-6;
 
-__global__ void __launch_bounds__(256, 4) k_cg_grid(Dev d, CgArgs a) {
+__global__ void __launch_bounds__(1024, 1) k_cg_grid(Dev d, CgArgs a) {
   cg::grid_group g = cg::this_grid();
   __shared__ double sh[32 * 4];
   __shared__ double tot_sh[32 * 4];
