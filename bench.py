@@ -254,18 +254,19 @@ def e2e_run(device, s, v, steps, warmup):
     stream = torch.cuda.ExternalStream(e.stream(), device=torch.device("cuda", device))
     e.set_positions(x)
     e.compute(qeq=True, grad_out=g)
-    kick = 0.5 * DT * ftm2v / m          # per-atom half-kick factor
-    tmp = np.empty_like(vel)
+    # velocity Verlet in its leapfrog form, in place: u is the half-step velocity times dt (the displacement of the
+    # next drift), so a step is one drift and one full kick, u -= 2 k dt g with k the per-atom half-kick factor
+    kick = np.ascontiguousarray(np.repeat(0.5 * DT * ftm2v / m, 3, axis=1))
+    fullkick_dt = 2.0 * kick * DT
+    u = (vel - kick * g) * DT
+    tmp = np.empty_like(u)
 
-    def step():                         # velocity Verlet on the host, in place
-        np.multiply(g, kick, out=tmp)
-        vel.__isub__(tmp)
-        np.multiply(vel, DT, out=tmp)
-        x.__iadd__(tmp)
+    def step():
+        x.__iadd__(u)
         e.set_positions(x)
         e.compute(qeq=True, grad_out=g)
-        np.multiply(g, kick, out=tmp)
-        vel.__isub__(tmp)
+        np.multiply(g, fullkick_dt, out=tmp)
+        u.__isub__(tmp)
 
     for _ in range(warmup):
         step()

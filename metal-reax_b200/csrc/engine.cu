@@ -148,6 +148,8 @@ struct Context {
   DBuf<int> census, status;
   DBuf<long long> counters;
   DBuf<double> energies, virial, vir, vir_nb, vir_h, vir_t;
+  DBuf<double> epart;   // per (system, 256-atom chunk) partial sums of the energy terms and virial components
+  int echunks = 1;
   // QEq
   DBuf<double2> cg_x, cg_b, cg_r, cg_d, cg_p, cg_q;
   DBuf<float2> cg_df;
@@ -614,6 +616,12 @@ struct Context {
     sys_flag.ensure(static_cast<size_t>(nsys)); cg_nref.ensure(1); cg_brk.ensure(static_cast<size_t>(nsys));
     energies.ensure(static_cast<size_t>(nsys) * kTerms);
     virial.ensure(static_cast<size_t>(nsys) * kVir);
+    {
+      int maxn = 1;
+      for (const auto& si : hsys) maxn = std::max(maxn, si.natoms);
+      echunks = (maxn + 255) / 256;
+      epart.ensure(static_cast<size_t>(nsys) * echunks * (kTerms + kVir));
+    }
     vir.ensure(n * kVir);
     vir_nb.ensure(n * kVir); vir_h.ensure(n * kVir); vir_t.ensure(n * kVir);
     fown_h.ensure(n); fown_t.ensure(n); fix_h.ensure(3 * n); pe_fix.ensure(n);
@@ -1012,8 +1020,10 @@ struct Context {
   bool forces_valid = false;   // the gradient buffer holds the forces of the current positions and systems
   void energy_sums() {
     have_virial = true;
-    ++launches;
-    k_energy_sum<<<dim3(nsys, kTerms + kVir), 256, 0, stream>>>(dev(), energies.p, virial.p);
+    launches += 2;
+    const Dev d = dev();
+    k_energy_part<<<dim3(echunks, nsys), 256, 0, stream>>>(d, epart.p, echunks);
+    k_energy_final<<<nsys, 32, 0, stream>>>(d, epart.p, echunks, energies.p, virial.p);
   }
 
   // ------------------------------------------------------------------ autotuning

@@ -58,7 +58,8 @@ __global__ void k_qeq_prepare(Dev d, DevFF ff, CgArgs a, const double* s_hist, c
 __global__ void k_qeq_prepare_given(Dev d, DevFF ff, CgArgs a, const double* b, const double* x0);
 __global__ void k_qeq_history(Dev d, const double2* x, double* s_hist, double* t_hist, int strict);
 __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y);
-__global__ void k_energy_sum(Dev d, double* out, double* out_vir);
+__global__ void k_energy_part(Dev d, double* part, int nchunk);
+__global__ void k_energy_final(Dev d, const double* part, int nchunk, double* out, double* out_vir);
 
 __global__ void k_bonds(Dev d, DevFF ff, DevCtl ctl);
 __global__ void k_bond_sym(Dev d);

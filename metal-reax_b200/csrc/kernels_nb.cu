@@ -1071,32 +1071,55 @@ __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y) {
 }
 
 // ------------------------------------------------------------------------------------------------ energy sums
-// Per system, per term: fixed-order sum over the system's atoms (one block per system and term). Terms kTerms ..
-// kTerms + kVir - 1 are the virial components, written to out_vir.
-__global__ void k_energy_sum(Dev d, double* out, double* out_vir) {
-  const int sidx = blockIdx.x, t = blockIdx.y;
-  const SysInfo s = d.sys[sidx];
-  __shared__ double sh[256];
-  double v = 0.0;
-  if (t < kTerms) {
-    for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) v += d.eatom[static_cast<size_t>(s.begin + r) * kTerms + t];
-  } else {
-    const int c = t - kTerms;
-    for (int r = threadIdx.x; r < s.natoms; r += blockDim.x) {
-      const size_t k = static_cast<size_t>(s.begin + r) * kVir + c;
-      v += ((d.vir[k] + d.vir_h[k]) + d.vir_t[k]) + d.vir_nb[k];
+// Per system: fixed-order sums of the 13 energy terms and the 6 virial components over the system's atoms, in two
+// passes. k_energy_part: one block per (256-atom chunk, system), a thread per atom, each of the 19 quantities summed by
+// a fixed shuffle tree per warp and then over the warps in order; k_energy_final: per system and quantity, the chunk
+// partials in chunk order. Chunks start at the system's first atom, so a system's sums are the same alone or in a
+// batch.
+constexpr int kESum = kTerms + kVir;
+__global__ void __launch_bounds__(256) k_energy_part(Dev d, double* part, int nchunk) {
+  const int c = blockIdx.x, sidx = blockIdx.y;
+  const SysInfo& s = d.sys[sidx];
+  if (c * 256 >= s.natoms) return;
+  __shared__ double sh[8][kESum];
+  const int r = c * 256 + threadIdx.x;
+  double v[kESum];
+  if (r < s.natoms) {
+    const size_t a = static_cast<size_t>(s.begin + r);
+#pragma unroll
+    for (int t = 0; t < kTerms; ++t) v[t] = d.eatom[a * kTerms + t];
+#pragma unroll
+    for (int k = 0; k < kVir; ++k) {
+      const size_t q = a * kVir + k;
+      v[kTerms + k] = ((d.vir[q] + d.vir_h[q]) + d.vir_t[q]) + d.vir_nb[q];
     }
+  } else {
+#pragma unroll
+    for (int t = 0; t < kESum; ++t) v[t] = 0.0;
   }
-  sh[threadIdx.x] = v;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < kESum; ++t) {
+    double x = v[t];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[w][t] = x;
+  }
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
+  if (threadIdx.x < kESum) {
+    double x = 0.0;
+    for (int k = 0; k < 8; ++k) x += sh[k][threadIdx.x];
+    part[(static_cast<size_t>(sidx) * nchunk + c) * kESum + threadIdx.x] = x;
   }
-  if (threadIdx.x == 0) {
-    if (t < kTerms) out[sidx * kTerms + t] = sh[0];
-    else out_vir[sidx * kVir + (t - kTerms)] = sh[0];
-  }
+}
+
+__global__ void k_energy_final(Dev d, const double* part, int nchunk, double* out, double* out_vir) {
+  const int sidx = blockIdx.x, t = threadIdx.x;
+  if (t >= kESum) return;
+  const int nc = (d.sys[sidx].natoms + 255) / 256;
+  double x = 0.0;
+  for (int c = 0; c < nc; ++c) x += part[(static_cast<size_t>(sidx) * nchunk + c) * kESum + t];
+  if (t < kTerms) out[sidx * kTerms + t] = x;
+  else out_vir[sidx * kVir + (t - kTerms)] = x;
 }
 
 }  // namespace rx
