@@ -497,3 +497,33 @@ def test_pinned_arrays_give_the_same_bits(engine):
     out = engine.compute(grad_out=g)
     assert np.array_equal(out["e"], ref["e"])
     assert np.array_equal(g, ref["grad"])
+
+
+def test_cg_block_size_changes_only_rounding():
+    """The single-system CG's threads per SM (RX_TUNE_CG_BLOCKS_PER_SM, one block per SM of 256 x value threads)
+    changes the order of its sums and nothing else: at tolerance 1e-12 every size gives the same charges to 1e-10 e,
+    each size is bitwise reproducible, and a size outside 0-4 is rejected."""
+    import rxcuda
+    import systems
+    s = systems.water_box(12)   # 5,184 atoms: above the lone-system size, so the single-system CG
+    e = rxcuda.Engine(0)
+    try:
+        e.set_forcefield(ffield_text())
+        e.set_control()
+        e.set_qeq(0.0, 10.0, 1e-12, 400)
+        e.set_systems([s])
+        q = {}
+        for units in (2, 1, 3, 4, 0, 2):
+            e.set_tuning("cg_blocks_per_sm", units)
+            e.qeq_reset()
+            e.qeq_solve()
+            got = e.get_charges()
+            if units in q:
+                assert np.array_equal(got, q[units]), units
+            q[units] = got
+        for units, qq in q.items():
+            assert np.abs(qq - q[2]).max() <= 1e-10, units
+        with pytest.raises(rxcuda.RxError):
+            e.set_tuning("cg_blocks_per_sm", 5)
+    finally:
+        e.close()
