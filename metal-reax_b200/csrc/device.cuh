@@ -163,7 +163,7 @@ struct Dev {
   AtomQ* aq;
   double4* fown;         // gradient on the atom itself (xyz), own CdDelta (w) (k_bonded_atom)
   double4* fown_h;       // H-bond: gradient on the hydrogen itself
-  unsigned long long* fix_h;   // H-bond: gradient on the acceptor, 3 per atom, fixed point (2^32 units)
+  unsigned long long* fix_h;   // scattered gradient shares (H-bond acceptors, non-bonded partners), 3 per atom, fixed point (2^32 units)
   double4* fown_t;       // torsion: gradient on the central atom (xyz), own CdDelta (w)
   double* cdtot;
   double* W;

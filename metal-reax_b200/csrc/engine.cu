@@ -885,7 +885,10 @@ struct Context {
   void launch_nonbonded(const Dev& d) {
     tic(5, "nonbonded");
     ++launches;
-    k_nonbonded<<<blocks(static_cast<long long>(na) * 32, tune.tpb_nb), tune.tpb_nb, 0, stream>>>(d, dff);
+    // each pair once (the partner's share through the fixed-point accumulator), except when the per-atom split of
+    // energies and virials is wanted
+    if (pe_on) k_nonbonded<<<blocks(static_cast<long long>(na) * 32, tune.tpb_nb), tune.tpb_nb, 0, stream>>>(d, dff);
+    else k_nonbonded_half<<<blocks(static_cast<long long>(na) * 32, tune.tpb_nb), tune.tpb_nb, 0, stream>>>(d, dff);
     if (acks2_on) {
       ++launches;
       k_acks2<<<blocks(static_cast<long long>(na) * 32, 128), 128, 0, stream>>>(d, dff, s_kin.p);

@@ -51,6 +51,7 @@ __global__ void k_rebuild_flag(Dev d, cudaGraphConditionalHandle h);
 __global__ void k_neighbors(Dev d, DevFF ff);
 __global__ void k_pairs(Dev d, DevFF ff, QeqParams qp);
 __global__ void k_nonbonded(Dev d, DevFF ff);
+__global__ void k_nonbonded_half(Dev d, DevFF ff);
 __global__ void k_acks2(Dev d, DevFF ff, const double* s_kin);
 __global__ void k_cg_grid(Dev d, CgArgs a);
 __global__ void k_cg_seg(Dev d, CgArgs a);

@@ -340,6 +340,68 @@ __global__ void __launch_bounds__(256) k_pairs(Dev d, DevFF ff, QeqParams qp) {
 }
 
 // ------------------------------------------------------------------------------------------------ non-bonded
+// The pair terms of one non-bonded entry at separation dvd (terms::nonbonded_pair, terms.hpp:282-323): returns CE with
+// gradient -CE dvd on i and +CE dvd on the partner, and the pair's van der Waals and Coulomb energies.
+__device__ __forceinline__ float nb_pair_terms(const DevFF& ff, int ti, int tj, float qi, float qj, const double* dvd,
+                                               float p_vdW1, float p_vdW1i, float swa, float inv_dd, float& e_vdW,
+                                               float& e_ele) {
+  // the exact cut-off test was taken in FP64 when the row was filtered; the pair terms run in FP32, division-free:
+  // 1/r from the reciprocal square root, reciprocals of the type-pair constants from the table, exp(a) as the square
+  // of exp(a/2), and the Coulomb shielding through the reciprocal cube root z = (r^3 + gamma^-3)^(-1/3), whose cube
+  // is 1/(r^3 + gamma^-3)
+  const float r2f = static_cast<float>(dvd[0] * dvd[0] + dvd[1] * dvd[1] + dvd[2] * dvd[2]);
+  const float inv_r = rsqrtf(r2f);
+  const float r = r2f * inv_r;
+  const float* pp = ff.nbf + (static_cast<size_t>(ti) * ff.nt + tj) * 12;
+  float Tap, dTap;
+  {   // taper_stable (include/reaxmetal/terms.hpp:268-272) in t = (r - swa)/(swb - swa)
+    const float t = (r - swa) * inv_dd, t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
+    Tap = 1.f - t4 * (35.f - 84.f * t + 70.f * t2 - 20.f * t3);
+    dTap = (t3 * (-140.f + 420.f * t - 420.f * t2 + 140.f * t3)) * (inv_dd * inv_r);
+  }
+  const float alpha = pp[0], D = pp[1], inv_rvdw = pp[10];
+  float CEvd;
+  e_vdW = 0.f;
+  if (ff.vdw_type == 1 || ff.vdw_type == 3) {
+    const float powr_vdW1 = exp2f(p_vdW1 * __log2f(r));   // r^p and (..)^(1/p) through the fast base-2 pair
+    const float sum = powr_vdW1 + pp[3];
+    const float fn13 = exp2f(p_vdW1i * __log2f(sum));
+    const float exp2 = __expf(0.5f * alpha * (1.f - fn13 * inv_rvdw));
+    const float exp1 = exp2 * exp2;
+    const float evd = D * (exp1 - 2.f * exp2);
+    e_vdW += Tap * evd;
+    // (sum)^(1/p - 1) r^(p - 2) = fn13 / sum * powr / r^2
+    const float dfn13 = __fdividef(fn13, sum) * (powr_vdW1 * inv_r * inv_r);
+    CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * dfn13;
+  } else {
+    const float exp2 = __expf(0.5f * alpha * (1.f - r * inv_rvdw));
+    const float exp1 = exp2 * exp2;
+    const float evd = D * (exp1 - 2.f * exp2);
+    e_vdW += Tap * evd;
+    CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * inv_r;
+  }
+  if (ff.vdw_type == 2 || ff.vdw_type == 3) {
+    const float ecore = pp[4], acore = pp[5], inv_rcore = pp[11];
+    const float e_core = ecore * __expf(acore * (1.f - r * inv_rcore));
+    e_vdW += Tap * e_core;
+    const float de_core = -(acore * inv_rcore) * e_core;
+    CEvd += dTap * e_core + Tap * de_core * inv_r;
+    if (ff.lg) {
+      const float r4 = r2f * r2f, r5 = r4 * r, r6 = r4 * r2f, re6 = pp[9];
+      const float inv6 = __fdividef(1.f, r6 + re6);
+      const float e_lg = -pp[8] * inv6;
+      e_vdW += Tap * e_lg;
+      const float de_lg = -6.f * e_lg * r5 * inv6;
+      CEvd += dTap * e_lg + Tap * de_lg * inv_r;
+    }
+  }
+  const float z = rcbrtf(r2f * r + pp[7]);
+  const float cq = 332.06371f * qi * qj;
+  e_ele = cq * (Tap * z);
+  const float CEclmb = cq * (dTap - Tap * r * (z * z * z)) * z;
+  return CEvd + CEclmb;
+}
+
 // One warp per atom over its full row (FP32 pair arithmetic, FP64 accumulation). The gradient of atom i collects
 // -CE * dvec from every entry of its own row, so no write ever touches another atom. Energies use the reference's
 // counted pairs (owner-computes rule, classify_nonbonded_entry, src/neighbor/neighbor.cpp:295-310): an entry counts
@@ -369,62 +431,9 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     const int sidx = static_cast<int>(code >> d.abits);
     double dvd[3];
     pair_dvec_x(d, s, i, j, sidx, xi4, d.x[j], dvd);
-    // the exact cut-off test was taken in FP64 when the row was filtered; the pair terms run in FP32, division-free:
-    // 1/r from the reciprocal square root, reciprocals of the type-pair constants from the table, exp(a) as the square
-    // of exp(a/2), and the Coulomb shielding through the reciprocal cube root z = (r^3 + gamma^-3)^(-1/3), whose cube
-    // is 1/(r^3 + gamma^-3)
-    const float r2f = static_cast<float>(dvd[0] * dvd[0] + dvd[1] * dvd[1] + dvd[2] * dvd[2]);
-    const float inv_r = rsqrtf(r2f);
-    const float r = r2f * inv_r;
     const int tj = d.type[j];
-    const float* pp = ff.nbf + (static_cast<size_t>(ti) * ff.nt + tj) * 12;
-    float Tap, dTap;
-    {   // taper_stable (include/reaxmetal/terms.hpp:268-272) in t = (r - swa)/(swb - swa)
-      const float t = (r - swa) * inv_dd, t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
-      Tap = 1.f - t4 * (35.f - 84.f * t + 70.f * t2 - 20.f * t3);
-      dTap = (t3 * (-140.f + 420.f * t - 420.f * t2 + 140.f * t3)) * (inv_dd * inv_r);
-    }
-    const float alpha = pp[0], D = pp[1], inv_rvdw = pp[10];
-    float e_vdW = 0.f, CEvd;
-    if (ff.vdw_type == 1 || ff.vdw_type == 3) {
-      const float powr_vdW1 = exp2f(p_vdW1 * __log2f(r));   // r^p and (..)^(1/p) through the fast base-2 pair
-      const float sum = powr_vdW1 + pp[3];
-      const float fn13 = exp2f(p_vdW1i * __log2f(sum));
-      const float exp2 = __expf(0.5f * alpha * (1.f - fn13 * inv_rvdw));
-      const float exp1 = exp2 * exp2;
-      const float evd = D * (exp1 - 2.f * exp2);
-      e_vdW += Tap * evd;
-      // (sum)^(1/p - 1) r^(p - 2) = fn13 / sum * powr / r^2
-      const float dfn13 = __fdividef(fn13, sum) * (powr_vdW1 * inv_r * inv_r);
-      CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * dfn13;
-    } else {
-      const float exp2 = __expf(0.5f * alpha * (1.f - r * inv_rvdw));
-      const float exp1 = exp2 * exp2;
-      const float evd = D * (exp1 - 2.f * exp2);
-      e_vdW += Tap * evd;
-      CEvd = dTap * evd - Tap * D * (alpha * inv_rvdw) * (exp1 - exp2) * inv_r;
-    }
-    if (ff.vdw_type == 2 || ff.vdw_type == 3) {
-      const float ecore = pp[4], acore = pp[5], inv_rcore = pp[11];
-      const float e_core = ecore * __expf(acore * (1.f - r * inv_rcore));
-      e_vdW += Tap * e_core;
-      const float de_core = -(acore * inv_rcore) * e_core;
-      CEvd += dTap * e_core + Tap * de_core * inv_r;
-      if (ff.lg) {
-        const float r4 = r2f * r2f, r5 = r4 * r, r6 = r4 * r2f, re6 = pp[9];
-        const float inv6 = __fdividef(1.f, r6 + re6);
-        const float e_lg = -pp[8] * inv6;
-        e_vdW += Tap * e_lg;
-        const float de_lg = -6.f * e_lg * r5 * inv6;
-        CEvd += dTap * e_lg + Tap * de_lg * inv_r;
-      }
-    }
-    const float qj = static_cast<float>(d.q[j]);
-    const float z = rcbrtf(r2f * r + pp[7]);
-    const float cq = 332.06371f * qi * qj;
-    const float e_ele = cq * (Tap * z);
-    const float CEclmb = cq * (dTap - Tap * r * (z * z * z)) * z;
-    const float CE = CEvd + CEclmb;
+    float e_vdW, e_ele;
+    const float CE = nb_pair_terms(ff, ti, tj, qi, static_cast<float>(d.q[j]), dvd, p_vdW1, p_vdW1i, swa, inv_dd, e_vdW, e_ele);
     const float dx = static_cast<float>(dvd[0]), dy = static_cast<float>(dvd[1]), dz = static_cast<float>(dvd[2]);
     gx -= static_cast<double>(CE * dx);
     gy -= static_cast<double>(CE * dy);
@@ -470,6 +479,113 @@ __global__ void k_nonbonded(Dev d, DevFF ff) {
     const double chi = ff.sb[ti * SB_N + SB_CHI], eta = ff.sb[ti * SB_N + SB_ETA], qd = d.q[i];
     d.eatom[static_cast<size_t>(i) * kTerms + E_POL] = 23.02 * (chi * qd + (eta / 2.) * (qd * qd));
     if (d.pe_on) pe_add(d, i, ehalf + 23.02 * (chi * qd + (eta / 2.) * (qd * qd)));
+    d.census[4 * d.na + i] = counted;
+  }
+}
+
+// Each non-bonded pair once: the same terms as k_nonbonded over the counted entries of every row only (the
+// owner-computes rule above picks exactly one entry of each pair), with the partner's gradient +CE dv added to its
+// fixed-point accumulator (2^32 units: integer additions give the same sum in any order, so the result is
+// deterministic). The counted entries of a row are gathered into a per-warp queue in row order, so every lane of a
+// batch of 32 has a pair to compute. The pair virial goes whole to the owner; the per-atom split of energies and
+// virials (RX_COMPUTE_PERATOM) takes k_nonbonded instead.
+__global__ void __launch_bounds__(256) k_nonbonded_half(Dev d, DevFF ff) {
+  if (lists_failed(d)) return;
+  __shared__ unsigned queue[8][64];
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  if (warp >= d.na) return;
+  const int i = warp;
+  const SysInfo s = d.sys[d.sys_of[i]];
+  const int ti = d.type[i];
+  const int cnt = min(d.nbr_cnt[i], d.ncap);
+  const float p_vdW1 = static_cast<float>(ff.gp[28]), p_vdW1i = 1.f / p_vdW1;
+  const float swa = static_cast<float>(ff.nonb_low), inv_dd = static_cast<float>(1.0 / (ff.nonb_cut - ff.nonb_low));
+  const float qi = static_cast<float>(d.q[i]);
+  const long long tag_i = d.tag[i];
+  const int center = (d.S * d.S * d.S - 1) / 2;
+  const unsigned lt = (1u << lane) - 1u;
+  double gx = 0, gy = 0, gz = 0, ev = 0, ee = 0;
+  float v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;   // pair virials (lane partials)
+  int counted = 0;
+  const double4 xi4 = d.x[i];
+  auto pair = [&](unsigned code) {
+    const int j = static_cast<int>(code & d.amask);
+    const int sidx = static_cast<int>(code >> d.abits);
+    double dvd[3];
+    pair_dvec_x(d, s, i, j, sidx, xi4, d.x[j], dvd);
+    float e_vdW, e_ele;
+    const float CE = nb_pair_terms(ff, ti, d.type[j], qi, static_cast<float>(d.q[j]), dvd, p_vdW1, p_vdW1i, swa, inv_dd,
+                                   e_vdW, e_ele);
+    const float dx = static_cast<float>(dvd[0]), dy = static_cast<float>(dvd[1]), dz = static_cast<float>(dvd[2]);
+    const float fx = CE * dx, fy = CE * dy, fz = CE * dz;
+    gx -= static_cast<double>(fx);
+    gy -= static_cast<double>(fy);
+    gz -= static_cast<double>(fz);
+    fix_add(d.fix_h + 3 * static_cast<size_t>(j), static_cast<double>(fx));
+    fix_add(d.fix_h + 3 * static_cast<size_t>(j) + 1, static_cast<double>(fy));
+    fix_add(d.fix_h + 3 * static_cast<size_t>(j) + 2, static_cast<double>(fz));
+    const float c = -CE;   // the pair virial -CE dv (x) dv, whole
+    v0 += c * dx * dx; v1 += c * dy * dy; v2 += c * dz * dz;
+    v3 += c * dx * dy; v4 += c * dx * dz; v5 += c * dy * dz;
+    ev += static_cast<double>(e_vdW);
+    ee += static_cast<double>(e_ele);
+    ++counted;
+  };
+  int qn = 0;   // entries waiting in this warp's queue (warp-uniform)
+  for (int base = 0; base < cnt; base += 32) {
+    const int e = base + lane;
+    bool own = false;
+    unsigned code = 0;
+    if (e < cnt) {
+      code = d.nbr[static_cast<size_t>(i) * d.ncap + e];
+      const int j = static_cast<int>(code & d.amask);
+      const int sidx = static_cast<int>(code >> d.abits);
+      if (sidx == center) {
+        own = j > i;
+      } else {
+        const long long tag_j = d.tag[j];
+        if (tag_i < tag_j) {
+          own = true;
+        } else if (tag_i == tag_j) {   // an image of i itself: the positive direction
+          double dvd[3];
+          pair_dvec_x(d, s, i, j, sidx, xi4, d.x[j], dvd);
+          const double SMALL = 1e-4;
+          if (dvd[2] > SMALL) own = true;
+          else if (fabs(dvd[2]) < SMALL) {
+            if (dvd[1] > SMALL) own = true;
+            else if (fabs(dvd[1]) < SMALL && dvd[0] > SMALL) own = true;
+          }
+        }
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, own);
+    if (own) queue[wb][qn + __popc(m & lt)] = code;
+    qn += __popc(m);
+    __syncwarp();
+    if (qn >= 32) {   // a full batch: one pair per lane; the rest moves to the front of the queue
+      const unsigned mine = queue[wb][lane];
+      const unsigned rest = lane + 32 < qn ? queue[wb][lane + 32] : 0u;
+      __syncwarp();
+      if (lane + 32 < qn) queue[wb][lane] = rest;
+      __syncwarp();
+      qn -= 32;
+      pair(mine);
+    }
+  }
+  if (lane < qn) pair(queue[wb][lane]);
+  gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); ev = warp_sum(ev); ee = warp_sum(ee);
+  const double w0 = warp_sum(static_cast<double>(v0)), w1 = warp_sum(static_cast<double>(v1)), w2 = warp_sum(static_cast<double>(v2));
+  const double w3 = warp_sum(static_cast<double>(v3)), w4 = warp_sum(static_cast<double>(v4)), w5 = warp_sum(static_cast<double>(v5));
+  for (int o = 16; o > 0; o >>= 1) counted += __shfl_xor_sync(0xffffffffu, counted, o);
+  if (lane == 0) {
+    d.fnb[i] = make_double4(gx, gy, gz, 0.0);
+    double* vi = d.vir_nb + static_cast<size_t>(i) * kVir;
+    vi[0] = w0; vi[1] = w1; vi[2] = w2; vi[3] = w3; vi[4] = w4; vi[5] = w5;
+    d.eatom[static_cast<size_t>(i) * kTerms + E_VDW] = ev;
+    d.eatom[static_cast<size_t>(i) * kTerms + E_ELE] = ee;
+    const double chi = ff.sb[ti * SB_N + SB_CHI], eta = ff.sb[ti * SB_N + SB_ETA], qd = d.q[i];
+    d.eatom[static_cast<size_t>(i) * kTerms + E_POL] = 23.02 * (chi * qd + (eta / 2.) * (qd * qd));
     d.census[4 * d.na + i] = counted;
   }
 }
