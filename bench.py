@@ -136,8 +136,10 @@ def phase_impl_bytes(name, N, E, D, I, R=1, EV=None):
     }.get(name, phase_model_bytes(name, N, E // 2, D, I))
 
 
-PHASE_KERNEL = {"neighbors": "k_neighbors", "qeq": "k_cg_grid", "bond_orders": "k_bonds", "bonded_terms": "k_bonded_atom",
-                "torsion": "k_torsion", "nonbonded": "k_nonbonded", "gather": "k_fold", "force_final": "k_force_final"}
+# the dominant kernel of each timed phase (the neighbor phase's every-step kernel is the row filter; the Verlet build
+# runs only on rebuild steps)
+PHASE_KERNEL = {"neighbors": "k_pairs", "qeq": "k_cg_grid", "bond_orders": "k_bonds", "bonded_terms": "k_bonded_atom",
+                "torsion": "k_torsion", "nonbonded": "k_nonbonded_half", "gather": "k_fold", "force_final": "k_force_final"}
 
 
 def profiled_traffic(kernel, passes):
