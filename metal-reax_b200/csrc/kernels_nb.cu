@@ -1189,8 +1189,8 @@ __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y) {
 // ------------------------------------------------------------------------------------------------ energy sums
 // Per system: fixed-order sums of the 13 energy terms and the 6 virial components over the system's atoms, in two
 // passes. k_energy_part: one block per (256-atom chunk, system), a thread per atom, each of the 19 quantities summed by
-// a fixed shuffle tree per warp and then over the warps in order; k_energy_final: per system and quantity, the chunk
-// partials in chunk order. Chunks start at the system's first atom, so a system's sums are the same alone or in a
+// a fixed shuffle tree per warp and then over the warps in order; k_energy_final: per system, a warp per quantity over
+// the chunk partials (lane-strided, then a fixed shuffle tree). Chunks start at the system's first atom, so a system's sums are the same alone or in a
 // batch.
 constexpr int kESum = kTerms + kVir;
 __global__ void __launch_bounds__(256) k_energy_part(Dev d, double* part, int nchunk) {
@@ -1229,13 +1229,16 @@ __global__ void __launch_bounds__(256) k_energy_part(Dev d, double* part, int nc
 }
 
 __global__ void k_energy_final(Dev d, const double* part, int nchunk, double* out, double* out_vir) {
-  const int sidx = blockIdx.x, t = threadIdx.x;
+  const int sidx = blockIdx.x, t = threadIdx.x >> 5, lane = threadIdx.x & 31;   // a warp per quantity
   if (t >= kESum) return;
   const int nc = (d.sys[sidx].natoms + 255) / 256;
   double x = 0.0;
-  for (int c = 0; c < nc; ++c) x += part[(static_cast<size_t>(sidx) * nchunk + c) * kESum + t];
-  if (t < kTerms) out[sidx * kTerms + t] = x;
-  else out_vir[sidx * kVir + (t - kTerms)] = x;
+  for (int c = lane; c < nc; c += 32) x += part[(static_cast<size_t>(sidx) * nchunk + c) * kESum + t];
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  if (lane == 0) {
+    if (t < kTerms) out[sidx * kTerms + t] = x;
+    else out_vir[sidx * kVir + (t - kTerms)] = x;
+  }
 }
 
 }  // namespace rx
