@@ -258,17 +258,17 @@ def e2e_run(device, s, v, steps, warmup):
     e.compute(qeq=True, grad_out=g)
     # velocity Verlet in its leapfrog form, in place: u is the half-step velocity times dt (the displacement of the
     # next drift), so a step is one drift and one full kick, u -= 2 k dt g with k the per-atom half-kick factor
+    # (host arithmetic through torch's multithreaded CPU kernels on views of the same arrays)
     kick = np.ascontiguousarray(np.repeat(0.5 * DT * ftm2v / m, 3, axis=1))
-    fullkick_dt = 2.0 * kick * DT
-    u = (vel - kick * g) * DT
-    tmp = np.empty_like(u)
+    fullkick_dt = torch.from_numpy(2.0 * kick * DT)
+    u = torch.from_numpy((vel - kick * g) * DT)
+    xt, gt = torch.from_numpy(x), torch.from_numpy(g)
 
     def step():
-        x.__iadd__(u)
+        xt.add_(u)
         e.set_positions(x)
         e.compute(qeq=True, grad_out=g)
-        np.multiply(g, fullkick_dt, out=tmp)
-        u.__isub__(tmp)
+        u.addcmul_(gt, fullkick_dt, value=-1.0)
 
     for _ in range(warmup):
         step()
