@@ -527,3 +527,20 @@ def test_cg_block_size_changes_only_rounding():
             e.set_tuning("cg_blocks_per_sm", 5)
     finally:
         e.close()
+
+
+def test_half_pair_nonbonded_matches_full_rows(engine):
+    """The step's non-bonded kernel computes each pair once and hands the partner its share through the fixed-point
+    accumulator; the full-row kernel (taken for per-atom tallies) computes every pair from both ends. Same pairs and the
+    same FP32 terms, so energies agree to summation order and the census is identical; the gradients agree to FP32
+    rounding (1e-6 of the largest component), because the two ends of a pair round the charge product and the type-pair
+    constants in their own order, so the full-row kernel's two shares of a pair differ in their last bits."""
+    for s in small_systems()[:3] + [__import__("systems").water_box(8)]:
+        q = fixed_charges(s)
+        engine.set_systems([s])
+        engine.set_charges(q)
+        half = engine.compute(census=True)
+        full = engine.compute(census=True, peratom=True)
+        assert np.abs(half["e"] - full["e"]).max() <= 1e-9 * max(1.0, np.abs(full["e"]).max()), s.get("name")
+        assert np.abs(half["grad"] - full["grad"]).max() <= 1e-6 * max(1.0, np.abs(full["grad"]).max()), s.get("name")
+        assert np.array_equal(half["census"], full["census"]), s.get("name")
