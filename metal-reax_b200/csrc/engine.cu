@@ -82,6 +82,7 @@ struct Context {
   cudaStream_t side = nullptr, side_h = nullptr, side_t = nullptr;
   cudaStream_t side_c = nullptr;   // capture of the rebuild kernels into their graph conditional
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join_h = nullptr, ev_join_t = nullptr;
+  cudaEvent_t ev_tail = nullptr, ev_tail_done = nullptr;   // rx_compute: the gradient's copy beside the energy sums
   // one captured MD step (replayed for every step of rx_md_run); dropped whenever a buffer or a parameter it holds
   // changes
   cudaGraphExec_t md_graph = nullptr;
@@ -226,7 +227,8 @@ struct Context {
     RXCU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     RXCU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     for (cudaStream_t* st : {&side, &side_h, &side_t, &side_c}) RXCU(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
-    for (cudaEvent_t* ev : {&ev_fork, &ev_join, &ev_fork2, &ev_join_h, &ev_join_t}) RXCU(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    for (cudaEvent_t* ev : {&ev_fork, &ev_join, &ev_fork2, &ev_join_h, &ev_join_t, &ev_tail, &ev_tail_done})
+      RXCU(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
     status.ensure(kStatusWords);
     counters.ensure(8);
     set_qeq(0.0, 10.0, 1e-6, 200, 0);
@@ -238,7 +240,7 @@ struct Context {
     if (pin_e) cudaFreeHost(pin_e);
     drop_graph();
     for (auto& p : phases) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
-    for (cudaEvent_t ev : {ev_fork, ev_join, ev_fork2, ev_join_h, ev_join_t})
+    for (cudaEvent_t ev : {ev_fork, ev_join, ev_fork2, ev_join_h, ev_join_t, ev_tail, ev_tail_done})
       if (ev) cudaEventDestroy(ev);
     for (cudaStream_t st : {side, side_h, side_t, side_c})
       if (st) cudaStreamDestroy(st);
@@ -1204,16 +1206,28 @@ struct Context {
     if (g_pinned) xyz3.ensure(3 * static_cast<size_t>(na));
     double* eh = nullptr;
     evaluate_with((flags & RX_COMPUTE_QEQ) != 0, [&] {
+      // the gradient's layout change and copy run on `side` (idle once the evaluation has joined) while `stream` sums
+      // the energies and copies them; `stream` waits for the copy before the status word is read
+      const bool fork = g || g_pinned;
+      cudaStream_t gs = fork ? side : stream;
+      if (fork) {
+        RXCU(cudaEventRecord(ev_tail, stream));
+        RXCU(cudaStreamWaitEvent(side, ev_tail, 0));
+      }
+      if (g) RXCU(cudaMemcpyAsync(g, grad.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, gs));
+      if (g_pinned) {
+        ++launches;
+        k_pack3<<<blocks(na, 256), 256, 0, gs>>>(na, grad.p, xyz3.p);
+        RXCU(cudaMemcpyAsync(g_out, xyz3.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, gs));
+      }
       energy_sums();
       if (e_out) {
         eh = energy_stage(static_cast<size_t>(kTerms) * nsys);
         RXCU(cudaMemcpyAsync(eh, energies.p, sizeof(double) * kTerms * nsys, cudaMemcpyDeviceToHost, stream));
       }
-      if (g) RXCU(cudaMemcpyAsync(g, grad.p, sizeof(double4) * na, cudaMemcpyDeviceToHost, stream));
-      if (g_pinned) {
-        ++launches;
-        k_pack3<<<blocks(na, 256), 256, 0, stream>>>(na, grad.p, xyz3.p);
-        RXCU(cudaMemcpyAsync(g_out, xyz3.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, stream));
+      if (fork) {
+        RXCU(cudaEventRecord(ev_tail_done, side));
+        RXCU(cudaStreamWaitEvent(stream, ev_tail_done, 0));
       }
     });
     have_peratom = pe_on != 0;
