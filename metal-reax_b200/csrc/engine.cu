@@ -1069,7 +1069,10 @@ struct Context {
     };
     pick(&tune.tpb_pairs, {64, 128, 256}, [&](int t) { k_pairs<<<blocks(nw, t), t, 0, stream>>>(d, dff, qp); });
     pick(&tune.tpb_bonds, {64, 128, 256}, [&](int t) { k_bonds<<<blocks(nw, t), t, 0, stream>>>(d, dff, ctl); });
-    pick(&tune.tpb_nb, {64, 128, 256}, [&](int t) { k_nonbonded<<<blocks(nw, t), t, 0, stream>>>(d, dff); });
+    pick(&tune.tpb_nb, {64, 128, 256}, [&](int t) {   // the non-bonded kernel the evaluations take
+      if (pe_on) k_nonbonded<<<blocks(nw, t), t, 0, stream>>>(d, dff);
+      else k_nonbonded_half<<<blocks(nw, t), t, 0, stream>>>(d, dff);
+    });
     pick(&tune.tpb_hb, {64, 128, 256}, [&](int t) { k_hbond<<<blocks(nw, t), t, 0, stream>>>(d, dff, ctl); });
     pick(&tune.tpb_atom, {32, 64, 128}, [&](int t) {
       k_bonded_atom<<<blocks(na, t), t, 0, stream>>>(d, dff, ctl);
