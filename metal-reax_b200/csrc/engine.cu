@@ -1027,7 +1027,7 @@ struct Context {
     have_virial = true;
     launches += 2;
     const Dev d = dev();
-    k_energy_part<<<dim3(echunks, nsys), 256, 0, stream>>>(d, epart.p, echunks);
+    k_energy_part<<<dim3(nsys, echunks), 256, 0, stream>>>(d, epart.p, echunks);
     k_energy_final<<<nsys, 32 * (kTerms + kVir), 0, stream>>>(d, epart.p, echunks, energies.p, virial.p);
   }
 

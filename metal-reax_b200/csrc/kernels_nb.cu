@@ -1188,13 +1188,13 @@ __global__ void k_qeq_matvec(Dev d, DevFF ff, const double2* v, double2* y) {
 
 // ------------------------------------------------------------------------------------------------ energy sums
 // Per system: fixed-order sums of the 13 energy terms and the 6 virial components over the system's atoms, in two
-// passes. k_energy_part: one block per (256-atom chunk, system), a thread per atom, each of the 19 quantities summed by
+// passes. k_energy_part: one block per (system, 256-atom chunk), a thread per atom, each of the 19 quantities summed by
 // a fixed shuffle tree per warp and then over the warps in order; k_energy_final: per system, a warp per quantity over
 // the chunk partials (lane-strided, then a fixed shuffle tree). Chunks start at the system's first atom, so a system's sums are the same alone or in a
 // batch.
 constexpr int kESum = kTerms + kVir;
 __global__ void __launch_bounds__(256) k_energy_part(Dev d, double* part, int nchunk) {
-  const int c = blockIdx.x, sidx = blockIdx.y;
+  const int sidx = blockIdx.x, c = blockIdx.y;   // systems along x: any number of them
   const SysInfo& s = d.sys[sidx];
   if (c * 256 >= s.natoms) return;
   __shared__ double sh[8][kESum];
