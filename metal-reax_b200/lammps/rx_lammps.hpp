@@ -14,7 +14,10 @@
 // the box: the engine does not exchange halos).
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
+#include <cstdlib>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -36,6 +39,45 @@ struct Result {
   double pvector[14];      // pair->pvector (eb, ea, elp, emol, ev, epen, ecoa, ehb, et, eco, ew, ep, efi, eqeq)
   double eng_vdwl, eng_coul;
   double virial[6];        // pair->virial (xx, yy, zz, xy, xz, yz)
+};
+
+// An array exchanged with the engine every step (positions in, gradient out), in page-locked memory from
+// rx_host_alloc, which rx_set_positions and rx_compute copy from and into directly; in ordinary memory where
+// page-locked memory cannot be had (the engine then copies through its own staging buffer).
+class HostBuf {
+ public:
+  HostBuf() = default;
+  ~HostBuf() { release(); }
+  HostBuf(const HostBuf&) = delete;
+  HostBuf& operator=(const HostBuf&) = delete;
+  void resize(size_t n) {
+    if (n <= cap_ && p_) { n_ = n; return; }
+    release();
+    const size_t bytes = (n > 0 ? n : 1) * sizeof(double);
+    void* p = rx_host_alloc(bytes);
+    pinned_ = p != nullptr;
+    if (!p) p = std::malloc(bytes);
+    if (!p) throw std::bad_alloc();
+    p_ = static_cast<double*>(p);
+    cap_ = n > 0 ? n : 1;
+    n_ = n;
+  }
+  double* data() { return p_; }
+  double& operator[](size_t i) { return p_[i]; }
+  size_t size() const { return n_; }
+
+ private:
+  void release() {
+    if (p_) {
+      if (pinned_) rx_host_free(p_);
+      else std::free(p_);
+    }
+    p_ = nullptr;
+    cap_ = n_ = 0;
+  }
+  double* p_ = nullptr;
+  size_t cap_ = 0, n_ = 0;
+  bool pinned_ = false;
 };
 
 class RxLammps {
@@ -75,7 +117,8 @@ class RxLammps {
   std::vector<int> types_;
   double origin_[3] = {0, 0, 0}, box9_[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   int periodic_[3] = {1, 1, 1};
-  std::vector<double> xbuf_, gbuf_, qbuf_;
+  HostBuf xbuf_, gbuf_;              // positions in, gradient out: every step
+  std::vector<double> qbuf_;
 };
 
 }  // namespace rx_lammps

@@ -2,6 +2,7 @@
 // module, a Fortran caller, the tests): LAMMPS-layout arrays in, forces added into f, pair energy vector and virial out.
 #include <cstring>
 #include <memory>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -19,6 +20,11 @@ int guard(F&& f) {
     g_err = e.what();
     return 1;
   }
+}
+// the bridge behind a handle; a null handle (rxl_create failed, e.g. no usable GPU) is an error, not a crash
+rx_lammps::RxLammps* obj(void* h) {
+  if (!h) throw std::runtime_error("CUDA backend: null bridge handle (rxl_create failed)");
+  return static_cast<rx_lammps::RxLammps*>(h);
 }
 }  // namespace
 
@@ -48,13 +54,13 @@ int rxl_coeff(void* h, const char* ffield_text, const char* elements, int lgvdw)
         cur.push_back(*p);
       }
     }
-    static_cast<rx_lammps::RxLammps*>(h)->coeff(ffield_text, el, lgvdw != 0);
+    obj(h)->coeff(ffield_text, el, lgvdw != 0);
   });
 }
 
 int rxl_type_element(void* h, int lammps_type) {
   int out = -2;
-  guard([&] { out = static_cast<rx_lammps::RxLammps*>(h)->type_element(lammps_type); });
+  guard([&] { out = obj(h)->type_element(lammps_type); });
   return out;
 }
 
@@ -79,7 +85,7 @@ int rxl_compute(void* h, int nlocal, const double* x, const int* type, const int
     for (int d = 0; d < 3; ++d) { b.boxlo[d] = boxlo[d]; b.boxhi[d] = boxhi[d]; b.periodic[d] = periodic ? periodic[d] : 1; }
     if (tilt3) { b.xy = tilt3[0]; b.xz = tilt3[1]; b.yz = tilt3[2]; }
     rx_lammps::Result r;
-    static_cast<rx_lammps::RxLammps*>(h)->compute(nlocal, xp.data(), type, tag, q, b, fp.data(), r, eatom);
+    obj(h)->compute(nlocal, xp.data(), type, tag, q, b, fp.data(), r, eatom);
     if (out14) std::memcpy(out14, r.pvector, sizeof r.pvector);
     if (out2) { out2[0] = r.eng_vdwl; out2[1] = r.eng_coul; }
     if (virial6) std::memcpy(virial6, r.virial, sizeof r.virial);
@@ -94,7 +100,7 @@ int rxl_equilibrate(void* h, int nlocal, const double* x, const int* type, const
     rx_lammps::LammpsBox b;
     for (int d = 0; d < 3; ++d) { b.boxlo[d] = boxlo[d]; b.boxhi[d] = boxhi[d]; b.periodic[d] = periodic ? periodic[d] : 1; }
     if (tilt3) { b.xy = tilt3[0]; b.xz = tilt3[1]; b.yz = tilt3[2]; }
-    const auto it = static_cast<rx_lammps::RxLammps*>(h)->equilibrate(nlocal, xp.data(), type, tag, b, q);
+    const auto it = obj(h)->equilibrate(nlocal, xp.data(), type, tag, b, q);
     if (iters2) { iters2[0] = it.first; iters2[1] = it.second; }
   });
 }

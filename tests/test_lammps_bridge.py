@@ -52,6 +52,20 @@ def test_pair_coeff_mapping_and_box():
     assert np.array_equal(box.reshape(3, 3), [[10.0, 0, 0], [0.5, 10.0, 0], [-1.0, 2.0, 12.0]])
 
 
+def test_null_handle_is_an_error_not_a_crash():
+    """Where rxl_create fails (no usable GPU, a bad device ordinal), the calls that take its NULL handle report an
+    error through rxl_last_error instead of dereferencing it."""
+    lib = _lib()
+    assert lib.rxl_coeff(None, ffield_text().encode(), b"C H O", 0) == 1
+    assert b"null bridge handle" in lib.rxl_last_error()
+    assert lib.rxl_type_element(None, 1) == -2
+    f = np.zeros((1, 3))
+    zero3 = np.zeros(3)
+    assert lib.rxl_compute(None, 1, zero3.ctypes.data, None, None, None, zero3.ctypes.data, zero3.ctypes.data, None,
+                           None, f.ctypes.data, None, None, None, None) == 1
+    lib.rxl_destroy(None)   # deleting nothing is allowed
+
+
 @pytest.mark.gpu
 def test_bridge_matches_engine():
     import rxcuda
